@@ -1,0 +1,522 @@
+#!/usr/bin/env python
+"""Benchmark of the sparse solve path on B200 (one JSON line on rank 0).
+
+Default workload: CRS SpMV y = A*x in FP64 on the 3D 7-point Laplacian
+256^3 (n = 16,777,216, nnz = 117,047,296; 1.74 GB of algorithmic traffic
+per SpMV, larger than the 126 MB L2, so no flush is needed between steps).
+A "step" is one SpMV over the whole matrix.  The metric is achieved HBM
+GB/s with algorithmic bytes  nnz*(V+4) + (n+1)*4 + 2*n*X  per SpMV.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+* ``value``  -- GB/s of the device-resident SpMV (inputs already in HBM),
+  CUDA events on the launching stream, max over ranks; N GPUs run
+  independent replicas (the single-system SpMV does not shard without a
+  halo exchange), so the whole-job value is the sum over ranks.
+* ``e2e``    -- the same metric through the C ABI with host buffers: every
+  step copies x host->device from pinned memory, runs the SpMV and reads y
+  back (the matrix stays resident, as after the reference's ``send()``).
+* ``roofline`` -- the SpMV kernel's algorithmic bytes per launch / average
+  launch time against the measured HBM copy bandwidth; ``traffic`` is DRAM
+  bytes per launch from the committed ncu summary of this workload.
+* ``cpu_baseline`` -- the reference's own CPU SpMV (OpenMP row loop,
+  compiled from the reference sources) on the same matrix and the box's
+  host cores.
+* ``--impl reference`` -- times that reference CPU SpMV as the run's arm.
+
+Other workloads (``--workload``): spmv_poisson3d_f32, spmv_zipf_f64,
+spmv_zipf_f32, cg_poisson2d (128x128 Jacobi-CG to 1e-10, solves/s),
+bicgstab_convdiff (160^3 Jacobi-BiCGSTAB to 1e-10, solves/s).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC_SPMV = "SpMV HBM GB/s"
+METRIC_SOLVE = "solves/s at 1e-10 rel. residual"
+
+WORKLOADS = {
+    "spmv_poisson3d_f64": dict(kind="spmv", matrix="poisson3d", m=256, dtype="f64"),
+    "spmv_poisson3d_f32": dict(kind="spmv", matrix="poisson3d", m=256, dtype="f32"),
+    "spmv_zipf_f64": dict(kind="spmv", matrix="zipf", n=4194304, dtype="f64"),
+    "spmv_zipf_f32": dict(kind="spmv", matrix="zipf", n=4194304, dtype="f32"),
+    "cg_poisson2d": dict(kind="cg", matrix="poisson2d", m=128, dtype="f64"),
+    "bicgstab_convdiff": dict(kind="bicgstab", matrix="convdiff3d", m=160, dtype="f64"),
+}
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def describe(wl):
+    if wl["matrix"] == "poisson3d":
+        return f"3D 7-point Laplacian {wl['m']}^3 CRS<{'double' if wl['dtype'] == 'f64' else 'float'}>"
+    if wl["matrix"] == "zipf":
+        return (f"Zipf(2) rows n={wl['n']}, lengths 1..10000, uniform sorted columns, "
+                f"U[-1,1] values (seed 1), CRS<{'double' if wl['dtype'] == 'f64' else 'float'}>")
+    if wl["matrix"] == "poisson2d":
+        return f"2D 5-point Poisson {wl['m']}x{wl['m']}, Jacobi-CG, x_true U[-1,1] seed 0, tol 1e-10*||b||"
+    if wl["matrix"] == "convdiff3d":
+        return (f"3D upwind convection-diffusion {wl['m']}^3, cell Peclet 10, Jacobi-BiCGSTAB, "
+                f"x_true U[-1,1] seed 2, tol 1e-10*||b||")
+    return wl["matrix"]
+
+
+def make_matrix(wl):
+    from monolish_b200 import workloads as W
+    if wl["matrix"] == "poisson3d":
+        n, rp, ci, v = W.poisson3d(wl["m"])
+        x = W.uniform_fast(n, -1.0, 1.0, 1)
+    elif wl["matrix"] == "zipf":
+        n, rp, ci, v = W.zipf(wl["n"], seed=1)
+        x = W.uniform_fast(n, -1.0, 1.0, 1)
+    elif wl["matrix"] == "poisson2d":
+        n, rp, ci, v = W.poisson2d(wl["m"])
+        x = W.uniform_mt(n, -1.0, 1.0, 0)
+    elif wl["matrix"] == "convdiff3d":
+        n, rp, ci, v = W.convdiff3d(wl["m"], peclet=10.0)
+        x = W.uniform_mt(n, -1.0, 1.0, 2)
+    else:
+        raise ValueError(wl)
+    if wl["dtype"] == "f32":
+        v = v.astype(np.float32)
+        x = x.astype(np.float32)
+    return n, rp, ci, v, x
+
+
+def spmv_bytes(n, nnz, vsz):
+    return nnz * (vsz + 4) + (n + 1) * 4 + 2 * n * vsz
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.path = None
+        self.gpu = gpu_index
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def mark(self, which):
+        setattr(self, which, time.time())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [s.strip() for s in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for nm, val in zip(names[1:], f[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(nm)
+            os.unlink(self.path)
+        except OSError:
+            pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic(workload):
+    """DRAM bytes per launch of the SpMV kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"{workload}.traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+# ------------------------------------------------------------- CPU leg
+def cpu_reference_spmv(rp, ci, v, x, reps, threads):
+    """The reference's CPU SpMV (oracle/_ref build, OpenMP row loop)."""
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    import oracle
+    ref = oracle.reference_or_none()
+    if ref is not None:
+        ref.set_threads(threads)
+        _, mean_s, best_s = ref.spmv(rp, ci, v, x, reps=reps)
+        return mean_s, "reference", threads
+    port = oracle.restatement()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        port.spmv(rp, ci, v, x)
+    return (time.perf_counter() - t0) / reps, "port", 1
+
+
+# ------------------------------------------------------------- our arm
+def run_spmv(args, wl, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    from monolish_b200 import _abi
+    from monolish_b200 import device as D
+
+    torch.cuda.set_device(local)
+    n, rp, ci, v, x = make_matrix(wl)
+    nnz = int(rp[-1])
+    vsz = 8 if wl["dtype"] == "f64" else 4
+    B = spmv_bytes(n, nnz, vsz)
+    h = D.Handle()
+    A = D.Crs(h, n, n, rp, ci, v, validate=False)
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.empty(n, dtype=dx.dtype, device="cuda")
+    stream = torch.cuda.current_stream()
+    lib, hh, plan = h.lib, h.h, A.plan
+    xp, yp = dx.data_ptr(), dy.data_ptr()
+
+    def launch():
+        st = lib.mlsh_spmv(hh, plan, 1.0, xp, 0.0, yp)
+        if st != 0:
+            raise _abi.MlshError(st, "spmv")
+
+    for _ in range(args.warmup):
+        launch()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    # keep the sampler running over a warm-up soak so short timed regions
+    # still have clock samples of the same work around them
+    soak_end = time.time() + 1.0
+    while time.time() < soak_end:
+        launch()
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        launch()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    cl = clocks.stop()
+    h.sync()
+
+    # ---- end to end through the C ABI with host buffers
+    hx = torch.from_numpy(x).pin_memory()
+    hy = torch.empty(n, dtype=dx.dtype).pin_memory()
+    for _ in range(2):
+        dx.copy_(hx, non_blocking=True)
+        launch()
+        hy.copy_(dy, non_blocking=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(args.steps, 50))
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        dx.copy_(hx, non_blocking=True)
+        launch()
+        hy.copy_(dy, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        dist.barrier()
+
+    # correctness spot check against the oracle on a sample of rows
+    y = hy.numpy()
+    rows = np.linspace(0, n - 1, 2048).astype(np.int64)
+    ref_rows = np.array([np.dot(v[rp[i]:rp[i + 1]].astype(np.float64),
+                                x[ci[rp[i]:rp[i + 1]]].astype(np.float64)) for i in rows])
+    tol = 1e-12 if vsz == 8 else 1e-4
+    scale = np.array([np.abs(v[rp[i]:rp[i + 1]] * x[ci[rp[i]:rp[i + 1]]]).sum() for i in rows])
+    ok = bool(np.all(np.abs(y[rows] - ref_rows) <= tol * np.maximum(scale, 1e-30)))
+
+    if world > 1:
+        t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    per_launch_s = ms / 1e3 / args.steps
+    value = world * B * args.steps / (ms / 1e3) / 1e9
+    e2e_value = world * B * e2e_steps / (e2e_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    achieved = B / per_launch_s / 1e9
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            reps = 5
+            threads = os.cpu_count() or 1
+            sec, kind, cores = cpu_reference_spmv(rp, ci, v, x, reps, threads)
+            cpu = {"value": round(B / sec / 1e9, 3), "unit": "GB/s", "cores": cores,
+                   "kind": kind,
+                   "sample": f"{reps} full SpMVs of the same matrix (mean), {cores} threads"}
+        info = A.info()
+        out = {
+            "metric": METRIC_SPMV, "value": round(value, 2), "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
+            "data": "synthetic (seeded generators)",
+            "config": {"workload": describe(wl), "n": n, "nnz": nnz,
+                       "bytes_per_step": B, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (no flush needed)",
+                       "n_tiles": info["n_tiles"], "n_long_rows": info["n_long_rows"]},
+            "e2e": {"value": round(e2e_value, 2), "unit": "GB/s",
+                    "h2d_bytes_per_step": n * vsz, "d2h_bytes_per_step": n * vsz,
+                    "steps": e2e_steps},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "peak_kind": peak_kind,
+                         "traffic": profile_traffic(args.workload)},
+            "gpu_launches": args.steps,
+            "check": {"rows_checked": len(rows), "ok": ok},
+        }
+        if cpu:
+            out["cpu_baseline"] = cpu
+        if cl:
+            out["clocks"] = cl
+    A.close()
+    h.close()
+    return out
+
+
+def run_solve(args, wl, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    from monolish_b200 import device as D
+    import oracle
+
+    torch.cuda.set_device(local)
+    n, rp, ci, v, xt = make_matrix(wl)
+    port = oracle.restatement()
+    b = port.spmv(rp, ci, v, xt)
+    tol = 1e-10 * float(np.linalg.norm(b))
+    h = D.Handle()
+    A = D.Crs(h, n, n, rp, ci, v, validate=False)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.zeros(n, dtype=torch.float64, device="cuda")
+    fn = D.cg_solve if wl["kind"] == "cg" else D.bicgstab_solve
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        dx.zero_()
+        r = fn(A, db, dx, tol, 20000)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dx.zero_()
+        r = fn(A, db, dx, tol, 20000)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    cl = clocks.stop()
+    rel = port.true_relres(rp, ci, v, b, dx.cpu().numpy())
+    # end to end: b from pinned host memory, x back to host, per solve
+    hb = torch.from_numpy(b).pin_memory()
+    hx = torch.empty(n, dtype=torch.float64).pin_memory()
+    e0.record(stream)
+    for _ in range(args.steps):
+        db.copy_(hb, non_blocking=True)
+        dx.zero_()
+        r = fn(A, db, dx, tol, 20000)
+        hx.copy_(dx, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    out = None
+    if rank == 0:
+        nnz = int(rp[-1])
+        B_it = spmv_bytes(n, nnz, 8) - 2 * n * 8 + 13 * n * 8 if wl["kind"] == "cg" else \
+            2 * (spmv_bytes(n, nnz, 8) - 2 * n * 8) + 22 * n * 8
+        per_solve_s = ms / 1e3 / args.steps
+        achieved = B_it * r.iters / per_solve_s / 1e9
+        peak, peak_kind = measured_peak()
+        out = {
+            "metric": METRIC_SOLVE, "value": round(world * args.steps / (ms / 1e3), 3),
+            "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generators)",
+            "config": {"workload": describe(wl), "n": n, "nnz": nnz, "iters": r.iters,
+                       "status": r.status, "true_rel_residual": rel,
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": round(world * args.steps / (e2e_ms / 1e3), 3), "unit": "solves/s",
+                    "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "peak_kind": peak_kind, "traffic": None,
+                         "note": "whole-solve algorithmic bytes (fused minimum) / solve time"},
+            "gpu_launches": args.steps * (r.iters * (3 if wl["kind"] == "cg" else 5) + 3),
+        }
+        if world == 1 and not args.no_cpu:
+            ref = oracle.reference_or_none()
+            if ref is not None:
+                ref.set_threads(os.cpu_count() or 1)
+                st, it, res, xr, sec = getattr(ref, wl["kind"])(rp, ci, v, b, np.zeros(n), tol,
+                                                                20000)
+                out["cpu_baseline"] = {"value": round(1.0 / sec, 3), "unit": "solves/s",
+                                       "cores": os.cpu_count(), "kind": "reference",
+                                       "sample": f"1 full solve ({it} iterations)"}
+        if cl:
+            out["clocks"] = cl
+    A.close()
+    h.close()
+    return out
+
+
+# ---------------------------------------------------------- reference arm
+def run_reference(args, wl, rank, world):
+    if rank != 0:
+        return None
+    threads = os.cpu_count() or 1
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    n, rp, ci, v, x = make_matrix(wl)
+    import oracle
+    ref = oracle.reference_or_none()
+    kind = "reference" if ref is not None else "port"
+    if wl["kind"] == "spmv":
+        nnz = int(rp[-1])
+        vsz = 8 if wl["dtype"] == "f64" else 4
+        B = spmv_bytes(n, nnz, vsz)
+        if ref is not None:
+            ref.set_threads(threads)
+            ref.spmv(rp, ci, v, x, reps=max(1, args.warmup))
+            _, mean_s, _ = ref.spmv(rp, ci, v, x, reps=args.steps)
+        else:
+            threads = 1
+            mean_s, _, _ = cpu_reference_spmv(rp, ci, v, x, args.steps, 1)
+        value = B / mean_s / 1e9
+        return {"metric": METRIC_SPMV, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(mean_s * 1e3, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
+                "data": "synthetic (seeded generators)", "impl": "reference",
+                "config": {"workload": describe(wl), "n": n, "nnz": nnz, "bytes_per_step": B,
+                           "parallelism": "host OpenMP"},
+                "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads,
+                                 "kind": kind,
+                                 "sample": f"{args.steps} full SpMVs (mean), {threads} threads"},
+                "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+    port = oracle.restatement()
+    b = port.spmv(rp, ci, v, x)
+    tol = 1e-10 * float(np.linalg.norm(b))
+    if ref is None:
+        raise SystemExit("reference CPU build missing")
+    ref.set_threads(threads)
+    secs = []
+    for _ in range(args.steps):
+        st, it, res, xr, sec = getattr(ref, wl["kind"])(rp, ci, v, b, np.zeros(n), tol, 20000)
+        secs.append(sec)
+    value = 1.0 / statistics.mean(secs)
+    return {"metric": METRIC_SOLVE, "value": round(value, 4), "unit": "solves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(statistics.mean(secs) * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generators)", "impl": "reference",
+            "config": {"workload": describe(wl), "n": n, "iters": it, "status": st},
+            "cpu_baseline": {"value": round(value, 4), "unit": "solves/s", "cores": threads,
+                             "kind": kind, "sample": f"{args.steps} full solves"},
+            "e2e": {"value": round(value, 4), "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="spmv_poisson3d_f64")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = env_rank()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        out = run_reference(args, wl, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    try:
+        if wl["kind"] == "spmv":
+            out = run_spmv(args, wl, rank, world, local)
+        else:
+            out = run_solve(args, wl, rank, world, local)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,196 @@
+/*
+ * mlsh.h -- C ABI of the B200 (sm_100a) sparse iterative-solve library.
+ *
+ * This is the boundary a host-side binding links against: plain C types,
+ * device pointers, sizes, and a CUDA stream passed as `void *`; every call
+ * returns an `int` status and never throws, never exits.  The C++ drop-in
+ * layer (monolish_b200/cpp, monolish's own class/function names) and the
+ * Python test harness both sit on top of these entry points.
+ *
+ * Each entry point replaces one reference interface; the citation is the
+ * reference source it stands in for (paths inside the monolish project).
+ *
+ * Conventions
+ *   dtype        MLSH_F64 (double) or MLSH_F32 (float): the element type of
+ *                the matrix values and of every vector in the call.
+ *   pointers     device pointers (cudaMalloc'd or equivalent) unless the
+ *                name says `host`.  Vectors may be unaligned; 16-byte
+ *                aligned vectors take the vectorised path.
+ *   streams      `stream` is a cudaStream_t (NULL = legacy default stream).
+ *                Calls are asynchronous w.r.t. the host unless stated.
+ *   reductions   accumulate in double for both dtypes, in a fixed order:
+ *                repeated calls with the same inputs give bit-identical
+ *                results.
+ *   concurrency  a handle or a plan is used by one stream at a time (they
+ *                hold scratch buffers); use one handle per stream.
+ */
+#ifndef MLSH_H
+#define MLSH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ statuses --
+ * Solver codes are the reference's (include/monolish/common/
+ * monolish_common.hpp:16-21); library errors are new negative codes. */
+#define MLSH_SUCCESS 0
+#define MLSH_SOLVER_SIZE_ERROR (-1)
+#define MLSH_SOLVER_MAXITER (-2)
+#define MLSH_SOLVER_BREAKDOWN (-3)
+#define MLSH_SOLVER_RESIDUAL_NAN (-4)
+#define MLSH_NOT_IMPL (-10)
+#define MLSH_ERR_CUDA (-20)         /* a CUDA runtime call failed */
+#define MLSH_ERR_INVALID_ARG (-21)  /* NULL handle/pointer, bad dtype, n < 0 */
+#define MLSH_ERR_INVALID_CSR (-22)  /* row_ptr not monotone / col out of range */
+#define MLSH_ERR_OOM (-23)          /* device allocation failed */
+#define MLSH_ERR_TIMEOUT (-24)      /* a bounded device-side wait gave up */
+#define MLSH_ERR_NO_DEVICE (-25)    /* no CUDA device / not sm_100 */
+
+#define MLSH_F64 0
+#define MLSH_F32 1
+
+#define MLSH_PRECOND_NONE 0   /* equation::none (src/equation/none.cpp:40-46) */
+#define MLSH_PRECOND_JACOBI 1 /* equation::Jacobi (src/equation/jacobi.cpp:12-61) */
+
+typedef struct mlsh_handle_s *mlsh_handle;
+typedef struct mlsh_csr_plan_s *mlsh_csr_plan;
+
+/* ------------------------------------------------------------- library -- */
+/* Version as major*10000 + minor*100 + patch. */
+int mlsh_version(void);
+/* Human-readable text for a status code (static storage). */
+const char *mlsh_status_string(int status);
+/* Last CUDA error text recorded by this thread (static per thread). */
+const char *mlsh_last_error(void);
+
+/* A handle owns a stream binding and the small scratch buffers used by the
+ * reductions and solvers, on the device current at creation.  Replaces the
+ * per-call cublasCreate/cusparseCreate of the reference GPU path
+ * (src/blas/vector/dot.hpp:21-25, src/blas/matrix/matvec/crs_matvec.hpp:42-64). */
+int mlsh_create(mlsh_handle *handle);
+int mlsh_destroy(mlsh_handle handle);
+int mlsh_set_stream(mlsh_handle handle, void *stream);
+int mlsh_get_stream(mlsh_handle handle, void **stream);
+int mlsh_synchronize(mlsh_handle handle);
+
+/* --------------------------------------------------------------- CRS ---- */
+/* Build an SpMV plan over a device-resident CRS matrix (0-based row_ptr
+ * [n_rows+1], col_ind [nnz], val [nnz] of `dtype`), as matrix::CRS<T>
+ * holds it (include/monolish/common/monolish_crs.hpp:39-110) once send()
+ * has copied it (src/utils/system/gpu_comm.cpp:89-110).  The plan keeps the
+ * pointers (it does not copy the arrays; they must outlive it) and derives
+ * row tiles from row_ptr: from `host_row_ptr` when given, else from a copy
+ * of the device row_ptr.  `validate` != 0 also checks the structure on the
+ * host (monotone row_ptr, columns in range) and returns
+ * MLSH_ERR_INVALID_CSR on failure.  Synchronous. */
+int mlsh_csr_plan_create(mlsh_handle handle, int n_rows, int n_cols, int nnz,
+                         const int *d_row_ptr, const int *d_col_ind,
+                         const void *d_val, int dtype,
+                         const int *host_row_ptr, int validate,
+                         mlsh_csr_plan *plan);
+int mlsh_csr_plan_destroy(mlsh_csr_plan plan);
+/* Values changed in place (same structure): drop cached derived data
+ * (inverse diagonal, FP32 copy). */
+int mlsh_csr_plan_values_changed(mlsh_csr_plan plan);
+/* Introspection for tests and the autotuner: number of row tiles, of long
+ * rows split into chunks, and the algorithmic bytes of one SpMV
+ * (nnz*(V+4) + (n+1)*4 + 2*n*X). */
+int mlsh_csr_plan_info(mlsh_csr_plan plan, int *n_tiles, int *n_long_rows,
+                       int64_t *spmv_bytes);
+
+/* y = alpha*A*x + beta*y.  Replaces blas::matvec(A,x,y) and the
+ * matvec(a,A,x,b,y) overload (src/blas/matrix/matvec/matvec_blas.cpp:3849-3877,
+ * core src/blas/matrix/matvec/crs_matvec.hpp:8-114).  beta == 0 does not
+ * read y.  x and y must not alias. */
+int mlsh_spmv(mlsh_handle handle, mlsh_csr_plan plan, double alpha,
+              const void *d_x, double beta, void *d_y);
+
+/* d_diag[i] = A(i,i) (0 where the row has no diagonal entry).  Replaces
+ * CRS::diag (src/utils/getvec/crs_getvec.cpp:8-55). */
+int mlsh_csr_diag(mlsh_handle handle, mlsh_csr_plan plan, void *d_diag);
+
+/* ------------------------------------------------------ vector BLAS ----- */
+/* Results returned to host memory, like blas::dot/nrm2 on the reference GPU
+ * path (src/blas/vector/dot.hpp:6-41, nrm2.hpp:6-36); synchronous. */
+int mlsh_dot(mlsh_handle handle, int dtype, int64_t n, const void *d_x,
+             const void *d_y, double *host_result);
+int mlsh_nrm2(mlsh_handle handle, int dtype, int64_t n, const void *d_x,
+              double *host_result);
+/* Same reductions left on the device (one double at d_result); async. */
+int mlsh_dot_device(mlsh_handle handle, int dtype, int64_t n, const void *d_x,
+                    const void *d_y, double *d_result);
+int mlsh_nrm2_device(mlsh_handle handle, int dtype, int64_t n,
+                     const void *d_x, double *d_result);
+/* y = alpha*x + y          (src/blas/vector/axpy.hpp:7-34) */
+int mlsh_axpy(mlsh_handle handle, int dtype, int64_t n, double alpha,
+              const void *d_x, void *d_y);
+/* y = x + alpha*y          (src/blas/vector/xpay.hpp:7-36) */
+int mlsh_xpay(mlsh_handle handle, int dtype, int64_t n, double alpha,
+              const void *d_x, void *d_y);
+/* z = alpha*x + y          (src/blas/vector/axpyz.hpp:7-37) */
+int mlsh_axpyz(mlsh_handle handle, int dtype, int64_t n, double alpha,
+               const void *d_x, const void *d_y, void *d_z);
+/* y = x                    (src/blas/vector/copy.hpp:5-16) */
+int mlsh_copy(mlsh_handle handle, int dtype, int64_t n, const void *d_x,
+              void *d_y);
+/* y = a - b                (vml::sub, src/internal/arithmetic/double_arithmetic.cpp:141-168) */
+int mlsh_vsub(mlsh_handle handle, int dtype, int64_t n, const void *d_a,
+              const void *d_b, void *d_y);
+/* y = a .* b               (vml::mul, double_arithmetic.cpp:170-197) */
+int mlsh_vmul(mlsh_handle handle, int dtype, int64_t n, const void *d_a,
+              const void *d_b, void *d_y);
+/* y = 1 ./ a               (vml::reciprocal, double_arithmetic.cpp:308-330) */
+int mlsh_vreciprocal(mlsh_handle handle, int dtype, int64_t n,
+                     const void *d_a, void *d_y);
+/* y[i] = value             (vector(N, value) fill) */
+int mlsh_fill(mlsh_handle handle, int dtype, int64_t n, double value,
+              void *d_y);
+
+/* ------------------------------------------------------------ solvers --- */
+typedef struct {
+  double tol;       /* absolute threshold on ||r||_2, like solver::set_tol
+                       (src/equation/cg.cpp:67, equation.cpp:8-11) */
+  int64_t maxiter;  /* set_maxiter */
+  int64_t miniter;  /* set_miniter */
+  int precond;      /* MLSH_PRECOND_NONE / MLSH_PRECOND_JACOBI */
+  int use_graph;    /* 1: whole solve as one CUDA graph with a device-side
+                       while loop (no host round trip); 0: eager launches
+                       with a host check every `check_every` iterations */
+  int check_every;  /* eager mode only; <= 0 picks a default */
+  int reserved;
+} mlsh_solver_opts;
+
+typedef struct {
+  int status;          /* MLSH_SUCCESS / MLSH_SOLVER_MAXITER / ... */
+  int reserved;
+  int64_t iters;       /* solver::get_final_iter */
+  double final_resid;  /* solver::get_final_residual = ||r||_2 (absolute) */
+} mlsh_solver_result;
+
+/* Fills `opts` with the reference defaults (tol 1e-8, maxiter SIZE_MAX ->
+ * INT64_MAX, miniter 0, Jacobi, graph on). */
+int mlsh_solver_opts_default(mlsh_solver_opts *opts);
+
+/* Jacobi-preconditioned (or unpreconditioned) CG on the plan's matrix:
+ * x is the initial guess on entry and the solution on exit.  Follows the
+ * textbook recurrence of equation::CG (src/equation/cg.cpp:13-86) with the
+ * same stopping rule (||r|| < tol && miniter <= iter, NaN check).
+ * Synchronous; returns result->status. */
+int mlsh_cg_solve(mlsh_handle handle, mlsh_csr_plan plan, const void *d_b,
+                  void *d_x, const mlsh_solver_opts *opts,
+                  mlsh_solver_result *result);
+/* BiCGSTAB, following equation::BiCGSTAB (src/equation/bicgstab.cpp:13-135),
+ * including its breakdown checks (rho == 0, omega == 0). */
+int mlsh_bicgstab_solve(mlsh_handle handle, mlsh_csr_plan plan,
+                        const void *d_b, void *d_x,
+                        const mlsh_solver_opts *opts,
+                        mlsh_solver_result *result);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MLSH_H */

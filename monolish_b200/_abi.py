@@ -1,0 +1,112 @@
+"""ctypes declarations for the C ABI in include/mlsh.h.
+
+The library is loaded from this package's ``lib/`` directory; a missing
+library raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libmlsh.so")
+
+SUCCESS = 0
+SOLVER_SIZE_ERROR = -1
+SOLVER_MAXITER = -2
+SOLVER_BREAKDOWN = -3
+SOLVER_RESIDUAL_NAN = -4
+NOT_IMPL = -10
+ERR_CUDA = -20
+ERR_INVALID_ARG = -21
+ERR_INVALID_CSR = -22
+ERR_OOM = -23
+ERR_TIMEOUT = -24
+ERR_NO_DEVICE = -25
+
+F64 = 0
+F32 = 1
+PRECOND_NONE = 0
+PRECOND_JACOBI = 1
+
+vp = C.c_void_p
+i32 = C.c_int
+i64 = C.c_int64
+f64 = C.c_double
+
+
+class SolverOpts(C.Structure):
+    _fields_ = [("tol", f64), ("maxiter", i64), ("miniter", i64), ("precond", i32),
+                ("use_graph", i32), ("check_every", i32), ("reserved", i32)]
+
+
+class SolverResult(C.Structure):
+    _fields_ = [("status", i32), ("reserved", i32), ("iters", i64), ("final_resid", f64)]
+
+
+# name -> (restype, argtypes); every symbol include/mlsh.h declares
+SIGNATURES = {
+    "mlsh_version": (i32, []),
+    "mlsh_status_string": (C.c_char_p, [i32]),
+    "mlsh_last_error": (C.c_char_p, []),
+    "mlsh_create": (i32, [C.POINTER(vp)]),
+    "mlsh_destroy": (i32, [vp]),
+    "mlsh_set_stream": (i32, [vp, vp]),
+    "mlsh_get_stream": (i32, [vp, C.POINTER(vp)]),
+    "mlsh_synchronize": (i32, [vp]),
+    "mlsh_csr_plan_create": (i32, [vp, i32, i32, i32, vp, vp, vp, i32, vp, i32, C.POINTER(vp)]),
+    "mlsh_csr_plan_destroy": (i32, [vp]),
+    "mlsh_csr_plan_values_changed": (i32, [vp]),
+    "mlsh_csr_plan_info": (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i64)]),
+    "mlsh_spmv": (i32, [vp, vp, f64, vp, f64, vp]),
+    "mlsh_csr_diag": (i32, [vp, vp, vp]),
+    "mlsh_dot": (i32, [vp, i32, i64, vp, vp, C.POINTER(f64)]),
+    "mlsh_nrm2": (i32, [vp, i32, i64, vp, C.POINTER(f64)]),
+    "mlsh_dot_device": (i32, [vp, i32, i64, vp, vp, vp]),
+    "mlsh_nrm2_device": (i32, [vp, i32, i64, vp, vp]),
+    "mlsh_axpy": (i32, [vp, i32, i64, f64, vp, vp]),
+    "mlsh_xpay": (i32, [vp, i32, i64, f64, vp, vp]),
+    "mlsh_axpyz": (i32, [vp, i32, i64, f64, vp, vp, vp]),
+    "mlsh_copy": (i32, [vp, i32, i64, vp, vp]),
+    "mlsh_vsub": (i32, [vp, i32, i64, vp, vp, vp]),
+    "mlsh_vmul": (i32, [vp, i32, i64, vp, vp, vp]),
+    "mlsh_vreciprocal": (i32, [vp, i32, i64, vp, vp]),
+    "mlsh_fill": (i32, [vp, i32, i64, f64, vp]),
+    "mlsh_solver_opts_default": (i32, [C.POINTER(SolverOpts)]),
+    "mlsh_cg_solve": (i32, [vp, vp, vp, vp, C.POINTER(SolverOpts), C.POINTER(SolverResult)]),
+    "mlsh_bicgstab_solve": (i32, [vp, vp, vp, vp, C.POINTER(SolverOpts),
+                                  C.POINTER(SolverResult)]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libmlsh.so (raises OSError if it is missing or fails to load)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"CUDA library not built: {path} (run __graft_entry__.build())")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class MlshError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        lib = _lib
+        msg = lib.mlsh_status_string(status).decode() if lib else str(status)
+        detail = lib.mlsh_last_error().decode() if lib else ""
+        super().__init__(f"{what}: {msg} ({status}) {detail}".strip())
+        self.status = status
+
+
+def check(status: int, what: str = "", ok=(SUCCESS,)):
+    if status not in ok:
+        raise MlshError(status, what)
+    return status

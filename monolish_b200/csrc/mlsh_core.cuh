@@ -1,0 +1,33 @@
+// Cross-translation-unit declarations.  Kernel templates are instantiated in
+// exactly one translation unit each; other units call the host launchers
+// declared here.
+#pragma once
+#include "mlsh_internal.cuh"
+#include "mlsh_spmv.cuh"
+#include "mlsh_vec.cuh"
+
+namespace mlsh {
+
+int init_kernel_attributes();
+
+void build_tiles(const int *rp, int n_rows, std::vector<Tile> &tiles,
+                 std::vector<LongRow> &longs, int &n_chunks);
+
+// y_out = alpha*A*x + beta*y_in with the fused dots selected by M0/M1
+// (instantiated in mlsh_core.cu for VT = double/float and the mode pairs
+// (none,none), (w,none), (w,self), (self,none)).
+template <typename VT, int M0, int M1>
+cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
+                          const VT *x, double beta, const VT *y_in, VT *y_out,
+                          const VT *w0, const VT *w1, double *dot_out,
+                          const int *done, cudaStream_t stream);
+
+int plan_diag(const CsrPlan &p, void *out, bool invert, cudaStream_t stream);
+int plan_inv_diag(CsrPlan &p, cudaStream_t stream, const void **out);
+
+// Solver-side resources kept on the handle / plan (mlsh_krylov.cu).
+void release_solver_graphs(Handle &h);
+void release_plan_extras(CsrPlan &p);
+void invalidate_plan_extras(CsrPlan &p);
+
+}  // namespace mlsh

@@ -1,0 +1,149 @@
+// Internal definitions shared by the CUDA translation units: the handle and
+// plan objects behind the opaque C types, the device solver-state block,
+// launch geometry constants and error plumbing.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <vector>
+
+#include "../../include/mlsh.h"
+
+namespace mlsh {
+
+// ----------------------------------------------------------- geometry ----
+// SpMV row tiles: at most kTileRows rows and kTileNnz nonzeros each, so one
+// consumer thread owns one row of a tile and a tile's values+indices fit a
+// pipeline stage in shared memory.  Rows longer than kTileNnz are split into
+// chunks of kTileNnz nonzeros that are summed by a second step.
+constexpr int kTileRows = 256;
+constexpr int kTileNnz = 1792;  // = 256 rows x 7 nonzeros (7-point stencil)
+constexpr int kConsumers = 256;  // consumer threads per CTA (8 warps)
+constexpr int kSpmvThreads = kConsumers + 32;  // + one producer warp
+constexpr int kStages = 3;       // shared-memory pipeline depth
+constexpr int kShortRow = 32;    // rows up to this length: thread-per-row sum
+
+// Elementwise / reduction kernels.
+constexpr int kVecThreads = 256;
+constexpr int kMaxVecBlocksPerSm = 8;
+constexpr int kMaxPartialBlocks = 4096;  // upper bound of any reduction grid
+constexpr int kMaxRed = 4;               // reduction values per kernel
+
+// Device waits give up after this long and report MLSH_ERR_TIMEOUT.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
+
+// Solver status while iterating.
+constexpr int kRunning = 1;
+
+// --------------------------------------------------------- tile record ---
+// Normal tile: rows [row_begin, row_end), nonzeros [nnz_begin, nnz_end).
+// Chunk of a long row: row_begin = row, row_end = -(long_index + 1).
+struct Tile {
+  int row_begin;
+  int row_end;
+  int nnz_begin;
+  int nnz_end;
+};
+
+struct LongRow {
+  int row;
+  int first_slot;  // index of chunk 0 in the plan's chunk-partial array
+  int n_chunks;
+  int pad;
+};
+
+// ------------------------------------------------- device solver state ---
+// One block per handle; written only by the last CTA of each kernel (after
+// every other CTA has finished reading it) or by single-thread kernels.
+struct SolverState {
+  // scalars of the recurrences (double for both dtypes)
+  double rz;       // CG: (z, r) of the current iterate
+  double rz_new;   // CG: (z, r) after the update
+  double pq;       // CG: (p, A p)
+  double rr;       // (r, r)
+  double rho;      // BiCGSTAB: (r, r0)
+  double rho_old;
+  double alpha;
+  double omega;
+  double vr0;      // BiCGSTAB: (v, r0)
+  double ts;       // BiCGSTAB: (t, s)
+  double tt;       // BiCGSTAB: (t, t)
+  double resid;    // ||r||_2 as the stopping rule sees it
+  double tol;      // absolute tolerance
+  double pad0;
+  long long iter;  // iterations completed
+  long long maxiter;
+  long long miniter;
+  int status;      // kRunning or a final MLSH_* code
+  int done;        // 1 once status is final
+  int error;       // MLSH_ERR_TIMEOUT if a device wait gave up
+  int pad1;
+};
+
+// ------------------------------------------------------------- objects ---
+struct Handle {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  // reduction scratch: per-block partials + one arrival counter per slot
+  double *partials = nullptr;    // kMaxPartialBlocks * kMaxRed doubles
+  unsigned *counters = nullptr;  // 8 counters, zero between kernels
+  double *scalars = nullptr;     // 8 doubles of device results
+  SolverState *state = nullptr;
+  SolverState *host_state = nullptr;  // pinned mirror
+  double *host_scalars = nullptr;     // pinned
+  int *err_flag = nullptr;            // device: nonzero after a timeout
+  cudaStream_t capture_stream = nullptr;  // private stream for graph capture
+  void *ws = nullptr;                 // solver work vectors
+  size_t ws_bytes = 0;
+  void *graph_cache = nullptr;        // instantiated solver graphs
+};
+
+struct CsrPlan {
+  Handle *handle = nullptr;
+  int n_rows = 0, n_cols = 0, nnz = 0;
+  int dtype = MLSH_F64;
+  const int *row_ptr = nullptr;
+  const int *col_ind = nullptr;
+  const void *val = nullptr;
+  // derived
+  int n_tiles = 0;
+  int n_long = 0;
+  int n_chunks = 0;
+  Tile *tiles = nullptr;          // device
+  LongRow *longs = nullptr;       // device
+  double *chunk_part = nullptr;   // device, n_chunks
+  unsigned *long_cnt = nullptr;   // device, n_long (zero between launches)
+  double *long_dot = nullptr;     // device, 2 * n_long
+  int spmv_grid = 0;              // CTAs of the SpMV launch
+  // cached derived data
+  void *inv_diag = nullptr;       // 1/diag(A), dtype elements
+  bool inv_diag_valid = false;
+  void *extras = nullptr;         // precision/format variants (mixed solver)
+};
+
+// -------------------------------------------------------------- errors ---
+void set_last_error(const char *where, cudaError_t e);
+
+#define MLSH_CUDA_TRY(expr)                         \
+  do {                                              \
+    cudaError_t _e = (expr);                        \
+    if (_e != cudaSuccess) {                        \
+      ::mlsh::set_last_error(#expr, _e);            \
+      return MLSH_ERR_CUDA;                         \
+    }                                               \
+  } while (0)
+
+inline int dtype_size(int dtype) {
+  return dtype == MLSH_F64 ? 8 : (dtype == MLSH_F32 ? 4 : 0);
+}
+
+}  // namespace mlsh
+
+struct mlsh_handle_s {
+  mlsh::Handle h;
+};
+struct mlsh_csr_plan_s {
+  mlsh::CsrPlan p;
+};

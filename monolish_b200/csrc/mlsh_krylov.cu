@@ -1,0 +1,718 @@
+// Plain CG and BiCGSTAB on one GPU with device-resident scalars.
+//
+// Reference recurrences kept term for term (no pipelined / s-step
+// variants, so iteration counts match the reference's):
+//   CG        src/equation/cg.cpp:13-86
+//   BiCGSTAB  src/equation/bicgstab.cpp:13-135
+//   Jacobi    src/equation/jacobi.cpp:12-61 (M = 1/diag(A), z = M.*r)
+//   stopping  ||r||_2 < tol && miniter <= iter, then NaN check
+//             (cg.cpp:61-78, equation.cpp:8-11)
+//
+// Where the reference makes 4-5 host round trips per iteration (every dot
+// returns to the host), here every scalar stays on the device: the last CTA
+// of each reduction kernel writes it into the handle's SolverState and the
+// next kernel reads it.  Per CG iteration there are three kernels:
+//   K1  q = A p              fused with (p, q)
+//   K2  x += a p, r -= a q   fused with (z, r), (r, r)   [z = M.*r on the fly]
+//   K3  p = z + b p          + stopping test in the last CTA
+// (BiCGSTAB: five).  The loop body is captured once into a CUDA graph whose
+// conditional WHILE node repeats it until the last CTA of K3 clears the
+// condition, so a whole solve is one graph launch and one final read.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "mlsh_core.cuh"
+
+namespace mlsh {
+
+template <typename T>
+__device__ __forceinline__ double resid_of(double rr) {
+  if constexpr (sizeof(T) == 8) {
+    return sqrt(rr);
+  } else {
+    return (double)sqrtf((float)rr);
+  }
+}
+
+struct CondRef {
+  cudaGraphConditionalHandle handle;
+  int enabled;
+  __device__ void set(int v) const {
+    if (enabled) cudaGraphSetConditional(handle, (unsigned)v);
+  }
+};
+
+// Final bookkeeping of one iteration (CG K3 / BiCGSTAB B5 last CTA).
+template <typename T>
+__device__ void finish_iteration(SolverState *st, const CondRef &cond) {
+  const long long it = st->iter + 1;
+  st->iter = it;
+  const double res = resid_of<T>(st->rr);
+  st->resid = res;
+  if (res < st->tol && st->miniter <= it) {
+    st->status = MLSH_SUCCESS;
+    st->done = 1;
+  } else if (isnan(res)) {
+    st->status = MLSH_SOLVER_RESIDUAL_NAN;
+    st->done = 1;
+  } else if (it >= st->maxiter) {
+    st->status = MLSH_SOLVER_MAXITER;
+    st->done = 1;
+  }
+}
+
+// ------------------------------------------------------------------- CG --
+template <typename T, bool JAC>
+struct CgInitBody : NoPrep {  // z = M r, p = z; sums (z,r), (r,r)
+  const T *r;
+  T *p;
+  const T *d;
+  SolverState *st;
+  CondRef cond;
+  __device__ void operator()(int64_t i, double *acc) const {
+    const T ri = r[i];
+    const T zi = JAC ? d[i] * ri : ri;
+    p[i] = zi;
+    acc[0] += (double)zi * (double)ri;
+    acc[1] += (double)ri * (double)ri;
+  }
+  __device__ void finish(const double *s) {
+    st->rz = s[0];
+    st->rr = s[1];
+    st->resid = resid_of<T>(s[1]);
+    if (st->maxiter <= 0) {
+      st->status = MLSH_SOLVER_MAXITER;
+      st->done = 1;
+    }
+    cond.set(st->done ? 0 : 1);
+  }
+};
+
+template <typename T, bool JAC>
+struct CgXRBody : NoPrep {  // x += a p; r -= a q; sums (z,r), (r,r)
+  T *x;
+  T *r;
+  const T *p;
+  const T *q;
+  const T *d;
+  SolverState *st;
+  T alpha;
+  __device__ void prepare() { alpha = (T)(st->rz / st->pq); }
+  __device__ void operator()(int64_t i, double *acc) const {
+    const T pi = p[i], qi = q[i];
+    x[i] = alpha * pi + x[i];
+    const T ri = -alpha * qi + r[i];
+    r[i] = ri;
+    const T zi = JAC ? d[i] * ri : ri;
+    acc[0] += (double)zi * (double)ri;
+    acc[1] += (double)ri * (double)ri;
+  }
+  __device__ void finish(const double *s) {
+    st->rz_new = s[0];
+    st->rr = s[1];
+  }
+};
+
+template <typename T, bool JAC>
+struct CgPBody : NoPrep {  // p = z + b p; stopping test
+  T *p;
+  const T *r;
+  const T *d;
+  SolverState *st;
+  CondRef cond;
+  T beta;
+  __device__ void prepare() { beta = (T)(st->rz_new / st->rz); }
+  __device__ void operator()(int64_t i, double *) const {
+    const T ri = r[i];
+    const T zi = JAC ? d[i] * ri : ri;
+    p[i] = zi + beta * p[i];
+  }
+  __device__ void finish(const double *) {
+    st->rz = st->rz_new;
+    finish_iteration<T>(st, cond);
+    cond.set(st->done ? 0 : 1);
+  }
+};
+
+// ------------------------------------------------------------- BiCGSTAB --
+template <typename T>
+__device__ void bicg_rho_check(SolverState *st) {
+  // start of the next iteration: rho = (r, r0) == 0 -> breakdown
+  // (bicgstab.cpp:56-63); final_iter is that iteration's index + 1.
+  if (!st->done && st->rho == 0.0) {
+    st->status = MLSH_SOLVER_BREAKDOWN;
+    st->done = 1;
+    st->iter = st->iter + 1;
+  }
+}
+
+template <typename T>
+struct BiInitBody : NoPrep {  // r0 = r; sums (r, r0), (r, r)
+  const T *r;
+  T *r0;
+  SolverState *st;
+  CondRef cond;
+  __device__ void operator()(int64_t i, double *acc) const {
+    const T ri = r[i];
+    r0[i] = ri;
+    acc[0] += (double)ri * (double)ri;
+    acc[1] += (double)ri * (double)ri;
+  }
+  __device__ void finish(const double *s) {
+    st->rho = s[0];
+    st->rr = s[1];
+    st->rho_old = 1.0;
+    st->alpha = 1.0;
+    st->omega = 1.0;
+    st->resid = resid_of<T>(s[1]);
+    if (st->maxiter <= 0) {
+      st->status = MLSH_SOLVER_MAXITER;
+      st->done = 1;
+    } else {
+      bicg_rho_check<T>(st);
+    }
+    cond.set(st->done ? 0 : 1);
+  }
+};
+
+template <typename T, bool JAC>
+struct BiPBody : NoPrep {  // p = r + beta (p - omega v); phat = M p
+  const T *r;
+  T *p;
+  const T *v;
+  T *phat;
+  const T *d;
+  SolverState *st;
+  T beta, omega;
+  int first;
+  __device__ void prepare() {
+    first = st->iter == 0;
+    omega = (T)st->omega;
+    beta = (T)((st->rho / st->rho_old) * (st->alpha / st->omega));
+  }
+  __device__ void operator()(int64_t i, double *) const {
+    T pi;
+    if (first) {
+      pi = r[i];
+    } else {
+      const T t = -omega * v[i] + p[i];
+      pi = r[i] + beta * t;
+    }
+    p[i] = pi;
+    if (JAC) phat[i] = d[i] * pi;
+  }
+};
+
+template <typename T, bool JAC>
+struct BiSBody : NoPrep {  // alpha = rho/(v,r0); s = r - alpha v; shat = M s
+  const T *r;
+  const T *v;
+  T *s;
+  T *shat;
+  const T *d;
+  SolverState *st;
+  T alpha;
+  double alpha_d;
+  __device__ void prepare() {
+    alpha_d = st->rho / st->vr0;
+    alpha = (T)alpha_d;
+  }
+  __device__ void operator()(int64_t i, double *) const {
+    const T si = -alpha * v[i] + r[i];
+    s[i] = si;
+    if (JAC) shat[i] = d[i] * si;
+  }
+  __device__ void finish(const double *) { st->alpha = (double)alpha; }
+};
+
+template <typename T>
+struct BiXRBody : NoPrep {  // omega = (t,s)/(t,t); x += a phat + w shat; r = s - w t
+  T *x;
+  T *r;
+  const T *r0;
+  const T *phat;
+  const T *shat;
+  const T *s;
+  const T *t;
+  SolverState *st;
+  CondRef cond;
+  T alpha, omega;
+  int brk;
+  __device__ void prepare() {
+    omega = (T)(st->ts / st->tt);
+    alpha = (T)st->alpha;
+    brk = (omega == T(0));
+  }
+  __device__ void operator()(int64_t i, double *acc) const {
+    if (brk) return;
+    T xi = alpha * phat[i] + x[i];
+    xi = omega * shat[i] + xi;
+    x[i] = xi;
+    const T ri = -omega * t[i] + s[i];
+    r[i] = ri;
+    acc[0] += (double)ri * (double)r0[i];
+    acc[1] += (double)ri * (double)ri;
+  }
+  __device__ void finish(const double *sums) {
+    if (brk) {
+      // bicgstab.cpp:93-98: breakdown before x and r are updated
+      st->status = MLSH_SOLVER_BREAKDOWN;
+      st->done = 1;
+      st->iter = st->iter + 1;
+      st->resid = resid_of<T>(st->rr);
+    } else {
+      st->omega = (double)omega;
+      st->rho_old = st->rho;
+      st->rho = sums[0];
+      st->rr = sums[1];
+      finish_iteration<T>(st, cond);
+      bicg_rho_check<T>(st);
+    }
+    cond.set(st->done ? 0 : 1);
+  }
+};
+
+// --------------------------------------------------------------- driver --
+namespace {
+
+template <int NR, bool FIN, typename Body>
+cudaError_t run_body(const Handle &h, int64_t n, const Body &b, const int *done,
+                     cudaStream_t s) {
+  RedArgs ra{h.partials, h.counters, done};
+  vec_kernel<NR, FIN, Body><<<vec_grid(n, h.num_sms), kVecThreads, 0, s>>>(n, b, ra);
+  return cudaGetLastError();
+}
+
+enum Kind { kCG = 0, kBiCGSTAB = 1 };
+
+struct SolveCtx {
+  Kind kind;
+  int dtype;
+  int jac;
+  const CsrPlan *plan;
+  const Handle *h;
+  const void *b;
+  void *x;
+  const void *d;  // inverse diagonal (Jacobi) or null
+  void *ws;       // work vectors, `stride` elements apart
+  int64_t n;
+  int64_t stride;
+};
+
+template <typename T>
+T *wsv(const SolveCtx &c, int k) {
+  return static_cast<T *>(c.ws) + (size_t)k * (size_t)c.stride;
+}
+
+// ---- CG
+template <typename T, bool JAC>
+cudaError_t cg_init(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  T *r = wsv<T>(c, 0), *p = wsv<T>(c, 1);
+  cudaError_t e = launch_spmv_t<T, kDotNone, kDotNone>(
+      *c.plan, *c.h, -1.0, static_cast<const T *>(c.x), 1.0,
+      static_cast<const T *>(c.b), r, nullptr, nullptr, nullptr, nullptr, s);
+  if (e != cudaSuccess) return e;
+  CgInitBody<T, JAC> ib;
+  ib.r = r; ib.p = p; ib.d = static_cast<const T *>(c.d); ib.st = c.h->state; ib.cond = cond;
+  return run_body<2, true>(*c.h, c.n, ib, nullptr, s);
+}
+
+template <typename T, bool JAC>
+cudaError_t cg_iter(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  T *r = wsv<T>(c, 0), *p = wsv<T>(c, 1), *q = wsv<T>(c, 2);
+  SolverState *st = c.h->state;
+  const int *done = &st->done;
+  cudaError_t e = launch_spmv_t<T, kDotW, kDotNone>(*c.plan, *c.h, 1.0, p, 0.0, nullptr, q,
+                                                    p, nullptr, &st->pq, done, s);
+  if (e != cudaSuccess) return e;
+  CgXRBody<T, JAC> xb;
+  xb.x = static_cast<T *>(c.x); xb.r = r; xb.p = p; xb.q = q;
+  xb.d = static_cast<const T *>(c.d); xb.st = st;
+  e = run_body<2, true>(*c.h, c.n, xb, done, s);
+  if (e != cudaSuccess) return e;
+  CgPBody<T, JAC> pb;
+  pb.p = p; pb.r = r; pb.d = static_cast<const T *>(c.d); pb.st = st; pb.cond = cond;
+  return run_body<0, true>(*c.h, c.n, pb, done, s);
+}
+
+// ---- BiCGSTAB: ws = r, r0, p, v, s, t, phat, shat
+template <typename T, bool JAC>
+cudaError_t bi_init(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  T *r = wsv<T>(c, 0), *r0 = wsv<T>(c, 1);
+  cudaError_t e = launch_spmv_t<T, kDotNone, kDotNone>(
+      *c.plan, *c.h, -1.0, static_cast<const T *>(c.x), 1.0,
+      static_cast<const T *>(c.b), r, nullptr, nullptr, nullptr, nullptr, s);
+  if (e != cudaSuccess) return e;
+  BiInitBody<T> ib;
+  ib.r = r; ib.r0 = r0; ib.st = c.h->state; ib.cond = cond;
+  return run_body<2, true>(*c.h, c.n, ib, nullptr, s);
+}
+
+template <typename T, bool JAC>
+cudaError_t bi_iter(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  T *r = wsv<T>(c, 0), *r0 = wsv<T>(c, 1), *p = wsv<T>(c, 2), *v = wsv<T>(c, 3);
+  T *sv = wsv<T>(c, 4), *t = wsv<T>(c, 5);
+  T *phat = JAC ? wsv<T>(c, 6) : p;
+  T *shat = JAC ? wsv<T>(c, 7) : sv;
+  const T *d = static_cast<const T *>(c.d);
+  SolverState *st = c.h->state;
+  const int *done = &st->done;
+  BiPBody<T, JAC> pb;
+  pb.r = r; pb.p = p; pb.v = v; pb.phat = phat; pb.d = d; pb.st = st;
+  cudaError_t e = run_body<0, false>(*c.h, c.n, pb, done, s);
+  if (e != cudaSuccess) return e;
+  e = launch_spmv_t<T, kDotW, kDotNone>(*c.plan, *c.h, 1.0, phat, 0.0, nullptr, v, r0,
+                                        nullptr, &st->vr0, done, s);
+  if (e != cudaSuccess) return e;
+  BiSBody<T, JAC> sb;
+  sb.r = r; sb.v = v; sb.s = sv; sb.shat = shat; sb.d = d; sb.st = st;
+  e = run_body<0, true>(*c.h, c.n, sb, done, s);
+  if (e != cudaSuccess) return e;
+  e = launch_spmv_t<T, kDotW, kDotSelf>(*c.plan, *c.h, 1.0, shat, 0.0, nullptr, t, sv,
+                                        nullptr, &st->ts, done, s);
+  if (e != cudaSuccess) return e;
+  BiXRBody<T> xb;
+  xb.x = static_cast<T *>(c.x); xb.r = r; xb.r0 = r0; xb.phat = phat; xb.shat = shat;
+  xb.s = sv; xb.t = t; xb.st = st; xb.cond = cond;
+  return run_body<2, true>(*c.h, c.n, xb, done, s);
+}
+
+using StepFn = cudaError_t (*)(const SolveCtx &, cudaStream_t, CondRef);
+
+void pick_steps(const SolveCtx &c, StepFn *init, StepFn *iter) {
+  const bool f64 = c.dtype == MLSH_F64;
+  if (c.kind == kCG) {
+    if (f64) {
+      *init = c.jac ? cg_init<double, true> : cg_init<double, false>;
+      *iter = c.jac ? cg_iter<double, true> : cg_iter<double, false>;
+    } else {
+      *init = c.jac ? cg_init<float, true> : cg_init<float, false>;
+      *iter = c.jac ? cg_iter<float, true> : cg_iter<float, false>;
+    }
+  } else {
+    if (f64) {
+      *init = c.jac ? bi_init<double, true> : bi_init<double, false>;
+      *iter = c.jac ? bi_iter<double, true> : bi_iter<double, false>;
+    } else {
+      *init = c.jac ? bi_init<float, true> : bi_init<float, false>;
+      *iter = c.jac ? bi_iter<float, true> : bi_iter<float, false>;
+    }
+  }
+}
+
+// ------------------------------------------------------- graph cache ----
+struct GraphEntry {
+  Kind kind;
+  int dtype, jac;
+  const CsrPlan *plan;
+  const void *b;
+  void *x;
+  const void *d;
+  void *ws;
+  int64_t n;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+  unsigned long long last_use;
+};
+
+struct GraphCache {
+  std::vector<GraphEntry> entries;
+  unsigned long long clock = 0;
+};
+
+GraphCache &cache_of(Handle &h) {
+  if (!h.graph_cache) h.graph_cache = new GraphCache();
+  return *static_cast<GraphCache *>(h.graph_cache);
+}
+
+void destroy_entry(GraphEntry &e) {
+  if (e.exec) cudaGraphExecDestroy(e.exec);
+  if (e.graph) cudaGraphDestroy(e.graph);
+  e.exec = nullptr;
+  e.graph = nullptr;
+}
+
+// Builds  [init kernels] -> WHILE(cond) { one iteration }  as one graph.
+int build_graph(const SolveCtx &c, Handle &h, GraphEntry &out) {
+  StepFn init, iter;
+  pick_steps(c, &init, &iter);
+  cudaGraph_t g = nullptr;
+  MLSH_CUDA_TRY(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle cond;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_last_error("cudaGraphConditionalHandleCreate", e);
+    return MLSH_ERR_CUDA;
+  }
+  CondRef cr{cond, 1};
+  // init part, captured into g
+  e = cudaStreamBeginCaptureToGraph(h.capture_stream, g, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaError_t e2 = init(c, h.capture_stream, cr);
+    cudaGraph_t gg = nullptr;
+    e = cudaStreamEndCapture(h.capture_stream, &gg);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_last_error("capture solver init", e);
+    return MLSH_ERR_CUDA;
+  }
+  // leaves of the init part
+  size_t nn = 0;
+  cudaGraphGetNodes(g, nullptr, &nn);
+  std::vector<cudaGraphNode_t> nodes(nn), leaves;
+  cudaGraphGetNodes(g, nodes.data(), &nn);
+  for (auto nd : nodes) {
+    size_t nd_out = 0;
+    cudaGraphNodeGetDependentNodes(nd, nullptr, &nd_out);
+    if (nd_out == 0) leaves.push_back(nd);
+  }
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  e = cudaGraphAddNode(&cnode, g, leaves.data(), leaves.size(), &cp);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_last_error("cudaGraphAddNode(while)", e);
+    return MLSH_ERR_CUDA;
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(h.capture_stream, body, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaError_t e2 = iter(c, h.capture_stream, cr);
+    cudaGraph_t bb = nullptr;
+    e = cudaStreamEndCapture(h.capture_stream, &bb);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_last_error("capture solver body", e);
+    return MLSH_ERR_CUDA;
+  }
+  cudaGraphExec_t ex = nullptr;
+  e = cudaGraphInstantiate(&ex, g, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_last_error("cudaGraphInstantiate", e);
+    return MLSH_ERR_CUDA;
+  }
+  out.graph = g;
+  out.exec = ex;
+  return MLSH_SUCCESS;
+}
+
+int get_graph(const SolveCtx &c, Handle &h, cudaGraphExec_t *ex) {
+  GraphCache &gc = cache_of(h);
+  ++gc.clock;
+  for (auto &e : gc.entries) {
+    if (e.kind == c.kind && e.dtype == c.dtype && e.jac == c.jac && e.plan == c.plan &&
+        e.b == c.b && e.x == c.x && e.d == c.d && e.ws == c.ws && e.n == c.n) {
+      e.last_use = gc.clock;
+      *ex = e.exec;
+      return MLSH_SUCCESS;
+    }
+  }
+  GraphEntry ne{c.kind, c.dtype, c.jac, c.plan, c.b, c.x, c.d, c.ws, c.n, nullptr, nullptr,
+                gc.clock};
+  int st = build_graph(c, h, ne);
+  if (st != MLSH_SUCCESS) return st;
+  constexpr size_t kMaxEntries = 16;
+  if (gc.entries.size() >= kMaxEntries) {
+    size_t victim = 0;
+    for (size_t i = 1; i < gc.entries.size(); ++i)
+      if (gc.entries[i].last_use < gc.entries[victim].last_use) victim = i;
+    destroy_entry(gc.entries[victim]);
+    gc.entries.erase(gc.entries.begin() + victim);
+  }
+  gc.entries.push_back(ne);
+  *ex = ne.exec;
+  return MLSH_SUCCESS;
+}
+
+void purge_graphs(Handle &h, const CsrPlan *plan, const void *ws) {
+  if (!h.graph_cache) return;
+  GraphCache &gc = cache_of(h);
+  for (size_t i = 0; i < gc.entries.size();) {
+    if ((plan && gc.entries[i].plan == plan) || (ws && gc.entries[i].ws == ws)) {
+      destroy_entry(gc.entries[i]);
+      gc.entries.erase(gc.entries.begin() + i);
+    } else {
+      ++i;
+    }
+  }
+}
+
+int ensure_ws(Handle &h, size_t bytes) {
+  if (h.ws_bytes >= bytes) return MLSH_SUCCESS;
+  if (h.ws) {
+    cudaStreamSynchronize(h.stream);
+    purge_graphs(h, nullptr, h.ws);
+    cudaFree(h.ws);
+    h.ws = nullptr;
+    h.ws_bytes = 0;
+  }
+  if (cudaMalloc(&h.ws, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return MLSH_ERR_OOM;
+  }
+  h.ws_bytes = bytes;
+  return MLSH_SUCCESS;
+}
+
+int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, void *x,
+                 const mlsh_solver_opts *opts, mlsh_solver_result *res) {
+  if (!hs || !ps || !opts) return MLSH_ERR_INVALID_ARG;
+  Handle &h = hs->h;
+  CsrPlan &p = ps->p;
+  if (p.n_rows != p.n_cols) {
+    if (res) res->status = MLSH_SOLVER_SIZE_ERROR;
+    return MLSH_SOLVER_SIZE_ERROR;
+  }
+  if (opts->precond != MLSH_PRECOND_NONE && opts->precond != MLSH_PRECOND_JACOBI)
+    return MLSH_ERR_INVALID_ARG;
+  const int64_t n = p.n_rows;
+  if (n > 0 && (!b || !x)) return MLSH_ERR_INVALID_ARG;
+  mlsh_solver_result local{};
+  if (!res) res = &local;
+  if (n == 0) {
+    // nothing to solve: ||r|| = 0 < tol unless tol <= 0
+    res->iters = opts->maxiter > 0 ? 1 : 0;
+    res->final_resid = 0.0;
+    res->status = (opts->maxiter > 0 && 0.0 < opts->tol && opts->miniter <= 1)
+                      ? MLSH_SUCCESS
+                      : MLSH_SOLVER_MAXITER;
+    return res->status;
+  }
+  SolveCtx c;
+  c.kind = kind;
+  c.dtype = p.dtype;
+  c.jac = opts->precond == MLSH_PRECOND_JACOBI;
+  c.plan = &p;
+  c.h = &h;
+  c.b = b;
+  c.x = x;
+  c.d = nullptr;
+  c.n = n;
+  c.stride = n;
+  if (c.jac) {
+    int st = plan_inv_diag(p, h.stream, &c.d);
+    if (st != MLSH_SUCCESS) return st;
+  }
+  const int nvec = kind == kCG ? 3 : 8;
+  const size_t esz = (size_t)dtype_size(p.dtype);
+  // round each vector up to 256 bytes so every work vector stays aligned
+  const int64_t n_al = (int64_t)(((size_t)n * esz + 255) / 256 * 256 / esz);
+  int st = ensure_ws(h, (size_t)nvec * (size_t)n_al * esz);
+  if (st != MLSH_SUCCESS) return st;
+  c.ws = h.ws;
+  c.stride = n_al;
+
+  // configuration + fresh iteration state
+  SolverState *hst = h.host_state;
+  std::memset(hst, 0, sizeof(SolverState));
+  hst->tol = opts->tol;
+  hst->maxiter = opts->maxiter;
+  hst->miniter = opts->miniter;
+  hst->status = kRunning;
+  hst->done = 0;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(h.state, hst, sizeof(SolverState), cudaMemcpyHostToDevice,
+                                h.stream));
+  MLSH_CUDA_TRY(cudaMemsetAsync(h.err_flag, 0, sizeof(int), h.stream));
+
+  bool graph_ok = false;
+  if (opts->use_graph) {
+    cudaGraphExec_t ex = nullptr;
+    if (get_graph(c, h, &ex) == MLSH_SUCCESS) {
+      MLSH_CUDA_TRY(cudaGraphLaunch(ex, h.stream));
+      graph_ok = true;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  if (!graph_ok) {
+    StepFn init, iter;
+    pick_steps(c, &init, &iter);
+    CondRef none{0, 0};
+    MLSH_CUDA_TRY(init(c, h.stream, none));
+    const int every = opts->check_every > 0 ? opts->check_every : 16;
+    while (true) {
+      for (int k = 0; k < every; ++k) MLSH_CUDA_TRY(iter(c, h.stream, none));
+      MLSH_CUDA_TRY(cudaMemcpyAsync(hst, h.state, sizeof(SolverState), cudaMemcpyDeviceToHost,
+                                    h.stream));
+      MLSH_CUDA_TRY(cudaStreamSynchronize(h.stream));
+      if (hst->done) break;
+    }
+  }
+  MLSH_CUDA_TRY(cudaMemcpyAsync(hst, h.state, sizeof(SolverState), cudaMemcpyDeviceToHost,
+                                h.stream));
+  int err = 0;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(&h.host_scalars[7], h.err_flag, sizeof(int),
+                                cudaMemcpyDeviceToHost, h.stream));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  std::memcpy(&err, &h.host_scalars[7], sizeof(int));
+  if (err != 0) return err;
+  res->status = hst->status;
+  res->iters = hst->iter;
+  res->final_resid = hst->resid;
+  return res->status;
+}
+
+}  // namespace
+
+void release_solver_graphs(Handle &h) {
+  if (h.graph_cache) {
+    GraphCache &gc = cache_of(h);
+    for (auto &e : gc.entries) destroy_entry(e);
+    delete static_cast<GraphCache *>(h.graph_cache);
+    h.graph_cache = nullptr;
+  }
+  if (h.ws) cudaFree(h.ws);
+  h.ws = nullptr;
+  h.ws_bytes = 0;
+}
+
+void release_plan_extras(CsrPlan &p) {
+  if (p.handle) purge_graphs(*p.handle, &p, nullptr);
+}
+
+void invalidate_plan_extras(CsrPlan &) {}
+
+}  // namespace mlsh
+
+using namespace mlsh;
+
+extern "C" {
+
+int mlsh_solver_opts_default(mlsh_solver_opts *o) {
+  if (!o) return MLSH_ERR_INVALID_ARG;
+  o->tol = 1.0e-8;
+  o->maxiter = INT64_MAX;
+  o->miniter = 0;
+  o->precond = MLSH_PRECOND_JACOBI;
+  o->use_graph = 1;
+  o->check_every = 0;
+  o->reserved = 0;
+  return MLSH_SUCCESS;
+}
+
+int mlsh_cg_solve(mlsh_handle hs, mlsh_csr_plan ps, const void *b, void *x,
+                  const mlsh_solver_opts *opts, mlsh_solver_result *res) {
+  return solve_common(kCG, hs, ps, b, x, opts, res);
+}
+
+int mlsh_bicgstab_solve(mlsh_handle hs, mlsh_csr_plan ps, const void *b, void *x,
+                        const mlsh_solver_opts *opts, mlsh_solver_result *res) {
+  return solve_common(kBiCGSTAB, hs, ps, b, x, opts, res);
+}
+
+}  // extern "C"

@@ -1,0 +1,192 @@
+"""Python harness over the C ABI (used by the tests and the benchmark).
+
+Device memory comes from torch (plumbing only); every computation is a call
+into libmlsh.so through ctypes.  Names follow the reference's vocabulary:
+a ``Crs`` is a device-resident ``matrix::CRS<T>`` after ``send()``, ``matvec``
+is ``blas::matvec``, ``cg_solve``/``bicgstab_solve`` are
+``equation::CG``/``BiCGSTAB`` ``::solve``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+
+try:
+    import torch
+except ImportError:  # pragma: no cover - torch is part of the image
+    torch = None
+
+
+def _dtype_code(np_dtype) -> int:
+    if np.dtype(np_dtype) == np.float64:
+        return _abi.F64
+    if np.dtype(np_dtype) == np.float32:
+        return _abi.F32
+    raise TypeError(f"unsupported dtype {np_dtype}")
+
+
+def _torch_dtype(np_dtype):
+    return torch.float64 if np.dtype(np_dtype) == np.float64 else torch.float32
+
+
+def ptr(t) -> int:
+    return t.data_ptr() if t is not None else 0
+
+
+class Handle:
+    """mlsh_handle bound to the current torch CUDA stream."""
+
+    def __init__(self, stream=None):
+        self.lib = _abi.load()
+        h = C.c_void_p()
+        _abi.check(self.lib.mlsh_create(C.byref(h)), "mlsh_create")
+        self.h = h
+        if stream is None and torch is not None and torch.cuda.is_available():
+            stream = torch.cuda.current_stream().cuda_stream
+        if stream:
+            _abi.check(self.lib.mlsh_set_stream(self.h, C.c_void_p(stream)), "set_stream")
+
+    def close(self):
+        if self.h:
+            self.lib.mlsh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        return _abi.check(self.lib.mlsh_synchronize(self.h), "synchronize")
+
+    # ---------------------------------------------------------- vector BLAS
+    def dot(self, x, y) -> float:
+        out = C.c_double()
+        _abi.check(self.lib.mlsh_dot(self.h, _dtype_code(_np(x)), x.numel(), ptr(x), ptr(y),
+                                     C.byref(out)), "dot")
+        return out.value
+
+    def nrm2(self, x) -> float:
+        out = C.c_double()
+        _abi.check(self.lib.mlsh_nrm2(self.h, _dtype_code(_np(x)), x.numel(), ptr(x),
+                                      C.byref(out)), "nrm2")
+        return out.value
+
+    def axpy(self, alpha, x, y):
+        _abi.check(self.lib.mlsh_axpy(self.h, _dtype_code(_np(x)), x.numel(), alpha, ptr(x),
+                                      ptr(y)), "axpy")
+
+    def xpay(self, alpha, x, y):
+        _abi.check(self.lib.mlsh_xpay(self.h, _dtype_code(_np(x)), x.numel(), alpha, ptr(x),
+                                      ptr(y)), "xpay")
+
+    def axpyz(self, alpha, x, y, z):
+        _abi.check(self.lib.mlsh_axpyz(self.h, _dtype_code(_np(x)), x.numel(), alpha, ptr(x),
+                                       ptr(y), ptr(z)), "axpyz")
+
+    def copy(self, x, y):
+        _abi.check(self.lib.mlsh_copy(self.h, _dtype_code(_np(x)), x.numel(), ptr(x), ptr(y)),
+                   "copy")
+
+    def vsub(self, a, b, y):
+        _abi.check(self.lib.mlsh_vsub(self.h, _dtype_code(_np(a)), a.numel(), ptr(a), ptr(b),
+                                      ptr(y)), "vsub")
+
+    def vmul(self, a, b, y):
+        _abi.check(self.lib.mlsh_vmul(self.h, _dtype_code(_np(a)), a.numel(), ptr(a), ptr(b),
+                                      ptr(y)), "vmul")
+
+    def vreciprocal(self, a, y):
+        _abi.check(self.lib.mlsh_vreciprocal(self.h, _dtype_code(_np(a)), a.numel(), ptr(a),
+                                             ptr(y)), "vreciprocal")
+
+
+def _np(t):
+    return np.float64 if t.dtype == torch.float64 else np.float32
+
+
+class Crs:
+    """A CRS matrix resident on the device, with its SpMV plan."""
+
+    def __init__(self, handle: Handle, n_rows, n_cols, row_ptr, col_ind, val,
+                 validate=True):
+        self.handle = handle
+        self.lib = handle.lib
+        self.n_rows, self.n_cols = int(n_rows), int(n_cols)
+        rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        self.dtype = np.dtype(val.dtype)
+        self.nnz = int(rp[-1]) if len(rp) else 0
+        dev = torch.device("cuda")
+        self.d_rp = torch.from_numpy(rp).to(dev)
+        self.d_ci = torch.from_numpy(np.ascontiguousarray(col_ind, dtype=np.int32)).to(dev)
+        self.d_val = torch.from_numpy(np.ascontiguousarray(val)).to(dev)
+        plan = C.c_void_p()
+        _abi.check(self.lib.mlsh_csr_plan_create(
+            handle.h, self.n_rows, self.n_cols, self.nnz, ptr(self.d_rp), ptr(self.d_ci),
+            ptr(self.d_val), _dtype_code(self.dtype), rp.ctypes.data_as(C.c_void_p),
+            1 if validate else 0, C.byref(plan)), "csr_plan_create")
+        self.plan = plan
+
+    def close(self):
+        if self.plan:
+            self.lib.mlsh_csr_plan_destroy(self.plan)
+            self.plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        nt, nl, b = C.c_int(), C.c_int(), C.c_int64()
+        _abi.check(self.lib.mlsh_csr_plan_info(self.plan, C.byref(nt), C.byref(nl),
+                                               C.byref(b)), "plan_info")
+        return {"n_tiles": nt.value, "n_long_rows": nl.value, "spmv_bytes": b.value}
+
+    def matvec(self, x, y, alpha=1.0, beta=0.0):
+        _abi.check(self.lib.mlsh_spmv(self.handle.h, self.plan, alpha, ptr(x), beta, ptr(y)),
+                   "spmv")
+
+    def diag(self, out):
+        _abi.check(self.lib.mlsh_csr_diag(self.handle.h, self.plan, ptr(out)), "diag")
+
+
+@dataclass
+class SolveResult:
+    status: int
+    iters: int
+    resid: float
+
+
+def _opts(tol, maxiter, miniter, precond, use_graph, check_every):
+    o = _abi.SolverOpts()
+    o.tol, o.maxiter, o.miniter = tol, maxiter, miniter
+    o.precond = precond
+    o.use_graph = 1 if use_graph else 0
+    o.check_every = check_every
+    return o
+
+
+def _solve(fn, A: Crs, b, x, tol, maxiter, miniter=0, precond=_abi.PRECOND_JACOBI,
+           use_graph=True, check_every=0):
+    o = _opts(tol, maxiter, miniter, precond, use_graph, check_every)
+    r = _abi.SolverResult()
+    st = fn(A.handle.h, A.plan, ptr(b), ptr(x), C.byref(o), C.byref(r))
+    if st not in (_abi.SUCCESS, _abi.SOLVER_MAXITER, _abi.SOLVER_BREAKDOWN,
+                  _abi.SOLVER_RESIDUAL_NAN, _abi.SOLVER_SIZE_ERROR):
+        raise _abi.MlshError(st, "solve")
+    return SolveResult(st, int(r.iters), float(r.final_resid))
+
+
+def cg_solve(A: Crs, b, x, tol, maxiter, **kw) -> SolveResult:
+    return _solve(A.lib.mlsh_cg_solve, A, b, x, tol, maxiter, **kw)
+
+
+def bicgstab_solve(A: Crs, b, x, tol, maxiter, **kw) -> SolveResult:
+    return _solve(A.lib.mlsh_bicgstab_solve, A, b, x, tol, maxiter, **kw)

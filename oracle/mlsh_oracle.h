@@ -1,0 +1,56 @@
+/*
+ * CPU restatement of the reference's sparse iterative-solve hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA library.  Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU baseline leg may load it.  The
+ * product never links, loads or calls it.
+ *
+ * Pinned against the reference itself: tests/test_oracle.py compares every
+ * routine here with the reference CPU library built from the reference
+ * sources (oracle/_ref) and with the committed golden fixtures made from it
+ * (tests/golden/make_golden.py).
+ *
+ * Return codes follow include/monolish/common/monolish_common.hpp:16-21 of
+ * the reference: 0 success, -2 maxiter, -3 breakdown, -4 residual NaN.
+ */
+#ifndef MLSH_ORACLE_H
+#define MLSH_ORACLE_H
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void oracle_spmv_d(int n, const int *rp, const int *ci, const double *v,
+                   const double *x, double *y);
+void oracle_spmv_s(int n, const int *rp, const int *ci, const float *v,
+                   const float *x, float *y);
+/* y = alpha*A*x + beta*y (the alpha/beta overload of blas::matvec). */
+void oracle_spmv_ab_d(int n, const int *rp, const int *ci, const double *v,
+                      double alpha, const double *x, double beta, double *y);
+
+double oracle_dot_d(long n, const double *x, const double *y);
+double oracle_nrm2_d(long n, const double *x);
+double oracle_dot_s(long n, const float *x, const float *y);
+
+int oracle_cg_d(int n, const int *rp, const int *ci, const double *v,
+                const double *b, double *x, double tol_abs, long maxiter,
+                long miniter, int precond, long *iters, double *resid);
+int oracle_cg_s(int n, const int *rp, const int *ci, const float *v,
+                const float *b, float *x, double tol_abs, long maxiter,
+                long miniter, int precond, long *iters, double *resid);
+int oracle_bicgstab_d(int n, const int *rp, const int *ci, const double *v,
+                      const double *b, double *x, double tol_abs, long maxiter,
+                      long miniter, int precond, long *iters, double *resid);
+int oracle_bicgstab_s(int n, const int *rp, const int *ci, const float *v,
+                      const float *b, float *x, double tol_abs, long maxiter,
+                      long miniter, int precond, long *iters, double *resid);
+
+/* ||b - A x||_2 / ||b||_2 in double. */
+double oracle_true_relres_d(int n, const int *rp, const int *ci,
+                            const double *v, const double *b, const double *x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

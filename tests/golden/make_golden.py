@@ -1,0 +1,115 @@
+"""Regenerate the golden fixtures in this directory from the reference.
+
+The fixtures pin the oracle (and through it the CUDA path) to the
+reference's own CPU implementation: each case runs the reference monolish
+CPU library built from the reference sources (oracle/_ref, see
+oracle/Makefile) through its public API -- CRS from raw arrays,
+blas::matvec/dot/nrm2/axpy/xpay/axpyz, equation::CG / BiCGSTAB::solve with
+Jacobi or none -- on seeded inputs from monolish_b200/workloads.py, and
+stores inputs and outputs.
+
+    python tests/golden/make_golden.py      # needs oracle/_ref built
+
+Cases (all small, so the CPU restatement replays them in seconds):
+  tridiag3     the reference's own test matrix test/test.mtx (3x3
+               tridiagonal 2,-1); b = A*ones, x0 ~ U(0,1) from
+               mt19937(1234) as in test/test_utils.hpp:21; CG and
+               BiCGSTAB, none/Jacobi, double (tol 1e-8) and float (1e-4).
+  poisson16    2D 5-point 16x16, x_true ~ U[-1,1] seed 0, x0 = 0,
+               tol = 1e-10*||b||, Jacobi CG and BiCGSTAB.
+  poisson128   the 128x128 Jacobi-CG workload (n = 16,384).
+  convdiff10   3D upwind convection-diffusion 10^3, Peclet 10, Jacobi
+               BiCGSTAB, tol 1e-10*||b||.
+  zipf_spmv    SpMV on an 8,000-row Zipf(2) matrix (lengths up to 8,000;
+               four rows exceed one 1,792-nonzero SpMV tile), double and
+               float.
+  blas1        dot/nrm2/axpy/xpay/axpyz on n = 1,000.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from monolish_b200 import workloads as W  # noqa: E402
+
+
+def tridiag3():
+    rp = np.array([0, 2, 5, 7], np.int32)
+    ci = np.array([0, 1, 0, 1, 2, 1, 2], np.int32)
+    v = np.array([2, -1, -1, 2, -1, -1, 2], np.float64)
+    return 3, rp, ci, v
+
+
+def main():
+    ref = oracle.Reference()
+    out = {}
+
+    # ---- tridiag3 (reference test/test.mtx) ----
+    n, rp, ci, v = tridiag3()
+    ones = np.ones(n)
+    b = ref.spmv(rp, ci, v, ones)[0]
+    x0 = ref.random_vector(n, 0.0, 1.0, 1234)
+    case = dict(rp=rp, ci=ci, v=v, b=b, x0=x0)
+    for solver in ("cg", "bicgstab"):
+        for pre in (0, 1):
+            st, it, res, x, _ = getattr(ref, solver)(rp, ci, v, b, x0, 1e-8, 10000, precond=pre)
+            case[f"{solver}_p{pre}_d"] = np.array([st, it, res])
+            case[f"{solver}_p{pre}_d_x"] = x
+            vf, bf, x0f = v.astype(np.float32), b.astype(np.float32), x0.astype(np.float32)
+            st, it, res, x, _ = getattr(ref, solver)(rp, ci, vf, bf, x0f, 1e-4, 10000,
+                                                     precond=pre)
+            case[f"{solver}_p{pre}_s"] = np.array([st, it, res])
+            case[f"{solver}_p{pre}_s_x"] = x
+    out["tridiag3"] = case
+
+    # ---- Poisson solves ----
+    for name, m in (("poisson16", 16), ("poisson128", 128)):
+        n, rp, ci, v = W.poisson2d(m)
+        xt = W.uniform_mt(n, -1.0, 1.0, 0)
+        b = ref.spmv(rp, ci, v, xt)[0]
+        tol = 1e-10 * np.linalg.norm(b)
+        case = dict(rp=rp, ci=ci, v=v, b=b, tol=np.array(tol))
+        solvers = ("cg", "bicgstab") if m == 16 else ("cg",)
+        for solver in solvers:
+            st, it, res, x, _ = getattr(ref, solver)(rp, ci, v, b, np.zeros(n), tol, 2000,
+                                                     precond=1)
+            case[f"{solver}"] = np.array([st, it, res])
+            case[f"{solver}_x"] = x
+        out[name] = case
+
+    # ---- convection-diffusion BiCGSTAB ----
+    n, rp, ci, v = W.convdiff3d(10, peclet=10.0)
+    xt = W.uniform_mt(n, -1.0, 1.0, 2)
+    b = ref.spmv(rp, ci, v, xt)[0]
+    tol = 1e-10 * np.linalg.norm(b)
+    st, it, res, x, _ = ref.bicgstab(rp, ci, v, b, np.zeros(n), tol, 2000, precond=1)
+    out["convdiff10"] = dict(rp=rp, ci=ci, v=v, b=b, tol=np.array(tol),
+                             bicgstab=np.array([st, it, res]), bicgstab_x=x)
+
+    # ---- Zipf SpMV (long rows split across tiles) ----
+    n, rp, ci, v = W.zipf(8000, seed=7, maxlen=8000)
+    x = W.uniform_mt(n, -1.0, 1.0, 11)
+    y = ref.spmv(rp, ci, v, x)[0]
+    ys = ref.spmv(rp, ci, v.astype(np.float32), x.astype(np.float32))[0]
+    out["zipf_spmv"] = dict(rp=rp, ci=ci, v=v, x=x, y=y, y_s=ys)
+
+    # ---- vector BLAS ----
+    a = W.uniform_mt(1000, -1.0, 1.0, 21)
+    c = W.uniform_mt(1000, -1.0, 1.0, 22)
+    out["blas1"] = dict(x=a, y=c, dot=np.array(ref.dot(a, c)), nrm2=np.array(ref.nrm2(a)),
+                        axpy=ref.axpy(0.75, a, c), xpay=ref.xpay(0.75, a, c),
+                        axpyz=ref.axpyz(0.75, a, c))
+
+    for name, case in out.items():
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **case)
+        print("wrote", path, os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()
