@@ -64,6 +64,8 @@ def env_rank():
 
 
 def describe(wl):
+    if wl.get("size"):
+        wl = dict(wl, **({"n": wl["size"]} if wl["matrix"] == "zipf" else {"m": wl["size"]}))
     if wl["matrix"] == "poisson3d":
         return f"3D 7-point Laplacian {wl['m']}^3 CRS<{'double' if wl['dtype'] == 'f64' else 'float'}>"
     if wl["matrix"] == "zipf":
@@ -79,6 +81,8 @@ def describe(wl):
 
 def make_matrix(wl):
     from monolish_b200 import workloads as W
+    if wl.get("size"):
+        wl = dict(wl, **({"n": wl["size"]} if wl["matrix"] == "zipf" else {"m": wl["size"]}))
     if wl["matrix"] == "poisson3d":
         n, rp, ci, v = W.poisson3d(wl["m"])
         x = W.uniform_fast(n, -1.0, 1.0, 1)
@@ -226,13 +230,14 @@ def run_spmv(args, wl, rank, world, local):
         launch()
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
-    clocks.start()
-    # keep the sampler running over a warm-up soak so short timed regions
-    # still have clock samples of the same work around them
-    soak_end = time.time() + 1.0
-    while time.time() < soak_end:
-        launch()
-        torch.cuda.synchronize()
+    if not args.quick:
+        clocks.start()
+        # keep the sampler running over a warm-up soak so short timed regions
+        # still have clock samples of the same work around them
+        soak_end = time.time() + 1.0
+        while time.time() < soak_end:
+            launch()
+            torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -252,26 +257,30 @@ def run_spmv(args, wl, rank, world, local):
     # ---- end to end through the C ABI with host buffers
     hx = torch.from_numpy(x).pin_memory()
     hy = torch.empty(n, dtype=dx.dtype).pin_memory()
-    for _ in range(2):
-        dx.copy_(hx, non_blocking=True)
-        launch()
-        hy.copy_(dy, non_blocking=True)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e2e_steps = max(1, min(args.steps, 50))
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        dx.copy_(hx, non_blocking=True)
-        launch()
-        hy.copy_(dy, non_blocking=True)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        dist.barrier()
+    e2e_steps = 0 if args.quick else max(1, min(args.steps, 50))
+    e2e_ms = 1.0
+    if e2e_steps:
+        for _ in range(2):
+            dx.copy_(hx, non_blocking=True)
+            launch()
+            hy.copy_(dy, non_blocking=True)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            dx.copy_(hx, non_blocking=True)
+            launch()
+            hy.copy_(dy, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+        if world > 1:
+            dist.barrier()
+    else:
+        hy.copy_(dy)
 
     # correctness spot check against the oracle on a sample of rows
     y = hy.numpy()
@@ -490,11 +499,19 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="spmv_poisson3d_f64")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--size", type=int, default=0,
+                    help="override the grid edge (n for zipf); for small profiling cases")
+    ap.add_argument("--quick", action="store_true",
+                    help="timed steps only: no clock soak, no e2e, no CPU leg (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.quick:
+        args.no_cpu = True
     rank, world, local = env_rank()
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
+    if args.size:
+        wl["size"] = args.size
     if args.impl == "reference":
         out = run_reference(args, wl, rank, world)
         if out is not None:

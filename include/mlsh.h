@@ -77,6 +77,23 @@ int mlsh_set_stream(mlsh_handle handle, void *stream);
 int mlsh_get_stream(mlsh_handle handle, void **stream);
 int mlsh_synchronize(mlsh_handle handle);
 
+/* ---------------------------------------------------- device memory ----- */
+/* Device residency for hosts that include no CUDA headers: these back the
+ * send() / recv() / nonfree_recv() / device_free() of vector and CRS
+ * (src/utils/system/gpu_comm.cpp:8-183, where the reference maps host
+ * arrays with OpenMP target data directives).  Allocations are 256-byte
+ * aligned.  The copies are synchronous with respect to the host and ordered
+ * on the handle's stream. */
+int mlsh_device_alloc(size_t bytes, void **d_ptr);
+int mlsh_device_free(void *d_ptr);
+int mlsh_memcpy_h2d(mlsh_handle handle, void *d_dst, const void *h_src,
+                    size_t bytes);
+int mlsh_memcpy_d2h(mlsh_handle handle, void *h_dst, const void *d_src,
+                    size_t bytes);
+/* Device-to-device copy, asynchronous on the handle's stream. */
+int mlsh_memcpy_d2d(mlsh_handle handle, void *d_dst, const void *d_src,
+                    size_t bytes);
+
 /* --------------------------------------------------------------- CRS ---- */
 /* Build an SpMV plan over a device-resident CRS matrix (0-based row_ptr
  * [n_rows+1], col_ind [nnz], val [nnz] of `dtype`), as matrix::CRS<T>
@@ -162,6 +179,9 @@ typedef struct {
                        with a host check every `check_every` iterations */
   int check_every;  /* eager mode only; <= 0 picks a default */
   int reserved;
+  double *history;     /* optional host buffer: ||r|| after each iteration
+                          (solver::set_print_rhistory, cg.cpp:62-65) */
+  int64_t history_len; /* capacity of `history` in doubles */
 } mlsh_solver_opts;
 
 typedef struct {

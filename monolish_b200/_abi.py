@@ -37,7 +37,8 @@ f64 = C.c_double
 
 class SolverOpts(C.Structure):
     _fields_ = [("tol", f64), ("maxiter", i64), ("miniter", i64), ("precond", i32),
-                ("use_graph", i32), ("check_every", i32), ("reserved", i32)]
+                ("use_graph", i32), ("check_every", i32), ("reserved", i32),
+                ("history", C.POINTER(f64)), ("history_len", i64)]
 
 
 class SolverResult(C.Structure):
@@ -54,6 +55,11 @@ SIGNATURES = {
     "mlsh_set_stream": (i32, [vp, vp]),
     "mlsh_get_stream": (i32, [vp, C.POINTER(vp)]),
     "mlsh_synchronize": (i32, [vp]),
+    "mlsh_device_alloc": (i32, [C.c_size_t, C.POINTER(vp)]),
+    "mlsh_device_free": (i32, [vp]),
+    "mlsh_memcpy_h2d": (i32, [vp, vp, vp, C.c_size_t]),
+    "mlsh_memcpy_d2h": (i32, [vp, vp, vp, C.c_size_t]),
+    "mlsh_memcpy_d2d": (i32, [vp, vp, vp, C.c_size_t]),
     "mlsh_csr_plan_create": (i32, [vp, i32, i32, i32, vp, vp, vp, i32, vp, i32, C.POINTER(vp)]),
     "mlsh_csr_plan_destroy": (i32, [vp]),
     "mlsh_csr_plan_values_changed": (i32, [vp]),

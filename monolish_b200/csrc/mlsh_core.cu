@@ -301,6 +301,49 @@ int mlsh_synchronize(mlsh_handle hs) {
   return err != 0 ? err : MLSH_SUCCESS;
 }
 
+// --------------------------------------------------------- device memory --
+int mlsh_device_alloc(size_t bytes, void **d_ptr) {
+  if (!d_ptr) return MLSH_ERR_INVALID_ARG;
+  *d_ptr = nullptr;
+  if (bytes == 0) return MLSH_SUCCESS;
+  const cudaError_t e = cudaMalloc(d_ptr, bytes);
+  if (e != cudaSuccess) {
+    set_last_error("cudaMalloc", e);
+    cudaGetLastError();
+    *d_ptr = nullptr;
+    return e == cudaErrorMemoryAllocation ? MLSH_ERR_OOM : MLSH_ERR_CUDA;
+  }
+  return MLSH_SUCCESS;
+}
+
+int mlsh_device_free(void *d_ptr) {
+  if (d_ptr) MLSH_CUDA_TRY(cudaFree(d_ptr));
+  return MLSH_SUCCESS;
+}
+
+int mlsh_memcpy_h2d(mlsh_handle hs, void *d, const void *h, size_t bytes) {
+  if (!hs || ((!d || !h) && bytes)) return MLSH_ERR_INVALID_ARG;
+  if (!bytes) return MLSH_SUCCESS;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, hs->h.stream));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(hs->h.stream));
+  return MLSH_SUCCESS;
+}
+
+int mlsh_memcpy_d2h(mlsh_handle hs, void *h, const void *d, size_t bytes) {
+  if (!hs || ((!d || !h) && bytes)) return MLSH_ERR_INVALID_ARG;
+  if (!bytes) return MLSH_SUCCESS;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, hs->h.stream));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(hs->h.stream));
+  return MLSH_SUCCESS;
+}
+
+int mlsh_memcpy_d2d(mlsh_handle hs, void *dst, const void *src, size_t bytes) {
+  if (!hs || ((!dst || !src) && bytes)) return MLSH_ERR_INVALID_ARG;
+  if (!bytes) return MLSH_SUCCESS;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, hs->h.stream));
+  return MLSH_SUCCESS;
+}
+
 // ------------------------------------------------------------------ plan --
 int mlsh_csr_plan_create(mlsh_handle hs, int n_rows, int n_cols, int nnz,
                          const int *d_row_ptr, const int *d_col_ind,

@@ -79,6 +79,8 @@ struct SolverState {
   int done;        // 1 once status is final
   int error;       // MLSH_ERR_TIMEOUT if a device wait gave up
   int pad1;
+  double *hist;    // optional residual history (device), hist_cap entries
+  long long hist_cap;
 };
 
 // ------------------------------------------------------------- objects ---
@@ -98,6 +100,8 @@ struct Handle {
   void *ws = nullptr;                 // solver work vectors
   size_t ws_bytes = 0;
   void *graph_cache = nullptr;        // instantiated solver graphs
+  double *hist = nullptr;             // residual history buffer (device)
+  long long hist_cap = 0;
 };
 
 struct CsrPlan {

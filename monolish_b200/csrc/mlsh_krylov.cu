@@ -20,6 +20,7 @@
 // condition, so a whole solve is one graph launch and one final read.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -52,6 +53,7 @@ __device__ void finish_iteration(SolverState *st, const CondRef &cond) {
   st->iter = it;
   const double res = resid_of<T>(st->rr);
   st->resid = res;
+  if (st->hist != nullptr && it <= st->hist_cap) st->hist[it - 1] = res;
   if (res < st->tol && st->miniter <= it) {
     st->status = MLSH_SUCCESS;
     st->done = 1;
@@ -625,6 +627,22 @@ int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, voi
   hst->miniter = opts->miniter;
   hst->status = kRunning;
   hst->done = 0;
+  const bool want_hist = opts->history != nullptr && opts->history_len > 0;
+  if (want_hist) {
+    if (h.hist_cap < opts->history_len) {
+      if (h.hist) cudaFree(h.hist);
+      h.hist = nullptr;
+      h.hist_cap = 0;
+      if (cudaMalloc(&h.hist, sizeof(double) * (size_t)opts->history_len) != cudaSuccess) {
+        cudaGetLastError();
+        h.hist = nullptr;
+        return MLSH_ERR_OOM;
+      }
+      h.hist_cap = opts->history_len;
+    }
+    hst->hist = h.hist;
+    hst->hist_cap = opts->history_len;
+  }
   MLSH_CUDA_TRY(cudaMemcpyAsync(h.state, hst, sizeof(SolverState), cudaMemcpyHostToDevice,
                                 h.stream));
   MLSH_CUDA_TRY(cudaMemsetAsync(h.err_flag, 0, sizeof(int), h.stream));
@@ -664,6 +682,12 @@ int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, voi
   res->status = hst->status;
   res->iters = hst->iter;
   res->final_resid = hst->resid;
+  if (want_hist) {
+    const int64_t k = std::min<int64_t>(hst->iter, opts->history_len);
+    if (k > 0)
+      MLSH_CUDA_TRY(cudaMemcpy(opts->history, h.hist, sizeof(double) * (size_t)k,
+                               cudaMemcpyDeviceToHost));
+  }
   return res->status;
 }
 
@@ -679,6 +703,9 @@ void release_solver_graphs(Handle &h) {
   if (h.ws) cudaFree(h.ws);
   h.ws = nullptr;
   h.ws_bytes = 0;
+  if (h.hist) cudaFree(h.hist);
+  h.hist = nullptr;
+  h.hist_cap = 0;
 }
 
 void release_plan_extras(CsrPlan &p) {
@@ -702,6 +729,8 @@ int mlsh_solver_opts_default(mlsh_solver_opts *o) {
   o->use_graph = 1;
   o->check_every = 0;
   o->reserved = 0;
+  o->history = nullptr;
+  o->history_len = 0;
   return MLSH_SUCCESS;
 }
 

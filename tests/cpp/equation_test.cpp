@@ -1,0 +1,83 @@
+// Solver test written against the monolish API (CRS + vector + send +
+// equation::CG/BiCGSTAB with Jacobi/none), built against the B200 drop-in
+// headers.  It follows the reference's own solver test flow
+// (test/equation/iterative/equation_kernel.hpp): read a MatrixMarket matrix,
+// b = A*ones, x0 = seeded U(0,1), solve, check x against ones at tol*10.
+//
+// usage: equation_test <matrix.mtx>
+#include <cmath>
+#include <cstdio>
+#include <iostream>
+#include <random>
+
+#include "monolish_blas.hpp"
+#include "monolish_equation.hpp"
+
+namespace {
+
+std::mt19937 engine(1234);
+
+template <typename T> bool close_to_ones(const monolish::vector<T> &x, double tol) {
+  for (size_t i = 0; i < x.size(); ++i) {
+    const double d = std::fabs((double)x.data()[i] - 1.0);
+    if (d > tol && d > tol * 1.0) {
+      std::cout << "  x[" << i << "] = " << x.data()[i] << std::endl;
+      return false;
+    }
+  }
+  return true;
+}
+
+template <typename T, typename SOLVER, typename PRECOND>
+bool run(const char *file, double tol, const char *label) {
+  monolish::matrix::COO<T> coo(file);
+  monolish::matrix::CRS<T> A(coo);
+  monolish::vector<T> ones(A.get_row(), 1.0);
+  monolish::vector<T> b(A.get_row(), 0.0);
+  monolish::vector<T> x(A.get_row(), 0.0, 1.0, engine());
+  monolish::util::send(A, x, b, ones);
+  monolish::blas::matvec(A, ones, b);
+
+  SOLVER solver;
+  solver.set_tol(tol);
+  solver.set_lib(0);
+  solver.set_miniter(0);
+  solver.set_maxiter(10000);
+  PRECOND precond;
+  solver.set_create_precond(precond);
+  solver.set_apply_precond(precond);
+  const int st = solver.solve(A, x, b);
+  x.recv();
+  std::cout << label << ": status " << st << ", iter " << solver.get_final_iter()
+            << ", resid " << solver.get_final_residual() << std::endl;
+  if (st != MONOLISH_SOLVER_SUCCESS) return false;
+  return close_to_ones(x, tol * 10);
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  if (argc != 2) {
+    std::cerr << "usage: equation_test <matrix.mtx>" << std::endl;
+    return 2;
+  }
+  using namespace monolish;
+  const char *f = argv[1];
+  using CD = matrix::CRS<double>;
+  using CF = matrix::CRS<float>;
+  bool ok = true;
+  ok &= run<double, equation::CG<CD, double>, equation::none<CD, double>>(f, 1e-8, "CG none d");
+  ok &= run<float, equation::CG<CF, float>, equation::none<CF, float>>(f, 1e-4, "CG none f");
+  ok &= run<double, equation::CG<CD, double>, equation::Jacobi<CD, double>>(f, 1e-8, "CG Jacobi d");
+  ok &= run<float, equation::CG<CF, float>, equation::Jacobi<CF, float>>(f, 1e-4, "CG Jacobi f");
+  ok &= run<double, equation::BiCGSTAB<CD, double>, equation::none<CD, double>>(
+      f, 1e-8, "BiCGSTAB none d");
+  ok &= run<float, equation::BiCGSTAB<CF, float>, equation::none<CF, float>>(
+      f, 1e-4, "BiCGSTAB none f");
+  ok &= run<double, equation::BiCGSTAB<CD, double>, equation::Jacobi<CD, double>>(
+      f, 1e-8, "BiCGSTAB Jacobi d");
+  ok &= run<float, equation::BiCGSTAB<CF, float>, equation::Jacobi<CF, float>>(
+      f, 1e-4, "BiCGSTAB Jacobi f");
+  std::cout << (ok ? "PASS" : "FAIL") << std::endl;
+  return ok ? 0 : 1;
+}
