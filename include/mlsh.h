@@ -142,6 +142,21 @@ int mlsh_dot_device(mlsh_handle handle, int dtype, int64_t n, const void *d_x,
                     const void *d_y, double *d_result);
 int mlsh_nrm2_device(mlsh_handle handle, int dtype, int64_t n,
                      const void *d_x, double *d_result);
+/* The device dot product above for callers that cannot allocate device
+ * memory (a framework that owns the device memory through its own pool, a
+ * latency-critical loop that cannot take cudaMalloc's implicit
+ * synchronisation): no handle, nothing allocated.  This entry point has no
+ * counterpart in the reference.  Same result as mlsh_dot_device.  Its
+ * scratch is a static 16,640-byte device array (an arrival counter plus
+ * partial sums for at most 2048 CTAs) that every GPU loading the library
+ * holds until exit; a device needing more CTAs than that is rejected with
+ * MLSH_ERR_INVALID_ARG (see mlsh_last_error).  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress) and should come before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU
+ * race; order them on one stream.  Runs on `stream` on the current device;
+ * asynchronous. */
+int mlsh_dot_noalloc(int dtype, int64_t n, const void *d_x, const void *d_y,
+                     double *d_result, void *stream);
 /* y = alpha*x + y          (src/blas/vector/axpy.hpp:7-34) */
 int mlsh_axpy(mlsh_handle handle, int dtype, int64_t n, double alpha,
               const void *d_x, void *d_y);

@@ -70,6 +70,7 @@ SIGNATURES = {
     "mlsh_nrm2": (i32, [vp, i32, i64, vp, C.POINTER(f64)]),
     "mlsh_dot_device": (i32, [vp, i32, i64, vp, vp, vp]),
     "mlsh_nrm2_device": (i32, [vp, i32, i64, vp, vp]),
+    "mlsh_dot_noalloc": (i32, [i32, i64, vp, vp, vp, vp]),
     "mlsh_axpy": (i32, [vp, i32, i64, f64, vp, vp]),
     "mlsh_xpay": (i32, [vp, i32, i64, f64, vp, vp]),
     "mlsh_axpyz": (i32, [vp, i32, i64, f64, vp, vp, vp]),

@@ -21,6 +21,10 @@ void set_last_error(const char *where, cudaError_t e) {
                 cudaGetErrorString(e));
 }
 
+void set_last_error_text(const char *text) {
+  std::snprintf(g_last_error, sizeof(g_last_error), "%s", text);
+}
+
 // --------------------------------------------------------------- tiling --
 void build_tiles(const int *rp, int n_rows, std::vector<Tile> &tiles,
                  std::vector<LongRow> &longs, int &n_chunks) {
