@@ -226,6 +226,12 @@ def run_spmv(args, wl, rank, world, local):
         if st != 0:
             raise _abi.MlshError(st, "spmv")
 
+    # setup (untimed): pick the SpMV kernel variant for this matrix
+    if args.variant >= 0:
+        A.set_variant(args.variant)
+        variant = args.variant
+    else:
+        variant, _ = A.autotune(dx, dy)
     for _ in range(args.warmup):
         launch()
     torch.cuda.synchronize()
@@ -320,7 +326,8 @@ def run_spmv(args, wl, rank, world, local):
             "config": {"workload": describe(wl), "n": n, "nnz": nnz,
                        "bytes_per_step": B, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (no flush needed)",
-                       "n_tiles": info["n_tiles"], "n_long_rows": info["n_long_rows"]},
+                       "n_tiles": info["n_tiles"], "n_long_rows": info["n_long_rows"],
+                       "spmv_variant": variant},
             "e2e": {"value": round(e2e_value, 2), "unit": "GB/s",
                     "h2d_bytes_per_step": n * vsz, "d2h_bytes_per_step": n * vsz,
                     "steps": e2e_steps},
@@ -501,6 +508,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--size", type=int, default=0,
                     help="override the grid edge (n for zipf); for small profiling cases")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="SpMV kernel variant (default: autotuned per matrix)")
     ap.add_argument("--quick", action="store_true",
                     help="timed steps only: no clock soak, no e2e, no CPU leg (profiling)")
     args = ap.parse_args()

@@ -119,6 +119,18 @@ int mlsh_csr_plan_values_changed(mlsh_csr_plan plan);
 int mlsh_csr_plan_info(mlsh_csr_plan plan, int *n_tiles, int *n_long_rows,
                        int64_t *spmv_bytes);
 
+/* SpMV kernel variants (shared-memory pipeline depth x CTAs per SM).  A plan
+ * starts with a default; mlsh_csr_plan_autotune times every variant on the
+ * plan's own matrix (x: n_cols elements, y: n_rows scratch elements, both
+ * of the plan's dtype) and keeps the fastest for all later SpMVs and
+ * solves.  Synchronous. */
+int mlsh_csr_plan_autotune(mlsh_handle handle, mlsh_csr_plan plan,
+                           const void *d_x, void *d_y, int *chosen_variant,
+                           double *best_seconds);
+int mlsh_csr_plan_set_variant(mlsh_csr_plan plan, int variant);
+int mlsh_csr_plan_get_variant(mlsh_csr_plan plan, int *variant,
+                              int *n_variants);
+
 /* y = alpha*A*x + beta*y.  Replaces blas::matvec(A,x,y) and the
  * matvec(a,A,x,b,y) overload (src/blas/matrix/matvec/matvec_blas.cpp:3849-3877,
  * core src/blas/matrix/matvec/crs_matvec.hpp:8-114).  beta == 0 does not

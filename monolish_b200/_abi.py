@@ -64,6 +64,9 @@ SIGNATURES = {
     "mlsh_csr_plan_destroy": (i32, [vp]),
     "mlsh_csr_plan_values_changed": (i32, [vp]),
     "mlsh_csr_plan_info": (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i64)]),
+    "mlsh_csr_plan_autotune": (i32, [vp, vp, vp, vp, C.POINTER(i32), C.POINTER(f64)]),
+    "mlsh_csr_plan_set_variant": (i32, [vp, i32]),
+    "mlsh_csr_plan_get_variant": (i32, [vp, C.POINTER(i32), C.POINTER(i32)]),
     "mlsh_spmv": (i32, [vp, vp, f64, vp, f64, vp]),
     "mlsh_csr_diag": (i32, [vp, vp, vp]),
     "mlsh_dot": (i32, [vp, i32, i64, vp, vp, C.POINTER(f64)]),

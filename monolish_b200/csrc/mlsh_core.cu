@@ -59,16 +59,36 @@ void build_tiles(const int *rp, int n_rows, std::vector<Tile> &tiles,
   }
 }
 
-template <typename VT, int M0, int M1>
-static int set_spmv_smem() {
-  const cudaError_t e = cudaFuncSetAttribute(
-      spmv_tiles_kernel<VT, VT, M0, M1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-      SpmvSmem<VT>::kBytes);
+// Every (type, dot modes, variant) instantiation of the SpMV kernel.
+template <typename VT, int M0, int M1, int V>
+static constexpr auto spmv_kernel_ptr() {
+  return spmv_tiles_kernel<VT, VT, M0, M1, kSpmvVariants[V].stages, kSpmvVariants[V].min_blocks>;
+}
+
+template <typename VT, int V>
+static constexpr int spmv_smem_bytes() {
+  return SpmvSmem<VT, kSpmvVariants[V].stages>::kBytes;
+}
+
+template <typename VT, int M0, int M1, int V>
+static int set_spmv_smem_one() {
+  const cudaError_t e = cudaFuncSetAttribute(spmv_kernel_ptr<VT, M0, M1, V>(),
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             spmv_smem_bytes<VT, V>());
   if (e != cudaSuccess) {
     set_last_error("cudaFuncSetAttribute(spmv)", e);
     return MLSH_ERR_CUDA;
   }
   return MLSH_SUCCESS;
+}
+
+template <typename VT, int M0, int M1>
+static int set_spmv_smem() {
+  int s = set_spmv_smem_one<VT, M0, M1, 0>();
+  if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 1>();
+  if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 2>();
+  if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 3>();
+  return s;
 }
 
 int init_kernel_attributes() {
@@ -92,19 +112,29 @@ int init_kernel_attributes() {
   return status;
 }
 
-template <typename VT>
-static int spmv_grid_for(int n_tiles, int num_sms) {
+template <typename VT, int V>
+static int spmv_grid_one(int n_tiles, int num_sms) {
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &per_sm, spmv_tiles_kernel<VT, VT, kDotNone, kDotNone>, kSpmvThreads,
-          SpmvSmem<VT>::kBytes) != cudaSuccess ||
-      per_sm < 1)
+          &per_sm, spmv_kernel_ptr<VT, kDotNone, kDotNone, V>(), kSpmvThreads,
+          spmv_smem_bytes<VT, V>()) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
     per_sm = 1;
+  }
   int g = per_sm * num_sms;
   if (g > n_tiles) g = n_tiles;
   if (g > kMaxPartialBlocks) g = kMaxPartialBlocks;
   if (g < 1) g = 1;
   return g;
+}
+
+template <typename VT>
+static void spmv_grids(int n_tiles, int num_sms, int *grid) {
+  grid[0] = spmv_grid_one<VT, 0>(n_tiles, num_sms);
+  grid[1] = spmv_grid_one<VT, 1>(n_tiles, num_sms);
+  grid[2] = spmv_grid_one<VT, 2>(n_tiles, num_sms);
+  grid[3] = spmv_grid_one<VT, 3>(n_tiles, num_sms);
 }
 
 // ------------------------------------------------------- SpMV launcher --
@@ -136,8 +166,22 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
   a.dot_out = dot_out;
   a.done = done;
   a.err = h.err_flag;
-  spmv_tiles_kernel<VT, VT, M0, M1>
-      <<<p.spmv_grid, kSpmvThreads, SpmvSmem<VT>::kBytes, stream>>>(a);
+  const int v = p.variant;
+  const int g = p.spmv_grid[v];
+  switch (v) {
+    case 1:
+      spmv_kernel_ptr<VT, M0, M1, 1>()<<<g, kSpmvThreads, spmv_smem_bytes<VT, 1>(), stream>>>(a);
+      break;
+    case 2:
+      spmv_kernel_ptr<VT, M0, M1, 2>()<<<g, kSpmvThreads, spmv_smem_bytes<VT, 2>(), stream>>>(a);
+      break;
+    case 3:
+      spmv_kernel_ptr<VT, M0, M1, 3>()<<<g, kSpmvThreads, spmv_smem_bytes<VT, 3>(), stream>>>(a);
+      break;
+    default:
+      spmv_kernel_ptr<VT, M0, M1, 0>()<<<g, kSpmvThreads, spmv_smem_bytes<VT, 0>(), stream>>>(a);
+      break;
+  }
   return cudaGetLastError();
 }
 
@@ -416,8 +460,11 @@ int mlsh_csr_plan_create(mlsh_handle hs, int n_rows, int n_cols, int nnz,
     mlsh_csr_plan_destroy(ps);
     return MLSH_ERR_OOM;
   }
-  p.spmv_grid = dtype == MLSH_F64 ? spmv_grid_for<double>(p.n_tiles, h.num_sms)
-                                  : spmv_grid_for<float>(p.n_tiles, h.num_sms);
+  if (dtype == MLSH_F64)
+    spmv_grids<double>(p.n_tiles, h.num_sms, p.spmv_grid);
+  else
+    spmv_grids<float>(p.n_tiles, h.num_sms, p.spmv_grid);
+  p.variant = kDefaultSpmvVariant;
   *out = ps;
   return MLSH_SUCCESS;
 }
@@ -479,6 +526,67 @@ int mlsh_spmv(mlsh_handle hs, mlsh_csr_plan ps, double alpha, const void *d_x,
     return MLSH_ERR_CUDA;
   }
   return MLSH_SUCCESS;
+}
+
+int mlsh_csr_plan_set_variant(mlsh_csr_plan ps, int variant) {
+  if (!ps || variant < 0 || variant >= kNumSpmvVariants) return MLSH_ERR_INVALID_ARG;
+  ps->p.variant = variant;
+  return MLSH_SUCCESS;
+}
+
+int mlsh_csr_plan_get_variant(mlsh_csr_plan ps, int *variant, int *n_variants) {
+  if (!ps) return MLSH_ERR_INVALID_ARG;
+  if (variant) *variant = ps->p.variant;
+  if (n_variants) *n_variants = kNumSpmvVariants;
+  return MLSH_SUCCESS;
+}
+
+int mlsh_csr_plan_autotune(mlsh_handle hs, mlsh_csr_plan ps, const void *d_x, void *d_y,
+                           int *chosen, double *best_seconds) {
+  if (!hs || !ps || (ps->p.n_rows > 0 && (!d_x || !d_y))) return MLSH_ERR_INVALID_ARG;
+  CsrPlan &p = ps->p;
+  const Handle &h = hs->h;
+  if (p.n_tiles == 0) {
+    if (chosen) *chosen = p.variant;
+    if (best_seconds) *best_seconds = 0.0;
+    return MLSH_SUCCESS;
+  }
+  cudaEvent_t e0, e1;
+  MLSH_CUDA_TRY(cudaEventCreate(&e0));
+  MLSH_CUDA_TRY(cudaEventCreate(&e1));
+  const int keep = p.variant;
+  int best = keep;
+  float best_ms = 1e30f;
+  int st = MLSH_SUCCESS;
+  for (int v = 0; v < kNumSpmvVariants && st == MLSH_SUCCESS; ++v) {
+    p.variant = v;
+    // warm up, then time enough launches for ~1 ms of work (at least 3)
+    int reps = 3;
+    for (int pass = 0; pass < 2 && st == MLSH_SUCCESS; ++pass) {
+      cudaEventRecord(e0, h.stream);
+      for (int r = 0; r < reps; ++r) {
+        st = mlsh_spmv(hs, ps, 1.0, d_x, 0.0, d_y);
+        if (st != MLSH_SUCCESS) break;
+      }
+      cudaEventRecord(e1, h.stream);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (pass == 0) {
+        const float per = ms / reps;
+        reps = per > 0.f ? (int)std::min(200.f, std::max(3.f, 1.0f / per)) : 3;
+      } else if (ms / reps < best_ms) {
+        best_ms = ms / reps;
+        best = v;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  p.variant = st == MLSH_SUCCESS ? best : keep;
+  if (chosen) *chosen = p.variant;
+  if (best_seconds) *best_seconds = best_ms * 1e-3;
+  return st;
 }
 
 int mlsh_csr_diag(mlsh_handle hs, mlsh_csr_plan ps, void *d_diag) {

@@ -21,8 +21,8 @@ constexpr int kTileRows = 256;
 constexpr int kTileNnz = 1792;  // = 256 rows x 7 nonzeros (7-point stencil)
 constexpr int kConsumers = 256;  // consumer threads per CTA (8 warps)
 constexpr int kSpmvThreads = kConsumers + 32;  // + one producer warp
-constexpr int kStages = 3;       // shared-memory pipeline depth
-constexpr int kShortRow = 32;    // rows up to this length: thread-per-row sum
+constexpr int kShortRow = 8;     // rows up to this length: thread-per-row sum
+constexpr int kDefaultSpmvVariant = 1;  // until the plan is autotuned
 
 // Elementwise / reduction kernels.
 constexpr int kVecThreads = 256;
@@ -120,7 +120,8 @@ struct CsrPlan {
   double *chunk_part = nullptr;   // device, n_chunks
   unsigned *long_cnt = nullptr;   // device, n_long (zero between launches)
   double *long_dot = nullptr;     // device, 2 * n_long
-  int spmv_grid = 0;              // CTAs of the SpMV launch
+  int spmv_grid[4] = {0, 0, 0, 0}; // CTAs of the SpMV launch, per kernel variant
+  int variant = 0;                // SpMV kernel variant in use
   // cached derived data
   void *inv_diag = nullptr;       // 1/diag(A), dtype elements
   bool inv_diag_valid = false;

@@ -11,22 +11,35 @@
 //  * A persistent grid (a few CTAs per SM) walks the tiles round-robin, so
 //    every CTA's work and summation order are fixed by the sizes.
 //  * Warp specialisation: warp 0 is the producer.  Lane 0 streams each
-//    tile's contiguous val[] and col_ind[] ranges into a kStages-deep ring
+//    tile's contiguous val[] and col_ind[] ranges into a STAGES-deep ring
 //    of shared-memory stages with 1-D bulk (TMA) copies that complete on an
 //    mbarrier; the other lanes fill the <16-byte ragged ends with plain
-//    loads.  HBM sees only long, aligned, fully used bursts.
-//  * 8 consumer warps: pass A forms val[j]*x[col[j]] in place over the
-//    tile's nonzeros (nonzero-parallel, so the x gathers are balanced and
-//    independent; x is read through the read-only path), pass B sums each
-//    row of up to kShortRow entries sequentially in one thread (the same
-//    order as the reference's row loop, so those rows are bit-identical to
-//    it), pass C gives longer rows a whole warp, pass D writes y coalesced
-//    and accumulates the fused dots in a fixed per-thread order.
+//    loads.  HBM sees only long, aligned, fully used bursts, and the copies
+//    carry an L2 evict-first policy so the once-read matrix does not push
+//    the gathered x out of L2.
+//  * 8 consumer warps.  Each thread first issues the row_ptr loads of its
+//    row of the tile (independent of the stage, so they overlap the wait),
+//    then:
+//      pass A  val[j]*x[col[j]] in place over the tile's nonzeros
+//              (nonzero-parallel: the x gathers are balanced and
+//              independent; x goes through the read-only path);
+//      pass B  one thread sums each row of up to kShortRow entries in row
+//              order (the reference's loop order, so those rows are
+//              bit-identical to it);
+//      pass C  longer rows are cut into kSegW-entry segments spread over
+//              all warps (an 8-lane tree per segment, four segments per
+//              warp instruction), then each row adds its segment sums in
+//              order -- balanced and deterministic;
+//      pass D  y written coalesced, fused dots accumulated in a fixed
+//              per-thread order.
 //  * Chunk tiles reduce their products CTA-wide into a per-chunk partial;
 //    the last chunk to arrive (atomic counter per long row) sums the
 //    partials in chunk order and writes the row.
 //  * Every wait on an mbarrier is bounded; on timeout the CTA records
 //    MLSH_ERR_TIMEOUT, drains its in-flight copies and exits.
+//  * Variants (pipeline depth x CTAs per SM) trade shared memory against
+//    L1 capacity for the x gathers and against occupancy; the plan keeps
+//    the one its autotuner measured fastest.
 #pragma once
 #include "mlsh_internal.cuh"
 #include "mlsh_ptx.cuh"
@@ -38,6 +51,13 @@ namespace mlsh {
 constexpr int kDotNone = 0;
 constexpr int kDotW = 1;     // sum w[i] * y[i]
 constexpr int kDotSelf = 2;  // sum y[i] * y[i]
+
+// Rows longer than kShortRow are summed in segments of kSegW entries.
+constexpr int kSegW = 8;
+// Upper bound of segments in one tile: each such row has > kSegW entries,
+// so ceil(len/kSegW) < 2*len/kSegW.
+constexpr int kMaxSegs = 2 * kTileNnz / kSegW;
+static_assert(kShortRow >= kSegW, "segments must not be longer than short rows");
 
 template <typename VT, typename XT>
 struct SpmvArgs {
@@ -65,16 +85,18 @@ struct SpmvArgs {
   int *err;         // set to MLSH_ERR_TIMEOUT if a wait gives up
 };
 
-template <typename VT>
+template <typename VT, int STAGES>
 struct SpmvSmem {
   static constexpr int kValBytes = ((kTileNnz * (int)sizeof(VT) + 16) + 15) & ~15;
   static constexpr int kColBytes = ((kTileNnz * 4 + 16) + 15) & ~15;
   static constexpr int kStageBytes = kValBytes + kColBytes;
-  static constexpr int kYsOff = kStages * kStageBytes;
-  static constexpr int kBarOff = kYsOff + kTileRows * (int)sizeof(VT) + 16;
-  static constexpr int kRedOff = kBarOff + 2 * kStages * 8;
+  static constexpr int kYsOff = STAGES * kStageBytes;
+  static constexpr int kSegSumOff = kYsOff + kTileRows * (int)sizeof(VT) + 16;
+  static constexpr int kSegIdxOff = kSegSumOff + kMaxSegs * (int)sizeof(VT) + 16;
+  static constexpr int kBarOff = (kSegIdxOff + 2 * kMaxSegs * 2 + 64 + 15) & ~15;
+  static constexpr int kRedOff = kBarOff + 2 * STAGES * 8;
   static constexpr int kFlagOff = kRedOff + 32 * 8;
-  static constexpr int kBytes = kFlagOff + 8 * 4;
+  static constexpr int kBytes = kFlagOff + 16 * 4;
 };
 
 // flags[] in shared memory
@@ -82,26 +104,40 @@ constexpr int kFlagProdAbort = 0;
 constexpr int kFlagConsAbort = 1;
 constexpr int kFlagConsumed = 2;
 constexpr int kFlagLast = 3;
+constexpr int kFlagWarpSeg = 4;  // 8 per-warp segment counts (4..11)
 
 template <typename T>
 __device__ __forceinline__ int head_elems(const T *base, int idx) {
   return (int)(((uintptr_t)(base + idx) & 15u) / sizeof(T));
 }
 
-// Producer side: stage tile `tl` of array `arr` (element type E) into smem
-// buffer `dst`, element nnz_begin landing at dst[head].  Returns the bytes
-// the bulk copy will deliver (0 if none).  Called by all 32 lanes.
+// Named barrier over the consumer threads that also ORs a predicate.
+__device__ __forceinline__ bool consumers_sync_or(bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "n"(kConsumers)
+      : "memory");
+  return r != 0;
+}
+
+// Producer side: stage tile elements [nb, ne) of `arr` into smem `dst`,
+// element nb landing at dst[head].  The <16-byte ragged ends are loaded by
+// lanes 0..15 (head) and 16..31 (tail).  Returns the bytes the bulk copy
+// of the aligned interior will deliver (0 if none).  Called by all lanes.
 template <typename E>
-__device__ __forceinline__ uint32_t stage_range(const E *arr, int nb, int ne,
-                                                E *dst, int lane,
-                                                uint32_t bar) {
+__device__ __forceinline__ uint32_t stage_range(const E *arr, int nb, int ne, E *dst,
+                                                int lane) {
   const uintptr_t b0 = (uintptr_t)(arr + nb);
   const uintptr_t b1 = (uintptr_t)(arr + ne);
   const uintptr_t lo = b0 & ~(uintptr_t)15;
   uintptr_t i0 = (b0 + 15) & ~(uintptr_t)15;
   uintptr_t i1 = b1 & ~(uintptr_t)15;
   const int head = (int)((b0 - lo) / sizeof(E));
-  // ragged elements: [nb, e0) and [e1, ne) with e0/e1 the interior bounds
   int e0, e1;
   if (i1 > i0) {
     e0 = nb + (int)((i0 - b0) / sizeof(E));
@@ -116,16 +152,14 @@ __device__ __forceinline__ uint32_t stage_range(const E *arr, int nb, int ne,
   if (lane < nhead) dst[head + lane] = arr[nb + lane];
   if (lane >= 16 && lane - 16 < ntail)
     dst[head + (e1 - nb) + (lane - 16)] = arr[e1 + (lane - 16)];
-  uint32_t bytes = (uint32_t)(i1 - i0);
-  (void)bar;
-  return bytes;
+  return (uint32_t)(i1 - i0);
 }
 
-template <typename VT, typename XT, int M0, int M1>
-__global__ void __launch_bounds__(kSpmvThreads, 3)
+template <typename VT, typename XT, int M0, int M1, int STAGES, int MINB>
+__global__ void __launch_bounds__(kSpmvThreads, MINB)
     spmv_tiles_kernel(const SpmvArgs<VT, XT> a) {
   constexpr int NR = (M0 != kDotNone ? 1 : 0) + (M1 != kDotNone ? 1 : 0);
-  using L = SpmvSmem<VT>;
+  using L = SpmvSmem<VT, STAGES>;
   extern __shared__ __align__(128) unsigned char smem[];
   if (a.done != nullptr && *a.done != 0) return;
 
@@ -133,16 +167,19 @@ __global__ void __launch_bounds__(kSpmvThreads, 3)
   double *red = reinterpret_cast<double *>(smem + L::kRedOff);
   volatile int *flags = reinterpret_cast<volatile int *>(smem + L::kFlagOff);
   VT *ys = reinterpret_cast<VT *>(smem + L::kYsOff);
+  VT *segsum = reinterpret_cast<VT *>(smem + L::kSegSumOff);
+  short *seg_lo = reinterpret_cast<short *>(smem + L::kSegIdxOff);
+  short *seg_hi = seg_lo + kMaxSegs;
   const int tid = threadIdx.x;
   const uint32_t full0 = smem_addr(bars);
-  const uint32_t empty0 = smem_addr(bars + kStages);
+  const uint32_t empty0 = smem_addr(bars + STAGES);
 
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < STAGES; ++s) {
       mbar_init(full0 + 8 * s, 1);
       mbar_init(empty0 + 8 * s, 1);
     }
-    for (int f = 0; f < 8; ++f) flags[f] = 0;
+    for (int f = 0; f < 16; ++f) flags[f] = 0;
     fence_mbar_init();
   }
   __syncthreads();
@@ -150,14 +187,15 @@ __global__ void __launch_bounds__(kSpmvThreads, 3)
   if (tid < 32) {
     // ------------------------------------------------------- producer ---
     const int lane = tid;
+    const uint64_t stream_policy = l2_evict_first_policy();
     int k = 0;
     bool aborted = false;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++k) {
-      const int s = k % kStages;
-      if (k >= kStages) {
+      const int s = k % STAGES;
+      if (k >= STAGES) {
         int ok = 1;
         if (lane == 0) {
-          const uint32_t par = (uint32_t)((k / kStages - 1) & 1);
+          const uint32_t par = (uint32_t)((k / STAGES - 1) & 1);
           const uint64_t t0 = global_timer_ns();
           ok = 0;
           while (true) {
@@ -177,8 +215,8 @@ __global__ void __launch_bounds__(kSpmvThreads, 3)
       VT *sv = reinterpret_cast<VT *>(st);
       int *sc = reinterpret_cast<int *>(st + L::kValBytes);
       const uint32_t bar = full0 + 8 * s;
-      const uint32_t vb = stage_range<VT>(a.val, tl.nnz_begin, tl.nnz_end, sv, lane, bar);
-      const uint32_t cb = stage_range<int>(a.col, tl.nnz_begin, tl.nnz_end, sc, lane, bar);
+      const uint32_t vb = stage_range<VT>(a.val, tl.nnz_begin, tl.nnz_end, sv, lane);
+      const uint32_t cb = stage_range<int>(a.col, tl.nnz_begin, tl.nnz_end, sc, lane);
       __threadfence_block();
       __syncwarp();
       if (lane == 0) {
@@ -187,12 +225,14 @@ __global__ void __launch_bounds__(kSpmvThreads, 3)
         if (vb) {
           const uintptr_t i0 = ((uintptr_t)(a.val + tl.nnz_begin) + 15) & ~(uintptr_t)15;
           const uintptr_t lo = (uintptr_t)(a.val + tl.nnz_begin) & ~(uintptr_t)15;
-          bulk_g2s(smem_addr(st) + (uint32_t)(i0 - lo), (const void *)i0, vb, bar);
+          bulk_g2s_hint(smem_addr(st) + (uint32_t)(i0 - lo), (const void *)i0, vb, bar,
+                        stream_policy);
         }
         if (cb) {
           const uintptr_t i0 = ((uintptr_t)(a.col + tl.nnz_begin) + 15) & ~(uintptr_t)15;
           const uintptr_t lo = (uintptr_t)(a.col + tl.nnz_begin) & ~(uintptr_t)15;
-          bulk_g2s(smem_addr(st + L::kValBytes) + (uint32_t)(i0 - lo), (const void *)i0, cb, bar);
+          bulk_g2s_hint(smem_addr(st + L::kValBytes) + (uint32_t)(i0 - lo), (const void *)i0,
+                        cb, bar, stream_policy);
         }
       }
       __syncwarp();
@@ -202,9 +242,9 @@ __global__ void __launch_bounds__(kSpmvThreads, 3)
     // no copy is in flight when the CTA exits).  If they aborted, wait for
     // the copies themselves instead.
     if (lane == 0) {
-      for (int kk = issued - kStages < 0 ? 0 : issued - kStages; kk < issued; ++kk) {
-        const int s = kk % kStages;
-        const uint32_t par = (uint32_t)((kk / kStages) & 1);
+      for (int kk = issued - STAGES < 0 ? 0 : issued - STAGES; kk < issued; ++kk) {
+        const int s = kk % STAGES;
+        const uint32_t par = (uint32_t)((kk / STAGES) & 1);
         const uint64_t t0 = global_timer_ns();
         bool ok = false;
         while (true) {
@@ -218,8 +258,8 @@ __global__ void __launch_bounds__(kSpmvThreads, 3)
         atomicExch(a.err, MLSH_ERR_TIMEOUT);
         const int consumed = flags[kFlagConsumed];
         for (int kk = consumed; kk < issued; ++kk) {
-          const int s = kk % kStages;
-          mbar_wait_bounded(full0 + 8 * s, (uint32_t)((kk / kStages) & 1), kWaitLimitNs);
+          const int s = kk % STAGES;
+          mbar_wait_bounded(full0 + 8 * s, (uint32_t)((kk / STAGES) & 1), kWaitLimitNs);
         }
       }
     }
@@ -237,9 +277,19 @@ __global__ void __launch_bounds__(kSpmvThreads, 3)
 
   int k = 0;
   for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++k) {
-    const int s = k % kStages;
+    const int s = k % STAGES;
+    const Tile tl = a.tiles[t];
+    const bool normal = tl.row_end >= 0;
+    const int rb = tl.row_begin;
+    const int nrows = normal ? tl.row_end - tl.row_begin : 0;
+    // row bounds of this thread's row, issued before the stage wait
+    int g0 = 0, g1 = 0;
+    if (ct < nrows) {
+      g0 = __ldg(a.row_ptr + rb + ct);
+      g1 = __ldg(a.row_ptr + rb + ct + 1);
+    }
     if (ct == 0) {
-      if (!mbar_wait_bounded(full0 + 8 * s, (uint32_t)((k / kStages) & 1), kWaitLimitNs)) {
+      if (!mbar_wait_bounded(full0 + 8 * s, (uint32_t)((k / STAGES) & 1), kWaitLimitNs)) {
         flags[kFlagConsAbort] = 1;
         atomicExch(a.err, MLSH_ERR_TIMEOUT);
       }
@@ -247,7 +297,6 @@ __global__ void __launch_bounds__(kSpmvThreads, 3)
     named_sync(1, kConsumers);
     if (flags[kFlagConsAbort]) break;
 
-    const Tile tl = a.tiles[t];
     const int nb = tl.nnz_begin, ne = tl.nnz_end, nt = ne - nb;
     unsigned char *st = smem + s * L::kStageBytes;
     VT *v = reinterpret_cast<VT *>(st) + head_elems(a.val, nb);
@@ -275,38 +324,68 @@ __global__ void __launch_bounds__(kSpmvThreads, 3)
     }
     named_sync(1, kConsumers);
 
-    if (tl.row_end >= 0) {
-      // -------------------------------------------------- normal tile ---
-      const int rb = tl.row_begin, nrows = tl.row_end - tl.row_begin;
-      bool med = false;
-      int s0 = 0, s1 = 0;
-      if (ct < nrows) {
-        s0 = __ldg(a.row_ptr + rb + ct) - nb;
-        s1 = __ldg(a.row_ptr + rb + ct + 1) - nb;
-        if (s1 - s0 <= kShortRow) {
+    if (normal) {
+      // ------------------------------------------------ pass B: short rows
+      const int s0 = g0 - nb, s1 = g1 - nb, len = s1 - s0;
+      const bool med = ct < nrows && len > kShortRow;
+      if (ct < nrows && !med) {
+        VT sum = VT(0);
+        for (int j = s0; j < s1; ++j) sum += v[j];
+        ys[ct] = sum;
+      }
+      // ------------------------------------ pass C: kSegW-entry segments
+      if (consumers_sync_or(med)) {
+        // exclusive scan of segment counts over the tile's rows
+        const int nseg = med ? (len + kSegW - 1) / kSegW : 0;
+        int inc = nseg;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o) inc += y;
+        }
+        if (lane == 31) flags[kFlagWarpSeg + warp] = inc;
+        named_sync(1, kConsumers);
+        int base = 0, total = 0;
+#pragma unroll
+        for (int w = 0; w < kConsumers / 32; ++w) {
+          const int cw = flags[kFlagWarpSeg + w];
+          if (w < warp) base += cw;
+          total += cw;
+        }
+        const int first = base + inc - nseg;
+        for (int q = 0; q < nseg; ++q) {
+          seg_lo[first + q] = (short)(s0 + kSegW * q);
+          seg_hi[first + q] = (short)min(s0 + kSegW * (q + 1), s1);
+        }
+        named_sync(1, kConsumers);
+        // four segments per warp step: lanes 8g..8g+7 take segment g
+        constexpr int kSegPerWarp = 32 / kSegW;
+        const int sub = lane / kSegW, sl = lane % kSegW;
+        for (int sg0 = warp * kSegPerWarp; sg0 < total; sg0 += kConsumers / kSegW) {
+          const int sg = sg0 + sub;
+          VT part = VT(0);
+          if (sg < total) {
+            const int j = seg_lo[sg] + sl;
+            if (j < seg_hi[sg]) part = v[j];
+          }
+#pragma unroll
+          for (int o = kSegW / 2; o > 0; o >>= 1)
+            part += __shfl_xor_sync(0xffffffffu, part, o, kSegW);
+          if (sl == 0 && sg < total) segsum[sg] = part;
+        }
+        named_sync(1, kConsumers);
+        if (med) {
           VT sum = VT(0);
-          for (int j = s0; j < s1; ++j) sum += v[j];
+          for (int q = 0; q < nseg; ++q) sum += segsum[first + q];
           ys[ct] = sum;
-        } else {
-          med = true;
         }
       }
-      unsigned mask = __ballot_sync(0xffffffffu, med);
-      while (mask) {
-        const int l = __ffs(mask) - 1;
-        mask &= mask - 1;
-        const int r0 = __shfl_sync(0xffffffffu, s0, l);
-        const int r1 = __shfl_sync(0xffffffffu, s1, l);
-        VT sum = VT(0);
-        for (int j = r0 + lane; j < r1; j += 32) sum += v[j];
-        sum = warp_sum(sum);
-        if (lane == 0) ys[warp * 32 + l] = sum;
-      }
-      named_sync(1, kConsumers);
+      // all reads of the stage are done (the last barrier above)
       if (ct == 0) {
         mbar_arrive(empty0 + 8 * s);
         flags[kFlagConsumed] = k + 1;
       }
+      // ----------------------------------------------------- pass D: y
       if (ct < nrows) {
         const int r = rb + ct;
         const double sum = (double)ys[ct];
@@ -377,5 +456,13 @@ __global__ void __launch_bounds__(kSpmvThreads, 3)
     }
   }
 }
+
+// Kernel variants: pipeline depth and CTAs per SM.
+struct SpmvVariant {
+  int stages;
+  int min_blocks;
+};
+constexpr int kNumSpmvVariants = 4;
+constexpr SpmvVariant kSpmvVariants[kNumSpmvVariants] = {{3, 3}, {2, 3}, {2, 4}, {4, 2}};
 
 }  // namespace mlsh

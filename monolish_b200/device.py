@@ -149,6 +149,22 @@ class Crs:
                                                C.byref(b)), "plan_info")
         return {"n_tiles": nt.value, "n_long_rows": nl.value, "spmv_bytes": b.value}
 
+    def autotune(self, x, y):
+        """Time every SpMV kernel variant on this matrix; keep the fastest."""
+        v, sec = C.c_int(), C.c_double()
+        _abi.check(self.lib.mlsh_csr_plan_autotune(self.handle.h, self.plan, ptr(x), ptr(y),
+                                                   C.byref(v), C.byref(sec)), "autotune")
+        return v.value, sec.value
+
+    def set_variant(self, v):
+        _abi.check(self.lib.mlsh_csr_plan_set_variant(self.plan, int(v)), "set_variant")
+
+    def variant(self):
+        v, nv = C.c_int(), C.c_int()
+        _abi.check(self.lib.mlsh_csr_plan_get_variant(self.plan, C.byref(v), C.byref(nv)),
+                   "get_variant")
+        return v.value, nv.value
+
     def matvec(self, x, y, alpha=1.0, beta=0.0):
         _abi.check(self.lib.mlsh_spmv(self.handle.h, self.plan, alpha, ptr(x), beta, ptr(y)),
                    "spmv")

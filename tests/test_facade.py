@@ -28,7 +28,7 @@ def write_mm(path, n, rp, ci, v):
         f.write(f"{n} {n} {len(v)}\n")
         for i in range(n):
             for j in range(rp[i], rp[i + 1]):
-                f.write(f"{i + 1} {ci[j] + 1} {v[j]!r}\n")
+                f.write(f"{i + 1} {int(ci[j]) + 1} {float(v[j])!r}\n")
 
 
 @pytest.fixture(scope="module")
