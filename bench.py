@@ -55,7 +55,9 @@ WORKLOADS = {
     "spmv_zipf_f32": dict(kind="spmv", matrix="zipf", n=4194304, dtype="f32"),
     "cg_poisson2d": dict(kind="cg", matrix="poisson2d", m=128, dtype="f64"),
     "bicgstab_convdiff": dict(kind="bicgstab", matrix="convdiff3d", m=160, dtype="f64"),
+    "batch_cg": dict(kind="batch", matrix="diffusion_batch", count=2048, dtype="f64"),
 }
+METRIC_BATCH = "solves/s at 1e-8 rel. residual, 2,048-system batch"
 
 
 def env_rank():
@@ -362,7 +364,13 @@ def run_solve(args, wl, rank, world, local):
     A = D.Crs(h, n, n, rp, ci, v, validate=False)
     db = torch.from_numpy(b).cuda()
     dx = torch.zeros(n, dtype=torch.float64, device="cuda")
-    fn = D.cg_solve if wl["kind"] == "cg" else D.bicgstab_solve
+    base_fn = D.cg_solve if wl["kind"] == "cg" else D.bicgstab_solve
+    engine = {"auto": 0, "kernels": 1, "cluster": 2}[args.engine]
+
+    def fn(A_, b_, x_, tol_, maxiter_):
+        return base_fn(A_, b_, x_, tol_, maxiter_, engine=engine,
+                       cluster_rows=args.cluster_rows)
+
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
         dx.zero_()
@@ -415,6 +423,7 @@ def run_solve(args, wl, rank, world, local):
             "data": "synthetic (seeded generators)",
             "config": {"workload": describe(wl), "n": n, "nnz": nnz, "iters": r.iters,
                        "status": r.status, "true_rel_residual": rel,
+                       "engine": args.engine, "cluster_rows": args.cluster_rows,
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": round(world * args.steps / (e2e_ms / 1e3), 3), "unit": "solves/s",
                     "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
@@ -440,10 +449,193 @@ def run_solve(args, wl, rank, world, local):
     return out
 
 
+# ----------------------------------------------------------- batch leg
+def batch_inputs(wl):
+    """Systems, right-hand sides b = A x_true (x_true ~ U[-1,1], seed 3 + k)
+    and per-system absolute tolerances 1e-8 * ||b_k||."""
+    import oracle
+    from monolish_b200 import workloads as W
+    count = wl.get("size") or wl["count"]
+    systems = W.diffusion_batch(count, seed=3)
+    port = oracle.restatement()
+    bs = [port.spmv(rp, ci, v, W.uniform_mt(len(rp) - 1, -1.0, 1.0, 3 + k))
+          for k, (rp, ci, v) in enumerate(systems)]
+    tol = np.array([1e-8 * np.linalg.norm(b) for b in bs])
+    return systems, bs, tol
+
+
+def cpu_reference_batch(systems, bs, tol, every, threads):
+    """The reference's CG (Jacobi) on every `every`-th system; returns the
+    extrapolated seconds for the whole batch and the sample size."""
+    import oracle
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    ref = oracle.reference_or_none()
+    if ref is None:
+        return None, 0, "port"
+    ref.set_threads(threads)
+    idx = list(range(0, len(systems), every))
+    total = 0.0
+    for k in idx:
+        rp, ci, v = systems[k]
+        st, it, res, x, sec = ref.cg(rp, ci, v, bs[k], np.zeros(len(bs[k])), float(tol[k]), 20000)
+        total += sec
+    return total * len(systems) / len(idx), len(idx), "reference"
+
+
+def run_batch(args, wl, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    import oracle
+    from monolish_b200 import device as D
+
+    torch.cuda.set_device(local)
+    systems, bs, tol = batch_inputs(wl)
+    count = len(systems)
+    h = D.Handle()
+    B = D.Batch(h, systems)
+    b_all = np.concatenate(bs)
+    db = torch.from_numpy(b_all).cuda()
+    dx = torch.zeros_like(db)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        dx.zero_()
+        status, iters, resid = B.solve("cg", db, dx, tol, 20000)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dx.zero_()
+        status, iters, resid = B.solve("cg", db, dx, tol, 20000)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    cl = clocks.stop()
+    x_all = dx.cpu().numpy()
+    # end to end: b from pinned host memory, x back, per batch solve
+    hb = torch.from_numpy(b_all).pin_memory()
+    hx = torch.empty_like(hb).pin_memory()
+    e0.record(stream)
+    for _ in range(max(1, min(args.steps, 3))):
+        db.copy_(hb, non_blocking=True)
+        dx.zero_()
+        B.solve("cg", db, dx, tol, 20000)
+        hx.copy_(dx, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / max(1, min(args.steps, 3))
+    # the comparison: a loop of single plain FP64 solves (mlsh_cg_solve per
+    # system, its default engine), device time over the whole loop
+    loop_ms = None
+    loop_iters = None
+    if not args.quick:
+        plans = [D.Crs(h, len(rp) - 1, len(rp) - 1, rp, ci, v, validate=False)
+                 for rp, ci, v in systems]
+        dbs = [torch.from_numpy(b).cuda() for b in bs]
+        dxs = [torch.zeros_like(d) for d in dbs]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(stream)
+        loop_iters = []
+        for k in range(count):
+            r = D.cg_solve(plans[k], dbs[k], dxs[k], float(tol[k]), 20000)
+            loop_iters.append(r.iters)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        loop_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
+        for A in plans:
+            A.close()
+    if world > 1:
+        t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    out = None
+    if rank == 0:
+        port = oracle.restatement()
+        xs = np.split(x_all, np.cumsum([len(b) for b in bs])[:-1])
+        sample = list(range(0, count, max(1, count // 32)))
+        worst = max(port.true_relres(*systems[k], bs[k], xs[k]) for k in sample)
+        per_step_s = ms / 1e3 / args.steps
+        value = world * count / per_step_s
+        rows = int(sum(len(b) for b in bs))
+        nnz = int(sum(int(rp[-1]) for rp, _, _ in systems))
+        iters = np.asarray(iters)
+        # algorithmic bytes of the fused CG iteration, summed over systems
+        bytes_all = float(sum(it * ((int(systems[k][0][-1]) * 12 + (len(bs[k]) + 1) * 4)
+                                    + 13 * len(bs[k]) * 8) for k, it in enumerate(iters)))
+        peak, peak_kind = measured_peak()
+        out = {
+            "metric": METRIC_BATCH, "value": round(value, 2), "unit": "solves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generators)",
+            "config": {"workload": f"{count} variable-coefficient 2D diffusion systems, n "
+                                   "log-uniform in [1e3, 1e5] (seed 3), Jacobi-CG to 1e-8 "
+                                   "relative residual, FP64, one launch per cluster-size group",
+                       "systems": count, "rows": rows, "nnz": nnz,
+                       "iters_total": int(iters.sum()), "iters_max": int(iters.max()),
+                       "all_converged": bool((np.asarray(status) == 0).all()),
+                       "worst_true_rel_residual_sampled": worst,
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": round(world * count / (e2e_ms / 1e3), 2), "unit": "solves/s",
+                    "h2d_bytes_per_step": b_all.nbytes, "d2h_bytes_per_step": b_all.nbytes},
+            "roofline": {"bound": "hbm", "achieved": round(bytes_all / per_step_s / 1e9, 1),
+                         "peak": peak, "unit": "GB/s",
+                         "frac": round(bytes_all / per_step_s / 1e9 / peak, 4),
+                         "peak_kind": peak_kind, "traffic": None,
+                         "note": "fused-CG algorithmic bytes summed over systems / batch time "
+                                 "(small systems run from L2, so this can exceed HBM)"},
+            "gpu_launches": args.steps,
+        }
+        if loop_ms is not None:
+            out["loop_of_single_solves"] = {
+                "value": round(count / (loop_ms / 1e3), 2), "unit": "solves/s",
+                "speedup_of_batch": round((count / per_step_s) / (count / (loop_ms / 1e3)), 2),
+                "iters_match": bool(np.array_equal(np.asarray(loop_iters), iters))}
+        if world == 1 and not args.no_cpu:
+            threads = os.cpu_count() or 1
+            sec, ns, kind = cpu_reference_batch(systems, bs, tol, max(1, count // 16), threads)
+            if sec:
+                out["cpu_baseline"] = {"value": round(count / sec, 3), "unit": "solves/s",
+                                       "cores": threads, "kind": kind,
+                                       "sample": f"{ns} of {count} systems (every "
+                                                 f"{max(1, count // 16)}th), time scaled to "
+                                                 "the whole batch"}
+        if cl:
+            out["clocks"] = cl
+    B.close()
+    h.close()
+    return out
+
+
 # ---------------------------------------------------------- reference arm
 def run_reference(args, wl, rank, world):
     if rank != 0:
         return None
+    if wl["kind"] == "batch":
+        threads = os.cpu_count() or 1
+        systems, bs, tol = batch_inputs(wl)
+        count = len(systems)
+        every = max(1, count // 16)
+        sec, ns, kind = cpu_reference_batch(systems, bs, tol, every, threads)
+        value = count / sec
+        return {"metric": METRIC_BATCH, "value": round(value, 3), "unit": "solves/s",
+                "n_gpus": world, "steps": 1, "warmup": 0,
+                "ms_per_step": round(sec * 1e3, 1), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generators)", "impl": "reference",
+                "config": {"workload": f"{count}-system diffusion batch, Jacobi-CG to 1e-8"},
+                "cpu_baseline": {"value": round(value, 3), "unit": "solves/s",
+                                 "cores": threads, "kind": kind,
+                                 "sample": f"{ns} of {count} systems (every {every}th), time "
+                                           "scaled to the whole batch"},
+                "e2e": {"value": round(value, 3), "unit": "solves/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
     threads = os.cpu_count() or 1
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
     os.environ.setdefault("OMP_PROC_BIND", "close")
@@ -508,6 +700,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--size", type=int, default=0,
                     help="override the grid edge (n for zipf); for small profiling cases")
+    ap.add_argument("--engine", choices=["auto", "kernels", "cluster"], default="auto",
+                    help="solve engine for the solver workloads")
+    ap.add_argument("--cluster-rows", type=int, default=0,
+                    help="cluster engine: rows per CTA (0 = auto)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="SpMV kernel variant (default: autotuned per matrix)")
     ap.add_argument("--quick", action="store_true",
@@ -535,6 +731,8 @@ def main():
     try:
         if wl["kind"] == "spmv":
             out = run_spmv(args, wl, rank, world, local)
+        elif wl["kind"] == "batch":
+            out = run_batch(args, wl, rank, world, local)
         else:
             out = run_solve(args, wl, rank, world, local)
     finally:

@@ -195,20 +195,38 @@ int mlsh_fill(mlsh_handle handle, int dtype, int64_t n, double value,
               void *d_y);
 
 /* ------------------------------------------------------------ solvers --- */
+/* Solve engines.
+ *   KERNELS  one kernel per step (SpMV+dot, update+dots, direction update),
+ *            the loop in a CUDA graph with a device-side while node; any n.
+ *   CLUSTER  the whole solve in one launch of one thread-block cluster (up
+ *            to 16 CTAs) with the iteration vectors in shared memory and
+ *            the gathered vector read across CTAs; for n up to 131,072
+ *            (CG, FP64) / 65,536 (BiCGSTAB, FP64), twice that in FP32.  A
+ *            wall-clock budget of 60 s per solve ends a solve that does not
+ *            terminate with MLSH_ERR_TIMEOUT.
+ *   AUTO     CLUSTER when the system fits and maxiter <= 2,000,000, else
+ *            KERNELS. */
+#define MLSH_ENGINE_AUTO 0
+#define MLSH_ENGINE_KERNELS 1
+#define MLSH_ENGINE_CLUSTER 2
+
 typedef struct {
   double tol;       /* absolute threshold on ||r||_2, like solver::set_tol
                        (src/equation/cg.cpp:67, equation.cpp:8-11) */
   int64_t maxiter;  /* set_maxiter */
   int64_t miniter;  /* set_miniter */
   int precond;      /* MLSH_PRECOND_NONE / MLSH_PRECOND_JACOBI */
-  int use_graph;    /* 1: whole solve as one CUDA graph with a device-side
-                       while loop (no host round trip); 0: eager launches
-                       with a host check every `check_every` iterations */
+  int use_graph;    /* KERNELS engine: 1: whole solve as one CUDA graph with a
+                       device-side while loop (no host round trip); 0: eager
+                       launches with a host check every `check_every` steps */
   int check_every;  /* eager mode only; <= 0 picks a default */
-  int reserved;
+  int engine;       /* MLSH_ENGINE_* */
   double *history;     /* optional host buffer: ||r|| after each iteration
                           (solver::set_print_rhistory, cg.cpp:62-65) */
   int64_t history_len; /* capacity of `history` in doubles */
+  int cluster_rows;    /* CLUSTER engine: rows per CTA (a power of two >= 1024);
+                          0 picks the smallest that fits 16 CTAs */
+  int reserved;
 } mlsh_solver_opts;
 
 typedef struct {
@@ -236,6 +254,38 @@ int mlsh_bicgstab_solve(mlsh_handle handle, mlsh_csr_plan plan,
                         const void *d_b, void *d_x,
                         const mlsh_solver_opts *opts,
                         mlsh_solver_result *result);
+
+/* ------------------------------------------------------ batched solves -- */
+/* Thousands of independent, uneven systems solved together (no reference
+ * counterpart: the reference solves one system per solve() call).
+ *
+ * Storage: the systems' CRS matrices concatenated.  System k owns rows
+ * [row_off[k], row_off[k+1]) of the concatenated vectors; `d_row_ptr`
+ * (total_rows + 1 entries) holds offsets into the concatenated col/val
+ * arrays, and column indices are local to their system (0 .. n_k - 1).
+ * Every system must fit the cluster engine (n_k <= 131,072 CG / 65,536
+ * BiCGSTAB in FP64).
+ *
+ * mlsh_batch_create groups the systems by the cluster size they need
+ * (largest first).  mlsh_batch_solve launches one persistent cluster
+ * kernel per group on its own stream; each cluster takes systems from the
+ * group's queue and solves them start to finish, so systems converge (and
+ * retire) independently and freed SMs go to the next group. */
+typedef struct mlsh_batch_s *mlsh_batch;
+
+int mlsh_batch_create(mlsh_handle handle, int n_systems, const int64_t *host_row_off,
+                      const int *d_row_ptr, const int *d_col_ind, const void *d_val,
+                      int dtype, mlsh_batch *batch);
+int mlsh_batch_destroy(mlsh_batch batch);
+/* kind 0 = CG, 1 = BiCGSTAB.  d_b / d_x: concatenated right-hand sides and
+ * initial guesses (solutions on exit).  host_tol: per-system absolute
+ * tolerances (NULL: opts->tol for all).  opts: maxiter, miniter, precond.
+ * host_status / host_iters / host_resid (may be NULL): per-system results
+ * in input order.  Synchronous; returns MLSH_SUCCESS when every system
+ * converged, else the first non-success status. */
+int mlsh_batch_solve(mlsh_handle handle, mlsh_batch batch, int kind, const void *d_b,
+                     void *d_x, const double *host_tol, const mlsh_solver_opts *opts,
+                     int *host_status, int64_t *host_iters, double *host_resid);
 
 #ifdef __cplusplus
 }

@@ -37,8 +37,14 @@ f64 = C.c_double
 
 class SolverOpts(C.Structure):
     _fields_ = [("tol", f64), ("maxiter", i64), ("miniter", i64), ("precond", i32),
-                ("use_graph", i32), ("check_every", i32), ("reserved", i32),
-                ("history", C.POINTER(f64)), ("history_len", i64)]
+                ("use_graph", i32), ("check_every", i32), ("engine", i32),
+                ("history", C.POINTER(f64)), ("history_len", i64),
+                ("cluster_rows", i32), ("reserved", i32)]
+
+
+ENGINE_AUTO = 0
+ENGINE_KERNELS = 1
+ENGINE_CLUSTER = 2
 
 
 class SolverResult(C.Structure):
@@ -86,6 +92,9 @@ SIGNATURES = {
     "mlsh_cg_solve": (i32, [vp, vp, vp, vp, C.POINTER(SolverOpts), C.POINTER(SolverResult)]),
     "mlsh_bicgstab_solve": (i32, [vp, vp, vp, vp, C.POINTER(SolverOpts),
                                   C.POINTER(SolverResult)]),
+    "mlsh_batch_create": (i32, [vp, i32, vp, vp, vp, vp, i32, C.POINTER(vp)]),
+    "mlsh_batch_destroy": (i32, [vp]),
+    "mlsh_batch_solve": (i32, [vp, vp, i32, vp, vp, vp, C.POINTER(SolverOpts), vp, vp, vp]),
 }
 
 _lib = None

@@ -1,0 +1,260 @@
+// Batched solves of independent systems on the cluster engine
+// (include/mlsh.h: mlsh_batch_*).
+//
+// Systems are grouped by the cluster size their row count needs and sorted
+// largest first inside a group (longest jobs start first, which bounds the
+// tail).  Each group is one persistent launch of the cluster kernel with as
+// many clusters as fit the device; clusters pull systems from the group's
+// queue.  Groups run on separate streams, largest cluster size first, so
+// when one group's queue drains its SMs are taken by the next group's
+// clusters.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "mlsh_cluster.cuh"
+#include "mlsh_core.cuh"
+
+namespace mlsh {
+
+constexpr int kMaxBatchGroups = 128;
+
+struct BatchGroup {
+  int csize = 1;
+  int rpc = 1024;
+  int first = 0;  // index of the group's first record in the system array
+  int count = 0;
+  cudaStream_t stream = nullptr;
+};
+
+struct Batch {
+  Handle *handle = nullptr;
+  int n_systems = 0;
+  int dtype = MLSH_F64;
+  int64_t total_rows = 0;
+  std::vector<int64_t> row_off;
+  std::vector<int> order[2];  // per kind: record i solves system order[i]
+  const int *row_ptr = nullptr;
+  const int *col_ind = nullptr;
+  const void *val = nullptr;
+  std::vector<BatchGroup> groups[2];  // per kind (CG, BiCGSTAB)
+  ClusterSystem *d_sys = nullptr;     // n_systems records
+  ClusterSystem *h_sys = nullptr;     // pinned mirror
+  unsigned *d_queue = nullptr;        // one counter per group
+  void *ws = nullptr;                 // inverse diagonal + BiCGSTAB r0
+  cudaEvent_t done_event = nullptr;
+};
+
+namespace {
+
+// Groups for one kind: systems by needed cluster size (largest first).
+int build_groups(Batch &B, int kind, std::vector<BatchGroup> &groups,
+                 std::vector<int> &order) {
+  const int n = B.n_systems;
+  std::vector<int> rpc(n), cs(n);
+  for (int k = 0; k < n; ++k) {
+    const int64_t nk = B.row_off[k + 1] - B.row_off[k];
+    // one CTA while the system fits one; otherwise the widest slices
+    int r = cluster_rows_for(kind, B.dtype, nk, 0);
+    if (r == 0) return MLSH_ERR_INVALID_ARG;
+    int single = cluster_rows_for(kind, B.dtype, nk, (int)std::max<int64_t>(nk, 1));
+    if (single > 0 && nk <= single) {
+      r = single;
+    } else {
+      // largest slice that fits: fewer CTAs per system
+      int best = r;
+      for (int t = r; t <= 16384; t <<= 1) {
+        const int ok = cluster_rows_for(kind, B.dtype, nk, t);
+        if (ok == t) best = t;
+      }
+      r = best;
+    }
+    rpc[k] = r;
+    cs[k] = (int)((nk + r - 1) / r);
+    if (cs[k] < 1) cs[k] = 1;
+  }
+  order.resize(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    if (cs[a] != cs[b]) return cs[a] > cs[b];
+    if (rpc[a] != rpc[b]) return rpc[a] > rpc[b];
+    const int64_t na = B.row_off[a + 1] - B.row_off[a];
+    const int64_t nb = B.row_off[b + 1] - B.row_off[b];
+    return na > nb;
+  });
+  groups.clear();
+  for (int i = 0; i < n; ++i) {
+    const int k = order[i];
+    if (groups.empty() || groups.back().csize != cs[k] || groups.back().rpc != rpc[k]) {
+      if ((int)groups.size() == kMaxBatchGroups) return MLSH_ERR_INVALID_ARG;
+      BatchGroup g;
+      g.csize = cs[k];
+      g.rpc = rpc[k];
+      g.first = i;
+      g.count = 0;
+      groups.push_back(g);
+    }
+    ++groups.back().count;
+  }
+  return MLSH_SUCCESS;
+}
+
+void free_batch(Batch &B) {
+  for (auto &gl : B.groups)
+    for (auto &g : gl)
+      if (g.stream) cudaStreamDestroy(g.stream);
+  cudaFree(B.d_sys);
+  cudaFreeHost(B.h_sys);
+  cudaFree(B.d_queue);
+  cudaFree(B.ws);
+  if (B.done_event) cudaEventDestroy(B.done_event);
+}
+
+}  // namespace
+}  // namespace mlsh
+
+struct mlsh_batch_s {
+  mlsh::Batch b;
+};
+
+using namespace mlsh;
+
+extern "C" {
+
+int mlsh_batch_create(mlsh_handle hs, int n_systems, const int64_t *row_off,
+                      const int *d_row_ptr, const int *d_col_ind, const void *d_val, int dtype,
+                      mlsh_batch *out) {
+  if (!hs || !out || n_systems < 0 || (n_systems > 0 && !row_off) || dtype_size(dtype) == 0)
+    return MLSH_ERR_INVALID_ARG;
+  *out = nullptr;
+  auto *bs = new (std::nothrow) mlsh_batch_s();
+  if (!bs) return MLSH_ERR_OOM;
+  Batch &B = bs->b;
+  B.handle = &hs->h;
+  B.n_systems = n_systems;
+  B.dtype = dtype;
+  B.row_off.assign(row_off, row_off + n_systems + 1);
+  B.total_rows = n_systems > 0 ? row_off[n_systems] : 0;
+  for (int k = 0; k < n_systems; ++k)
+    if (row_off[k + 1] < row_off[k]) {
+      delete bs;
+      return MLSH_ERR_INVALID_ARG;
+    }
+  B.row_ptr = d_row_ptr;
+  B.col_ind = d_col_ind;
+  B.val = d_val;
+  // CG grouping now (it also validates the sizes); BiCGSTAB on first use
+  {
+    const int st = build_groups(B, 0, B.groups[0], B.order[0]);
+    if (st != MLSH_SUCCESS) {
+      delete bs;
+      return st;
+    }
+  }
+  const size_t esz = (size_t)dtype_size(dtype);
+  const size_t n_rec = (size_t)std::max(n_systems, 1);
+  bool ok = cudaMalloc(&B.d_sys, sizeof(ClusterSystem) * n_rec) == cudaSuccess &&
+            cudaMallocHost(&B.h_sys, sizeof(ClusterSystem) * n_rec) == cudaSuccess &&
+            cudaMalloc(&B.d_queue, sizeof(unsigned) * kMaxBatchGroups) == cudaSuccess &&
+            cudaMalloc(&B.ws, 2 * esz * (size_t)std::max<int64_t>(B.total_rows, 1) + 256) ==
+                cudaSuccess &&
+            cudaEventCreateWithFlags(&B.done_event, cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    free_batch(B);
+    delete bs;
+    return MLSH_ERR_OOM;
+  }
+  *out = bs;
+  return MLSH_SUCCESS;
+}
+
+int mlsh_batch_destroy(mlsh_batch bs) {
+  if (!bs) return MLSH_ERR_INVALID_ARG;
+  if (bs->b.handle) cudaStreamSynchronize(bs->b.handle->stream);
+  free_batch(bs->b);
+  delete bs;
+  return MLSH_SUCCESS;
+}
+
+int mlsh_batch_solve(mlsh_handle hs, mlsh_batch bs, int kind, const void *d_b, void *d_x,
+                     const double *host_tol, const mlsh_solver_opts *opts, int *host_status,
+                     int64_t *host_iters, double *host_resid) {
+  if (!hs || !bs || !opts || (kind != 0 && kind != 1)) return MLSH_ERR_INVALID_ARG;
+  Batch &B = bs->b;
+  Handle &h = hs->h;
+  if (B.n_systems == 0) return MLSH_SUCCESS;
+  if (!d_b || !d_x) return MLSH_ERR_INVALID_ARG;
+  std::vector<BatchGroup> &groups = B.groups[kind];
+  std::vector<int> &order = B.order[kind];
+  if (groups.empty()) {
+    const int st = build_groups(B, kind, groups, order);
+    if (st != MLSH_SUCCESS) return st;
+  }
+  if ((int)order.size() != B.n_systems) return MLSH_ERR_INVALID_ARG;
+  const size_t esz = (size_t)dtype_size(B.dtype);
+  char *ws = static_cast<char *>(B.ws);
+  const bool jac = opts->precond == MLSH_PRECOND_JACOBI;
+  for (int i = 0; i < B.n_systems; ++i) {
+    const int k = order[i];
+    ClusterSystem &S = B.h_sys[i];
+    std::memset(&S, 0, sizeof(S));
+    const int64_t r0 = B.row_off[k];
+    S.rp = B.row_ptr + r0;
+    S.ci = B.col_ind;
+    S.val = B.val;
+    S.b = static_cast<const char *>(d_b) + r0 * esz;
+    S.x = static_cast<char *>(d_x) + r0 * esz;
+    S.dinv = ws + r0 * esz;
+    S.aux = ws + (B.total_rows + r0) * esz;
+    S.n = (int)(B.row_off[k + 1] - r0);
+    S.tol = host_tol ? host_tol[k] : opts->tol;
+    S.maxiter = opts->maxiter;
+    S.miniter = opts->miniter;
+    S.status = kRunning;
+  }
+  MLSH_CUDA_TRY(cudaMemcpyAsync(B.d_sys, B.h_sys, sizeof(ClusterSystem) * B.n_systems,
+                                cudaMemcpyHostToDevice, h.stream));
+  MLSH_CUDA_TRY(cudaMemsetAsync(B.d_queue, 0, sizeof(unsigned) * kMaxBatchGroups, h.stream));
+  MLSH_CUDA_TRY(cudaEventRecord(B.done_event, h.stream));
+  // one stream per group, ordered after the uploads on the handle's stream
+  const int n_groups = (int)groups.size();
+  for (int gi = 0; gi < n_groups; ++gi) {
+    BatchGroup &g = groups[gi];
+    if (!g.stream) MLSH_CUDA_TRY(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+    MLSH_CUDA_TRY(cudaStreamWaitEvent(g.stream, B.done_event, 0));
+    int n_clusters = cluster_max_active(kind, B.dtype, jac, g.rpc, g.csize);
+    if (n_clusters < 1) return MLSH_NOT_IMPL;
+    n_clusters = std::min(n_clusters, g.count);
+    const int st = cluster_launch(h, kind, B.dtype, jac, B.d_sys + g.first, g.count,
+                                  B.d_queue + gi, g.rpc, g.csize, n_clusters,
+                                  kClusterBudgetSeconds, g.stream);
+    if (st != MLSH_SUCCESS) return st;
+  }
+  for (int gi = 0; gi < n_groups; ++gi) {
+    cudaEvent_t ev;
+    MLSH_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    MLSH_CUDA_TRY(cudaEventRecord(ev, groups[gi].stream));
+    MLSH_CUDA_TRY(cudaStreamWaitEvent(h.stream, ev, 0));
+    cudaEventDestroy(ev);
+  }
+  MLSH_CUDA_TRY(cudaMemcpyAsync(B.h_sys, B.d_sys, sizeof(ClusterSystem) * B.n_systems,
+                                cudaMemcpyDeviceToHost, h.stream));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  int first_bad = MLSH_SUCCESS;
+  for (int i = 0; i < B.n_systems; ++i) {
+    const int k = order[i];
+    const ClusterSystem &S = B.h_sys[i];
+    if (host_status) host_status[k] = S.status;
+    if (host_iters) host_iters[k] = S.iters;
+    if (host_resid) host_resid[k] = S.resid;
+    if (S.status != MLSH_SUCCESS && first_bad == MLSH_SUCCESS) first_bad = S.status;
+  }
+  return first_bad;
+}
+
+}  // extern "C"

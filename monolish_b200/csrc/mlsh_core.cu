@@ -297,6 +297,7 @@ int mlsh_create(mlsh_handle *out) {
             cudaMalloc(&h.err_flag, sizeof(int)) == cudaSuccess &&
             cudaMallocHost(&h.host_state, sizeof(SolverState)) == cudaSuccess &&
             cudaMallocHost(&h.host_scalars, sizeof(double) * 8) == cudaSuccess &&
+            cudaMallocHost(&h.host_cluster, 512) == cudaSuccess &&
             cudaStreamCreateWithFlags(&h.capture_stream, cudaStreamNonBlocking) == cudaSuccess;
   if (ok) {
     ok = cudaMemset(h.counters, 0, sizeof(unsigned) * 8) == cudaSuccess &&
@@ -324,6 +325,7 @@ int mlsh_destroy(mlsh_handle hs) {
   cudaFree(h.err_flag);
   cudaFreeHost(h.host_state);
   cudaFreeHost(h.host_scalars);
+  cudaFreeHost(h.host_cluster);
   if (h.capture_stream) cudaStreamDestroy(h.capture_stream);
   delete hs;
   return MLSH_SUCCESS;

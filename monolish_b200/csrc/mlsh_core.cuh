@@ -25,6 +25,17 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
 int plan_diag(const CsrPlan &p, void *out, bool invert, cudaStream_t stream);
 int plan_inv_diag(CsrPlan &p, cudaStream_t stream, const void **out);
 
+// Cluster engine (mlsh_cluster.cu).  kind: 0 = CG, 1 = BiCGSTAB.
+struct ClusterSystem;
+// Rows per CTA for an n-row system (0 if it does not fit 16 CTAs).
+int cluster_rows_for(int kind, int dtype, int64_t n, int requested);
+// Launches n_clusters clusters of csize CTAs that take systems from
+// d_queue (zero it first) until n_systems are done.
+int cluster_launch(const Handle &h, int kind, int dtype, bool jac, ClusterSystem *d_systems,
+                   int n_systems, unsigned *d_queue, int rpc, int csize, int n_clusters,
+                   double budget_s, cudaStream_t stream);
+int cluster_max_active(int kind, int dtype, bool jac, int rpc, int csize);
+
 // Solver-side resources kept on the handle / plan (mlsh_krylov.cu).
 void release_solver_graphs(Handle &h);
 void release_plan_extras(CsrPlan &p);

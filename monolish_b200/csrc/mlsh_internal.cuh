@@ -102,6 +102,7 @@ struct Handle {
   void *graph_cache = nullptr;        // instantiated solver graphs
   double *hist = nullptr;             // residual history buffer (device)
   long long hist_cap = 0;
+  void *host_cluster = nullptr;       // pinned record for the cluster engine
 };
 
 struct CsrPlan {

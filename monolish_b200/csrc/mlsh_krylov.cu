@@ -25,6 +25,7 @@
 #include <cstring>
 #include <vector>
 
+#include "mlsh_cluster.cuh"
 #include "mlsh_core.cuh"
 
 namespace mlsh {
@@ -571,6 +572,71 @@ int ensure_ws(Handle &h, size_t bytes) {
   return MLSH_SUCCESS;
 }
 
+// One system on the cluster engine.  Returns MLSH_NOT_IMPL when the system
+// does not fit it (the caller then uses the kernel engine).
+int cluster_solve_one(Kind kind, Handle &h, CsrPlan &p, const void *b, void *x,
+                      const mlsh_solver_opts *opts, mlsh_solver_result *res) {
+  const int64_t n = p.n_rows;
+  const int rpc = cluster_rows_for(kind == kCG ? 0 : 1, p.dtype, n, opts->cluster_rows);
+  if (rpc == 0) return MLSH_NOT_IMPL;
+  const int csize = (int)((n + rpc - 1) / rpc);
+  const bool jac = opts->precond == MLSH_PRECOND_JACOBI;
+  const size_t esz = (size_t)dtype_size(p.dtype);
+  const size_t vec = ((size_t)n * esz + 255) / 256 * 256;
+  // workspace: [system record][queue][inverse diagonal][r0]
+  int st = ensure_ws(h, 512 + 2 * vec);
+  if (st != MLSH_SUCCESS) return st;
+  char *ws = static_cast<char *>(h.ws);
+  ClusterSystem *d_sys = reinterpret_cast<ClusterSystem *>(ws);
+  unsigned *d_queue = reinterpret_cast<unsigned *>(ws + 256);
+  const bool want_hist = opts->history != nullptr && opts->history_len > 0;
+  if (want_hist && h.hist_cap < opts->history_len) {
+    if (h.hist) cudaFree(h.hist);
+    h.hist = nullptr;
+    h.hist_cap = 0;
+    if (cudaMalloc(&h.hist, sizeof(double) * (size_t)opts->history_len) != cudaSuccess) {
+      cudaGetLastError();
+      return MLSH_ERR_OOM;
+    }
+    h.hist_cap = opts->history_len;
+  }
+  ClusterSystem *hs = static_cast<ClusterSystem *>(h.host_cluster);
+  std::memset(hs, 0, sizeof(ClusterSystem));
+  hs->rp = p.row_ptr;
+  hs->ci = p.col_ind;
+  hs->val = p.val;
+  hs->b = b;
+  hs->x = x;
+  hs->dinv = ws + 512;
+  hs->aux = ws + 512 + vec;
+  hs->n = (int)n;
+  hs->tol = opts->tol;
+  hs->maxiter = opts->maxiter;
+  hs->miniter = opts->miniter;
+  hs->hist = want_hist ? h.hist : nullptr;
+  hs->hist_cap = want_hist ? opts->history_len : 0;
+  hs->status = kRunning;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(d_sys, hs, sizeof(ClusterSystem), cudaMemcpyHostToDevice,
+                                h.stream));
+  MLSH_CUDA_TRY(cudaMemsetAsync(d_queue, 0, sizeof(unsigned), h.stream));
+  st = cluster_launch(h, kind == kCG ? 0 : 1, p.dtype, jac, d_sys, 1, d_queue, rpc, csize, 1,
+                      kClusterBudgetSeconds, h.stream);
+  if (st != MLSH_SUCCESS) return st;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(hs, d_sys, sizeof(ClusterSystem), cudaMemcpyDeviceToHost,
+                                h.stream));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  res->status = hs->status;
+  res->iters = hs->iters;
+  res->final_resid = hs->resid;
+  if (want_hist) {
+    const int64_t k = std::min<int64_t>(hs->iters, opts->history_len);
+    if (k > 0)
+      MLSH_CUDA_TRY(cudaMemcpy(opts->history, h.hist, sizeof(double) * (size_t)k,
+                               cudaMemcpyDeviceToHost));
+  }
+  return res->status;
+}
+
 int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, void *x,
                  const mlsh_solver_opts *opts, mlsh_solver_result *res) {
   if (!hs || !ps || !opts) return MLSH_ERR_INVALID_ARG;
@@ -587,13 +653,24 @@ int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, voi
   mlsh_solver_result local{};
   if (!res) res = &local;
   if (n == 0) {
-    // nothing to solve: ||r|| = 0 < tol unless tol <= 0
-    res->iters = opts->maxiter > 0 ? 1 : 0;
+    // nothing to solve: ||r|| = 0 < tol from the first iteration on, so the
+    // loop ends at max(1, miniter) unless maxiter comes first or tol <= 0
+    const int64_t need = std::max<int64_t>(1, opts->miniter);
     res->final_resid = 0.0;
-    res->status = (opts->maxiter > 0 && 0.0 < opts->tol && opts->miniter <= 1)
-                      ? MLSH_SUCCESS
-                      : MLSH_SOLVER_MAXITER;
+    if (0.0 < opts->tol && need <= opts->maxiter) {
+      res->iters = need;
+      res->status = MLSH_SUCCESS;
+    } else {
+      res->iters = std::max<int64_t>(0, opts->maxiter);
+      res->status = MLSH_SOLVER_MAXITER;
+    }
     return res->status;
+  }
+  if (opts->engine == MLSH_ENGINE_CLUSTER ||
+      (opts->engine == MLSH_ENGINE_AUTO && opts->maxiter <= kClusterMaxIterAuto)) {
+    const int st = cluster_solve_one(kind, h, p, b, x, opts, res);
+    if (st != MLSH_NOT_IMPL) return st;
+    if (opts->engine == MLSH_ENGINE_CLUSTER) return MLSH_ERR_INVALID_ARG;
   }
   SolveCtx c;
   c.kind = kind;
@@ -728,9 +805,11 @@ int mlsh_solver_opts_default(mlsh_solver_opts *o) {
   o->precond = MLSH_PRECOND_JACOBI;
   o->use_graph = 1;
   o->check_every = 0;
-  o->reserved = 0;
+  o->engine = MLSH_ENGINE_AUTO;
   o->history = nullptr;
   o->history_len = 0;
+  o->cluster_rows = 0;
+  o->reserved = 0;
   return MLSH_SUCCESS;
 }
 

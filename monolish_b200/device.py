@@ -180,24 +180,92 @@ class SolveResult:
     resid: float
 
 
-def _opts(tol, maxiter, miniter, precond, use_graph, check_every):
+def _opts(tol, maxiter, miniter, precond, use_graph, check_every, engine, cluster_rows):
     o = _abi.SolverOpts()
+    _abi.load().mlsh_solver_opts_default(C.byref(o))
     o.tol, o.maxiter, o.miniter = tol, maxiter, miniter
     o.precond = precond
     o.use_graph = 1 if use_graph else 0
     o.check_every = check_every
+    o.engine = engine
+    o.cluster_rows = cluster_rows
     return o
 
 
 def _solve(fn, A: Crs, b, x, tol, maxiter, miniter=0, precond=_abi.PRECOND_JACOBI,
-           use_graph=True, check_every=0):
-    o = _opts(tol, maxiter, miniter, precond, use_graph, check_every)
+           use_graph=True, check_every=0, engine=_abi.ENGINE_AUTO, cluster_rows=0,
+           history=None):
+    o = _opts(tol, maxiter, miniter, precond, use_graph, check_every, engine, cluster_rows)
+    if history is not None:
+        o.history = history.ctypes.data_as(C.POINTER(C.c_double))
+        o.history_len = len(history)
     r = _abi.SolverResult()
     st = fn(A.handle.h, A.plan, ptr(b), ptr(x), C.byref(o), C.byref(r))
     if st not in (_abi.SUCCESS, _abi.SOLVER_MAXITER, _abi.SOLVER_BREAKDOWN,
                   _abi.SOLVER_RESIDUAL_NAN, _abi.SOLVER_SIZE_ERROR):
         raise _abi.MlshError(st, "solve")
     return SolveResult(st, int(r.iters), float(r.final_resid))
+
+
+class Batch:
+    """Independent systems stored as one concatenated CRS (column indices
+    local to each system), solved together by mlsh_batch_solve."""
+
+    def __init__(self, handle: Handle, systems, dtype=np.float64):
+        self.handle = handle
+        self.lib = handle.lib
+        self.dtype = np.dtype(dtype)
+        sizes = np.array([len(rp) - 1 for rp, _, _ in systems], np.int64)
+        self.row_off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        nnz = np.array([int(rp[-1]) for rp, _, _ in systems], np.int64)
+        nnz_off = np.concatenate([[0], np.cumsum(nnz)])
+        total_rows = int(self.row_off[-1])
+        rp_all = np.empty(total_rows + 1, np.int64)
+        for k, (rp, _, _) in enumerate(systems):
+            rp_all[self.row_off[k]:self.row_off[k + 1]] = rp[:-1] + nnz_off[k]
+        rp_all[-1] = nnz_off[-1]
+        if nnz_off[-1] > 2**31 - 1:
+            raise ValueError("concatenated nnz exceeds int32")
+        ci_all = np.concatenate([ci for _, ci, _ in systems]).astype(np.int32)
+        v_all = np.concatenate([v for _, _, v in systems]).astype(self.dtype)
+        dev = torch.device("cuda")
+        self.d_rp = torch.from_numpy(rp_all.astype(np.int32)).to(dev)
+        self.d_ci = torch.from_numpy(ci_all).to(dev)
+        self.d_val = torch.from_numpy(v_all).to(dev)
+        self.n_systems = len(systems)
+        bh = C.c_void_p()
+        _abi.check(self.lib.mlsh_batch_create(
+            handle.h, self.n_systems, self.row_off.ctypes.data_as(C.c_void_p), ptr(self.d_rp),
+            ptr(self.d_ci), ptr(self.d_val), _dtype_code(self.dtype), C.byref(bh)),
+            "batch_create")
+        self.b = bh
+
+    def close(self):
+        if self.b:
+            self.lib.mlsh_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, kind, d_b, d_x, tol, maxiter, miniter=0, precond=_abi.PRECOND_JACOBI):
+        """kind 'cg' or 'bicgstab'; tol: scalar or per-system absolute array."""
+        o = _opts(1e-8, maxiter, miniter, precond, True, 0, _abi.ENGINE_CLUSTER, 0)
+        tol_arr = np.ascontiguousarray(np.broadcast_to(np.asarray(tol, np.float64),
+                                                       (self.n_systems,)))
+        status = np.zeros(self.n_systems, np.int32)
+        iters = np.zeros(self.n_systems, np.int64)
+        resid = np.zeros(self.n_systems, np.float64)
+        st = self.lib.mlsh_batch_solve(
+            self.handle.h, self.b, 0 if kind == "cg" else 1, ptr(d_b), ptr(d_x),
+            tol_arr.ctypes.data_as(C.c_void_p), C.byref(o), status.ctypes.data_as(C.c_void_p),
+            iters.ctypes.data_as(C.c_void_p), resid.ctypes.data_as(C.c_void_p))
+        if st < _abi.NOT_IMPL:
+            raise _abi.MlshError(st, "batch_solve")
+        return status, iters, resid
 
 
 def cg_solve(A: Crs, b, x, tol, maxiter, **kw) -> SolveResult:

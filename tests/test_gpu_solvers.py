@@ -36,14 +36,19 @@ def solve(handle, solver, rp, ci, v, b, x0, tol, maxiter, **kw):
     return r, x
 
 
+ENGINES = {"kernels-graph": dict(engine=_abi.ENGINE_KERNELS, use_graph=True),
+           "kernels-eager": dict(engine=_abi.ENGINE_KERNELS, use_graph=False),
+           "cluster": dict(engine=_abi.ENGINE_CLUSTER)}
+
+
 @pytest.mark.parametrize("name,solver", [("poisson16", "cg"), ("poisson16", "bicgstab"),
                                          ("poisson128", "cg"), ("convdiff10", "bicgstab")])
-@pytest.mark.parametrize("use_graph", [True, False])
-def test_golden_solves(handle, restatement, name, solver, use_graph):
+@pytest.mark.parametrize("engine", sorted(ENGINES))
+def test_golden_solves(handle, restatement, name, solver, engine):
     g = golden(name)
     rp, ci, v, b = g["rp"], g["ci"], g["v"], g["b"]
     tol = float(g["tol"])
-    r, x = solve(handle, solver, rp, ci, v, b, np.zeros_like(b), tol, 2000, use_graph=use_graph)
+    r, x = solve(handle, solver, rp, ci, v, b, np.zeros_like(b), tol, 2000, **ENGINES[engine])
     gst, git, gres = g[solver]
     assert r.status == int(gst) == 0
     slack = 0.10 if (solver == "bicgstab" and name.startswith("poisson")) else 0.02
@@ -54,12 +59,67 @@ def test_golden_solves(handle, restatement, name, solver, use_graph):
     assert r.resid < tol
 
 
-def test_poisson128_cg_matches_reference_exactly(handle):
+@pytest.mark.parametrize("engine", sorted(ENGINES))
+def test_poisson128_cg_matches_reference_exactly(handle, engine):
     """The 128x128 Jacobi-CG workload: 382 iterations, as the reference."""
     g = golden("poisson128")
     r, x = solve(handle, "cg", g["rp"], g["ci"], g["v"], g["b"], np.zeros(16384),
-                 float(g["tol"]), 2000)
+                 float(g["tol"]), 2000, **ENGINES[engine])
     assert r.status == 0 and r.iters == 382
+
+
+@pytest.mark.parametrize("solver", ["cg", "bicgstab"])
+@pytest.mark.parametrize("rows", [1024, 2048, 4096])
+def test_cluster_partitions(handle, restatement, solver, rows):
+    """The cluster engine on 16, 8 and 4 CTAs (rows per CTA 1024..4096)."""
+    if solver == "cg":
+        g = golden("poisson128")
+        rp, ci, v, b = g["rp"], g["ci"], g["v"], g["b"]
+        tol = float(g["tol"])
+        want = int(g["cg"][1])
+    else:
+        n, rp, ci, v = W.convdiff3d(24, peclet=10.0)
+        b = restatement.spmv(rp, ci, v, W.uniform_mt(n, -1, 1, 2))
+        tol = 1e-10 * np.linalg.norm(b)
+        want = restatement.bicgstab(rp, ci, v, b, np.zeros(n), tol, 3000)[1]
+    r, x = solve(handle, solver, rp, ci, v, b, np.zeros_like(b), tol, 3000,
+                 engine=_abi.ENGINE_CLUSTER, cluster_rows=rows)
+    assert r.status == 0
+    assert abs(r.iters - want) <= max(1, int(0.02 * want))
+    assert restatement.true_relres(rp, ci, v, b, x) < 1e-10
+
+
+def test_cluster_rejects_too_large(handle):
+    import torch
+    from monolish_b200 import device as D
+    n, rp, ci, v = W.poisson2d(400)  # 160,000 rows > 16 CTAs x 8192
+    A = D.Crs(handle, n, n, rp, ci, v)
+    d = torch.zeros(n, dtype=torch.float64, device="cuda")
+    with pytest.raises(_abi.MlshError):
+        D.cg_solve(A, d, d, 1e-8, 10, engine=_abi.ENGINE_CLUSTER)
+    A.close()
+
+
+@pytest.mark.parametrize("solver", ["cg", "bicgstab"])
+def test_history_both_engines(handle, restatement, solver):
+    n, rp, ci, v = W.vardiff2d(40, 33, 3, 2)
+    b = restatement.spmv(rp, ci, v, W.uniform_mt(n, -1, 1, 4))
+    tol = 1e-10 * np.linalg.norm(b)
+    out = {}
+    for name in ("kernels-graph", "cluster"):
+        hist = np.full(5000, np.nan)
+        r, _ = solve(handle, solver, rp, ci, v, b, np.zeros(n), tol, 5000, history=hist,
+                     **ENGINES[name])
+        assert r.status == 0
+        h = hist[:r.iters]
+        assert np.isfinite(h).all() and np.isnan(hist[r.iters:]).all()
+        assert h[-1] == r.resid and h[-1] < tol
+        out[name] = (r.iters, h)
+    (i1, h1), (i2, h2) = out["kernels-graph"], out["cluster"]
+    assert abs(i1 - i2) <= max(1, int(0.02 * i1))
+    # the engines sum in different orders; the early history agrees closely
+    k = min(i1, i2, 15)
+    np.testing.assert_allclose(h1[:k], h2[:k], rtol=1e-6)
 
 
 @pytest.mark.parametrize("solver", ["cg", "bicgstab"])
@@ -89,31 +149,33 @@ def test_bicgstab_convdiff_vs_oracle(handle, restatement):
 
 
 @pytest.mark.parametrize("solver", ["cg", "bicgstab"])
-def test_status_codes_match_oracle(handle, restatement, solver):
+@pytest.mark.parametrize("engine", ["kernels-graph", "cluster"])
+def test_status_codes_match_oracle(handle, restatement, solver, engine):
+    kw = ENGINES[engine]
     n, rp, ci, v = W.poisson2d(8)
     # b = 0, x0 = 0: CG -> NaN residual, BiCGSTAB -> breakdown
     st, it, _, _ = getattr(restatement, solver)(rp, ci, v, np.zeros(n), np.zeros(n), 1e-10, 100)
-    r, _ = solve(handle, solver, rp, ci, v, np.zeros(n), np.zeros(n), 1e-10, 100)
+    r, _ = solve(handle, solver, rp, ci, v, np.zeros(n), np.zeros(n), 1e-10, 100, **kw)
     assert (r.status, r.iters) == (st, it)
     # maxiter
     b = restatement.spmv(rp, ci, v, np.ones(n))
-    r, _ = solve(handle, solver, rp, ci, v, b, np.zeros(n), 1e-30, 5)
+    r, _ = solve(handle, solver, rp, ci, v, b, np.zeros(n), 1e-30, 5, **kw)
     assert (r.status, r.iters) == (_abi.SOLVER_MAXITER, 5)
     # NaN in b
     bn = b.copy()
     bn[3] = np.nan
     st, it, _, _ = getattr(restatement, solver)(rp, ci, v, bn, np.zeros(n), 1e-10, 100)
-    r, _ = solve(handle, solver, rp, ci, v, bn, np.zeros(n), 1e-10, 100)
+    r, _ = solve(handle, solver, rp, ci, v, bn, np.zeros(n), 1e-10, 100, **kw)
     assert (r.status, r.iters) == (st, it)
     # miniter holds the loop open past convergence
     n, rp, ci, v = W.poisson2d(30)
     b = restatement.spmv(rp, ci, v, np.ones(n))
     t = 0.5 * np.linalg.norm(b)
     st, it, _, _ = getattr(restatement, solver)(rp, ci, v, b, np.zeros(n), t, 100, miniter=25)
-    r, _ = solve(handle, solver, rp, ci, v, b, np.zeros(n), t, 100, miniter=25)
+    r, _ = solve(handle, solver, rp, ci, v, b, np.zeros(n), t, 100, miniter=25, **kw)
     assert (r.status, r.iters) == (st, it) == (0, 25)
     # maxiter = 0
-    r, _ = solve(handle, solver, rp, ci, v, b, np.zeros(n), 1e-3, 0)
+    r, _ = solve(handle, solver, rp, ci, v, b, np.zeros(n), 1e-3, 0, **kw)
     assert r.status == _abi.SOLVER_MAXITER and r.iters == 0
 
 
@@ -126,8 +188,9 @@ def test_zero_diagonal_jacobi_gives_nan_status(handle, restatement):
     v[idx] = 0.0
     b = np.ones(n)
     st, it, _, _ = restatement.cg(rp, ci, v, b, np.zeros(n), 1e-10, 100)
-    r, _ = solve(handle, "cg", rp, ci, v, b, np.zeros(n), 1e-10, 100)
-    assert (r.status, r.iters) == (st, it) == (_abi.SOLVER_RESIDUAL_NAN, 1)
+    for kw in (ENGINES["kernels-graph"], ENGINES["cluster"]):
+        r, _ = solve(handle, "cg", rp, ci, v, b, np.zeros(n), 1e-10, 100, **kw)
+        assert (r.status, r.iters) == (st, it) == (_abi.SOLVER_RESIDUAL_NAN, 1)
 
 
 def test_graph_and_eager_identical(handle):
@@ -135,9 +198,11 @@ def test_graph_and_eager_identical(handle):
     b = np.random.default_rng(0).uniform(-1, 1, n)
     tol = 1e-10 * np.linalg.norm(b)
     for solver in ("cg", "bicgstab"):
-        r1, x1 = solve(handle, solver, rp, ci, v, b, np.zeros(n), tol, 5000, use_graph=True)
-        r2, x2 = solve(handle, solver, rp, ci, v, b, np.zeros(n), tol, 5000, use_graph=False)
-        r3, x3 = solve(handle, solver, rp, ci, v, b, np.zeros(n), tol, 5000, use_graph=True)
+        kw = dict(engine=_abi.ENGINE_KERNELS)
+        r1, x1 = solve(handle, solver, rp, ci, v, b, np.zeros(n), tol, 5000, use_graph=True, **kw)
+        r2, x2 = solve(handle, solver, rp, ci, v, b, np.zeros(n), tol, 5000, use_graph=False,
+                       **kw)
+        r3, x3 = solve(handle, solver, rp, ci, v, b, np.zeros(n), tol, 5000, use_graph=True, **kw)
         assert r1.iters == r2.iters == r3.iters
         assert np.array_equal(x1, x2) and np.array_equal(x1, x3)
 
