@@ -365,13 +365,36 @@ def run_solve(args, wl, rank, world, local):
     db = torch.from_numpy(b).cuda()
     dx = torch.zeros(n, dtype=torch.float64, device="cuda")
     base_fn = D.cg_solve if wl["kind"] == "cg" else D.bicgstab_solve
+    mixed_fn = D.cg_solve_mixed if wl["kind"] == "cg" else D.bicgstab_solve_mixed
     engine = {"auto": 0, "kernels": 1, "cluster": 2}[args.engine]
 
-    def fn(A_, b_, x_, tol_, maxiter_):
+    def plain_fn(A_, b_, x_, tol_, maxiter_):
         return base_fn(A_, b_, x_, tol_, maxiter_, engine=engine,
                        cluster_rows=args.cluster_rows)
 
+    def fn(A_, b_, x_, tol_, maxiter_):
+        if args.precision == "mixed":
+            return mixed_fn(A_, b_, x_, tol_, maxiter_, inner_tol=1e-4, engine=engine)
+        return plain_fn(A_, b_, x_, tol_, maxiter_)
+
     stream = torch.cuda.current_stream()
+    # the plain FP64 solve, timed beside the mixed one for the speed-up
+    plain_ms = None
+    if args.precision == "mixed" and not args.quick:
+        for _ in range(args.warmup):
+            dx.zero_()
+            rp_res = plain_fn(A, db, dx, tol, 20000)
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(args.steps):
+            dx.zero_()
+            rp_res = plain_fn(A, db, dx, tol, 20000)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = p0.elapsed_time(p1) / args.steps
+        plain_rel = port.true_relres(rp, ci, v, b, dx.cpu().numpy())
     for _ in range(args.warmup):
         dx.zero_()
         r = fn(A, db, dx, tol, 20000)
@@ -433,6 +456,17 @@ def run_solve(args, wl, rank, world, local):
                          "note": "whole-solve algorithmic bytes (fused minimum) / solve time"},
             "gpu_launches": args.steps * (r.iters * (3 if wl["kind"] == "cg" else 5) + 3),
         }
+        if args.precision == "mixed":
+            out["dtype"] = "f32 inner / f64 refinement"
+            out["config"]["precision"] = "mixed: FP32 inner (tol 1e-4 rel), FP64 outer"
+            out["config"]["outer_steps"] = r.outer
+            out["roofline"]["note"] = ("FP64-equivalent algorithmic bytes of the plain solve's "
+                                       "iteration count would differ; see speedup_vs_plain")
+            if plain_ms is not None:
+                out["plain_fp64"] = {"value": round(1e3 / plain_ms, 3), "unit": "solves/s",
+                                     "iters": rp_res.iters, "true_rel_residual": plain_rel,
+                                     "speedup_of_mixed": round(plain_ms / (ms / args.steps),
+                                                               3)}
         if world == 1 and not args.no_cpu:
             ref = oracle.reference_or_none()
             if ref is not None:
@@ -700,6 +734,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--size", type=int, default=0,
                     help="override the grid edge (n for zipf); for small profiling cases")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="solver workloads: plain FP64 or FP32-inner/FP64-refinement")
     ap.add_argument("--engine", choices=["auto", "kernels", "cluster"], default="auto",
                     help="solve engine for the solver workloads")
     ap.add_argument("--cluster-rows", type=int, default=0,

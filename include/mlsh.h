@@ -231,8 +231,8 @@ typedef struct {
 
 typedef struct {
   int status;          /* MLSH_SUCCESS / MLSH_SOLVER_MAXITER / ... */
-  int reserved;
-  int64_t iters;       /* solver::get_final_iter */
+  int outer_iters;     /* mixed-precision solves: refinement steps; else 0 */
+  int64_t iters;       /* solver::get_final_iter (mixed: inner iterations) */
   double final_resid;  /* solver::get_final_residual = ||r||_2 (absolute) */
 } mlsh_solver_result;
 
@@ -254,6 +254,26 @@ int mlsh_bicgstab_solve(mlsh_handle handle, mlsh_csr_plan plan,
                         const void *d_b, void *d_x,
                         const mlsh_solver_opts *opts,
                         mlsh_solver_result *result);
+
+/* Mixed precision (no reference counterpart; the reference solves in the
+ * matrix's own precision): FP32 inner CG / BiCGSTAB iterations on an FP32
+ * copy of an FP64 plan's values (with 16-bit column offsets when every row
+ * tile's columns span < 65,536), inside an FP64 iterative-refinement loop
+ * that computes the true residual r = b - A x and the update x += d in
+ * FP64.  opts->tol is the absolute threshold on that true residual;
+ * inner_tol (0 < inner_tol < 1) is the inner solves' relative tolerance;
+ * opts->maxiter bounds the total inner iterations.  result->iters counts
+ * inner iterations, result->outer_iters the refinement steps, and
+ * opts->history (if given) receives the true residual per outer step.
+ * The FP32 copy is derived on the first call and kept with the plan until
+ * its values change (mlsh_csr_plan_values_changed). */
+int mlsh_cg_solve_mixed(mlsh_handle handle, mlsh_csr_plan plan, const void *d_b,
+                        void *d_x, const mlsh_solver_opts *opts, double inner_tol,
+                        mlsh_solver_result *result);
+int mlsh_bicgstab_solve_mixed(mlsh_handle handle, mlsh_csr_plan plan,
+                              const void *d_b, void *d_x,
+                              const mlsh_solver_opts *opts, double inner_tol,
+                              mlsh_solver_result *result);
 
 /* ------------------------------------------------------ batched solves -- */
 /* Thousands of independent, uneven systems solved together (no reference

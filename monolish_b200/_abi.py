@@ -48,7 +48,7 @@ ENGINE_CLUSTER = 2
 
 
 class SolverResult(C.Structure):
-    _fields_ = [("status", i32), ("reserved", i32), ("iters", i64), ("final_resid", f64)]
+    _fields_ = [("status", i32), ("outer_iters", i32), ("iters", i64), ("final_resid", f64)]
 
 
 # name -> (restype, argtypes); every symbol include/mlsh.h declares
@@ -92,6 +92,10 @@ SIGNATURES = {
     "mlsh_cg_solve": (i32, [vp, vp, vp, vp, C.POINTER(SolverOpts), C.POINTER(SolverResult)]),
     "mlsh_bicgstab_solve": (i32, [vp, vp, vp, vp, C.POINTER(SolverOpts),
                                   C.POINTER(SolverResult)]),
+    "mlsh_cg_solve_mixed": (i32, [vp, vp, vp, vp, C.POINTER(SolverOpts), f64,
+                                  C.POINTER(SolverResult)]),
+    "mlsh_bicgstab_solve_mixed": (i32, [vp, vp, vp, vp, C.POINTER(SolverOpts), f64,
+                                        C.POINTER(SolverResult)]),
     "mlsh_batch_create": (i32, [vp, i32, vp, vp, vp, vp, i32, C.POINTER(vp)]),
     "mlsh_batch_destroy": (i32, [vp]),
     "mlsh_batch_solve": (i32, [vp, vp, i32, vp, vp, vp, C.POINTER(SolverOpts), vp, vp, vp]),

@@ -60,21 +60,22 @@ void build_tiles(const int *rp, int n_rows, std::vector<Tile> &tiles,
 }
 
 // Every (type, dot modes, variant) instantiation of the SpMV kernel.
-template <typename VT, int M0, int M1, int V>
+template <typename VT, int M0, int M1, int V, bool C16 = false>
 static constexpr auto spmv_kernel_ptr() {
-  return spmv_tiles_kernel<VT, VT, M0, M1, kSpmvVariants[V].stages, kSpmvVariants[V].min_blocks>;
+  return spmv_tiles_kernel<VT, VT, M0, M1, kSpmvVariants[V].stages, kSpmvVariants[V].min_blocks,
+                           C16>;
 }
 
-template <typename VT, int V>
+template <typename VT, int V, bool C16 = false>
 static constexpr int spmv_smem_bytes() {
-  return SpmvSmem<VT, kSpmvVariants[V].stages>::kBytes;
+  return SpmvSmem<VT, kSpmvVariants[V].stages, C16 ? 2 : 4>::kBytes;
 }
 
-template <typename VT, int M0, int M1, int V>
+template <typename VT, int M0, int M1, int V, bool C16 = false>
 static int set_spmv_smem_one() {
-  const cudaError_t e = cudaFuncSetAttribute(spmv_kernel_ptr<VT, M0, M1, V>(),
+  const cudaError_t e = cudaFuncSetAttribute(spmv_kernel_ptr<VT, M0, M1, V, C16>(),
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             spmv_smem_bytes<VT, V>());
+                                             spmv_smem_bytes<VT, V, C16>());
   if (e != cudaSuccess) {
     set_last_error("cudaFuncSetAttribute(spmv)", e);
     return MLSH_ERR_CUDA;
@@ -88,6 +89,12 @@ static int set_spmv_smem() {
   if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 1>();
   if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 2>();
   if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 3>();
+  if constexpr (sizeof(VT) == 4) {
+    if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 0, true>();
+    if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 1, true>();
+    if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 2, true>();
+    if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 3, true>();
+  }
   return s;
 }
 
@@ -146,6 +153,8 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
   SpmvArgs<VT, VT> a;
   a.row_ptr = p.row_ptr;
   a.col = p.col_ind;
+  a.col16 = p.col16;
+  a.tile_base = p.tile_base;
   a.val = static_cast<const VT *>(p.val);
   a.tiles = p.tiles;
   a.n_tiles = p.n_tiles;
@@ -168,6 +177,29 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
   a.err = h.err_flag;
   const int v = p.variant;
   const int g = p.spmv_grid[v];
+  if constexpr (sizeof(VT) == 4) {
+    if (p.col16 != nullptr) {
+      switch (v) {
+        case 1:
+          spmv_kernel_ptr<VT, M0, M1, 1, true>()
+              <<<g, kSpmvThreads, spmv_smem_bytes<VT, 1, true>(), stream>>>(a);
+          break;
+        case 2:
+          spmv_kernel_ptr<VT, M0, M1, 2, true>()
+              <<<g, kSpmvThreads, spmv_smem_bytes<VT, 2, true>(), stream>>>(a);
+          break;
+        case 3:
+          spmv_kernel_ptr<VT, M0, M1, 3, true>()
+              <<<g, kSpmvThreads, spmv_smem_bytes<VT, 3, true>(), stream>>>(a);
+          break;
+        default:
+          spmv_kernel_ptr<VT, M0, M1, 0, true>()
+              <<<g, kSpmvThreads, spmv_smem_bytes<VT, 0, true>(), stream>>>(a);
+          break;
+      }
+      return cudaGetLastError();
+    }
+  }
   switch (v) {
     case 1:
       spmv_kernel_ptr<VT, M0, M1, 1>()<<<g, kSpmvThreads, spmv_smem_bytes<VT, 1>(), stream>>>(a);
@@ -481,6 +513,8 @@ int mlsh_csr_plan_destroy(mlsh_csr_plan ps) {
   cudaFree(p.long_cnt);
   cudaFree(p.long_dot);
   cudaFree(p.inv_diag);
+  cudaFree(p.col16);
+  cudaFree(p.tile_base);
   release_plan_extras(p);
   delete ps;
   return MLSH_SUCCESS;

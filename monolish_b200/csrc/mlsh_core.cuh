@@ -36,6 +36,10 @@ int cluster_launch(const Handle &h, int kind, int dtype, bool jac, ClusterSystem
                    double budget_s, cudaStream_t stream);
 int cluster_max_active(int kind, int dtype, bool jac, int rpc, int csize);
 
+// Mixed-precision data kept with an FP64 plan (mlsh_mixed.cu).
+void mixed_release(CsrPlan &p);
+void mixed_invalidate(CsrPlan &p);
+
 // Solver-side resources kept on the handle / plan (mlsh_krylov.cu).
 void release_solver_graphs(Handle &h);
 void release_plan_extras(CsrPlan &p);

@@ -787,9 +787,10 @@ void release_solver_graphs(Handle &h) {
 
 void release_plan_extras(CsrPlan &p) {
   if (p.handle) purge_graphs(*p.handle, &p, nullptr);
+  mixed_release(p);
 }
 
-void invalidate_plan_extras(CsrPlan &) {}
+void invalidate_plan_extras(CsrPlan &p) { mixed_invalidate(p); }
 
 }  // namespace mlsh
 

@@ -63,6 +63,9 @@ template <typename VT, typename XT>
 struct SpmvArgs {
   const int *row_ptr;
   const int *col;
+  // 16-bit column format: col16[j] = col[j] - tile_base[tile of j]
+  const uint16_t *col16;
+  const int *tile_base;
   const VT *val;
   const Tile *tiles;
   int n_tiles;
@@ -85,10 +88,10 @@ struct SpmvArgs {
   int *err;         // set to MLSH_ERR_TIMEOUT if a wait gives up
 };
 
-template <typename VT, int STAGES>
+template <typename VT, int STAGES, int CSZ = 4>
 struct SpmvSmem {
   static constexpr int kValBytes = ((kTileNnz * (int)sizeof(VT) + 16) + 15) & ~15;
-  static constexpr int kColBytes = ((kTileNnz * 4 + 16) + 15) & ~15;
+  static constexpr int kColBytes = ((kTileNnz * CSZ + 16) + 15) & ~15;
   static constexpr int kStageBytes = kValBytes + kColBytes;
   static constexpr int kYsOff = STAGES * kStageBytes;
   static constexpr int kSegSumOff = kYsOff + kTileRows * (int)sizeof(VT) + 16;
@@ -155,11 +158,14 @@ __device__ __forceinline__ uint32_t stage_range(const E *arr, int nb, int ne, E 
   return (uint32_t)(i1 - i0);
 }
 
-template <typename VT, typename XT, int M0, int M1, int STAGES, int MINB>
+// C16: columns stored as 16-bit offsets from a per-tile base (2 bytes per
+// nonzero instead of 4) -- the plan picks it when every tile's columns span
+// fewer than 65,536 values.
+template <typename VT, typename XT, int M0, int M1, int STAGES, int MINB, bool C16 = false>
 __global__ void __launch_bounds__(kSpmvThreads, MINB)
     spmv_tiles_kernel(const SpmvArgs<VT, XT> a) {
   constexpr int NR = (M0 != kDotNone ? 1 : 0) + (M1 != kDotNone ? 1 : 0);
-  using L = SpmvSmem<VT, STAGES>;
+  using L = SpmvSmem<VT, STAGES, C16 ? 2 : 4>;
   extern __shared__ __align__(128) unsigned char smem[];
   if (a.done != nullptr && *a.done != 0) return;
 
@@ -213,10 +219,19 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
       const Tile tl = a.tiles[t];
       unsigned char *st = smem + s * L::kStageBytes;
       VT *sv = reinterpret_cast<VT *>(st);
-      int *sc = reinterpret_cast<int *>(st + L::kValBytes);
       const uint32_t bar = full0 + 8 * s;
       const uint32_t vb = stage_range<VT>(a.val, tl.nnz_begin, tl.nnz_end, sv, lane);
-      const uint32_t cb = stage_range<int>(a.col, tl.nnz_begin, tl.nnz_end, sc, lane);
+      uint32_t cb;
+      const void *col_src;
+      if constexpr (C16) {
+        cb = stage_range<uint16_t>(a.col16, tl.nnz_begin, tl.nnz_end,
+                                   reinterpret_cast<uint16_t *>(st + L::kValBytes), lane);
+        col_src = a.col16 + tl.nnz_begin;
+      } else {
+        cb = stage_range<int>(a.col, tl.nnz_begin, tl.nnz_end,
+                              reinterpret_cast<int *>(st + L::kValBytes), lane);
+        col_src = a.col + tl.nnz_begin;
+      }
       __threadfence_block();
       __syncwarp();
       if (lane == 0) {
@@ -229,8 +244,8 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
                         stream_policy);
         }
         if (cb) {
-          const uintptr_t i0 = ((uintptr_t)(a.col + tl.nnz_begin) + 15) & ~(uintptr_t)15;
-          const uintptr_t lo = (uintptr_t)(a.col + tl.nnz_begin) & ~(uintptr_t)15;
+          const uintptr_t i0 = ((uintptr_t)col_src + 15) & ~(uintptr_t)15;
+          const uintptr_t lo = (uintptr_t)col_src & ~(uintptr_t)15;
           bulk_g2s_hint(smem_addr(st + L::kValBytes) + (uint32_t)(i0 - lo), (const void *)i0,
                         cb, bar, stream_policy);
         }
@@ -288,6 +303,7 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
       g0 = __ldg(a.row_ptr + rb + ct);
       g1 = __ldg(a.row_ptr + rb + ct + 1);
     }
+    const int col_base = C16 ? __ldg(a.tile_base + t) : 0;
     if (ct == 0) {
       if (!mbar_wait_bounded(full0 + 8 * s, (uint32_t)((k / STAGES) & 1), kWaitLimitNs)) {
         flags[kFlagConsAbort] = 1;
@@ -300,16 +316,26 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
     const int nb = tl.nnz_begin, ne = tl.nnz_end, nt = ne - nb;
     unsigned char *st = smem + s * L::kStageBytes;
     VT *v = reinterpret_cast<VT *>(st) + head_elems(a.val, nb);
-    const int *c = reinterpret_cast<const int *>(st + L::kValBytes) + head_elems(a.col, nb);
 
     // pass A: products in place
     {
       int cc[kPer];
       XT xx[kPer];
+      if constexpr (C16) {
+        const uint16_t *c = reinterpret_cast<const uint16_t *>(st + L::kValBytes) +
+                            head_elems(a.col16, nb);
 #pragma unroll
-      for (int u = 0; u < kPer; ++u) {
-        const int j = ct + u * kConsumers;
-        cc[u] = (j < nt) ? c[j] : 0;
+        for (int u = 0; u < kPer; ++u) {
+          const int j = ct + u * kConsumers;
+          cc[u] = (j < nt) ? col_base + (int)c[j] : 0;
+        }
+      } else {
+        const int *c = reinterpret_cast<const int *>(st + L::kValBytes) + head_elems(a.col, nb);
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+          const int j = ct + u * kConsumers;
+          cc[u] = (j < nt) ? c[j] : 0;
+        }
       }
 #pragma unroll
       for (int u = 0; u < kPer; ++u) {

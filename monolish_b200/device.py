@@ -178,6 +178,7 @@ class SolveResult:
     status: int
     iters: int
     resid: float
+    outer: int = 0
 
 
 def _opts(tol, maxiter, miniter, precond, use_graph, check_every, engine, cluster_rows):
@@ -204,7 +205,31 @@ def _solve(fn, A: Crs, b, x, tol, maxiter, miniter=0, precond=_abi.PRECOND_JACOB
     if st not in (_abi.SUCCESS, _abi.SOLVER_MAXITER, _abi.SOLVER_BREAKDOWN,
                   _abi.SOLVER_RESIDUAL_NAN, _abi.SOLVER_SIZE_ERROR):
         raise _abi.MlshError(st, "solve")
-    return SolveResult(st, int(r.iters), float(r.final_resid))
+    return SolveResult(st, int(r.iters), float(r.final_resid), int(r.outer_iters))
+
+
+def _solve_mixed(fn, A: Crs, b, x, tol, maxiter, inner_tol=1e-4, miniter=0,
+                 precond=_abi.PRECOND_JACOBI, engine=_abi.ENGINE_AUTO, history=None):
+    o = _opts(tol, maxiter, miniter, precond, True, 0, engine, 0)
+    if history is not None:
+        o.history = history.ctypes.data_as(C.POINTER(C.c_double))
+        o.history_len = len(history)
+    r = _abi.SolverResult()
+    st = fn(A.handle.h, A.plan, ptr(b), ptr(x), C.byref(o), inner_tol, C.byref(r))
+    if st not in (_abi.SUCCESS, _abi.SOLVER_MAXITER, _abi.SOLVER_BREAKDOWN,
+                  _abi.SOLVER_RESIDUAL_NAN, _abi.SOLVER_SIZE_ERROR):
+        raise _abi.MlshError(st, "mixed solve")
+    return SolveResult(st, int(r.iters), float(r.final_resid), int(r.outer_iters))
+
+
+def cg_solve_mixed(A: Crs, b, x, tol, maxiter, **kw) -> SolveResult:
+    """FP32 inner CG inside FP64 iterative refinement (A must be FP64)."""
+    return _solve_mixed(A.lib.mlsh_cg_solve_mixed, A, b, x, tol, maxiter, **kw)
+
+
+def bicgstab_solve_mixed(A: Crs, b, x, tol, maxiter, **kw) -> SolveResult:
+    """FP32 inner BiCGSTAB inside FP64 iterative refinement (A must be FP64)."""
+    return _solve_mixed(A.lib.mlsh_bicgstab_solve_mixed, A, b, x, tol, maxiter, **kw)
 
 
 class Batch:
