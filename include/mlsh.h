@@ -307,6 +307,70 @@ int mlsh_batch_solve(mlsh_handle handle, mlsh_batch batch, int kind, const void 
                      void *d_x, const double *host_tol, const mlsh_solver_opts *opts,
                      int *host_status, int64_t *host_iters, double *host_resid);
 
+/* ------------------------------------------------------------- serving -- */
+/* A solve server (no reference counterpart): requests of different sizes
+ * are submitted from any host thread while others run; a scheduler thread
+ * admits them in arrival order while their device-memory footprint fits
+ * the budget, uploads them, and runs them concurrently:
+ *   - plain-FP64 requests that fit a 16-CTA cluster (n <= 65,536) go to
+ *     persistent cluster kernels that claim work from a ring the host
+ *     publishes into while they run (continuous batching: a finished
+ *     cluster retires its system and takes the next one mid-flight);
+ *   - larger or mixed-precision requests run on worker lanes (one handle
+ *     and stream each), overlapping with the cluster kernels and each other.
+ * A request's host arrays (row_ptr, col_ind, val, b, x0) must stay valid
+ * until the request completes; x_out receives the solution. */
+#define MLSH_PENDING 1 /* mlsh_server_poll: not finished yet */
+
+typedef struct mlsh_server_s *mlsh_server;
+
+typedef struct {
+  int kind;            /* 0 CG, 1 BiCGSTAB */
+  int precision;       /* 0 plain FP64, 1 mixed FP32/FP64 */
+  int precond;         /* MLSH_PRECOND_* */
+  int n;               /* rows = columns */
+  int nnz;
+  int reserved;
+  const int *row_ptr;  /* host CRS (0-based) */
+  const int *col_ind;
+  const double *val;
+  const double *b;     /* host right-hand side */
+  const double *x0;    /* host initial guess, or NULL for zeros */
+  double *x_out;       /* host buffer for the solution, or NULL */
+  double tol;          /* absolute ||r|| threshold */
+  int64_t maxiter;
+  double inner_tol;    /* mixed precision: inner relative tolerance */
+} mlsh_request;
+
+typedef struct {
+  int status;
+  int path;            /* 0 cluster ring, 1 worker lane */
+  int64_t iters;
+  double resid;
+  double t_submit;     /* seconds on the server's steady clock */
+  double t_admit;
+  double t_done;
+} mlsh_request_result;
+
+/* memory_budget_bytes: device bytes the admitted requests may hold;
+ * n_lanes: worker lanes for large / mixed requests (>= 1). */
+int mlsh_server_create(size_t memory_budget_bytes, int n_lanes, mlsh_server *server);
+int mlsh_server_submit(mlsh_server server, const mlsh_request *request,
+                       int64_t *request_id);
+/* poll: MLSH_SUCCESS and the result when done, MLSH_PENDING otherwise;
+ * wait blocks until done.  A returned result releases the request id (a
+ * later poll or wait on it is MLSH_ERR_INVALID_ARG). */
+int mlsh_server_poll(mlsh_server server, int64_t request_id, mlsh_request_result *result);
+int mlsh_server_wait(mlsh_server server, int64_t request_id, mlsh_request_result *result);
+/* Blocks until every submitted request has completed. */
+int mlsh_server_drain(mlsh_server server);
+/* Seconds on the server's steady clock (the clock of the result times). */
+double mlsh_server_now(mlsh_server server);
+/* Counters since creation: serving-kernel launches (each runs until its
+ * ring stays empty for a short idle period) and requests solved on lanes. */
+int mlsh_server_stats(mlsh_server server, int64_t *ring_launches, int64_t *lane_solves);
+int mlsh_server_destroy(mlsh_server server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,6 +23,7 @@ ERR_INVALID_CSR = -22
 ERR_OOM = -23
 ERR_TIMEOUT = -24
 ERR_NO_DEVICE = -25
+PENDING = 1
 
 F64 = 0
 F32 = 1
@@ -49,6 +50,17 @@ ENGINE_CLUSTER = 2
 
 class SolverResult(C.Structure):
     _fields_ = [("status", i32), ("outer_iters", i32), ("iters", i64), ("final_resid", f64)]
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", i32), ("precision", i32), ("precond", i32), ("n", i32), ("nnz", i32),
+                ("reserved", i32), ("row_ptr", vp), ("col_ind", vp), ("val", vp), ("b", vp),
+                ("x0", vp), ("x_out", vp), ("tol", f64), ("maxiter", i64), ("inner_tol", f64)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", i32), ("path", i32), ("iters", i64), ("resid", f64),
+                ("t_submit", f64), ("t_admit", f64), ("t_done", f64)]
 
 
 # name -> (restype, argtypes); every symbol include/mlsh.h declares
@@ -99,6 +111,14 @@ SIGNATURES = {
     "mlsh_batch_create": (i32, [vp, i32, vp, vp, vp, vp, i32, C.POINTER(vp)]),
     "mlsh_batch_destroy": (i32, [vp]),
     "mlsh_batch_solve": (i32, [vp, vp, i32, vp, vp, vp, C.POINTER(SolverOpts), vp, vp, vp]),
+    "mlsh_server_create": (i32, [C.c_size_t, i32, C.POINTER(vp)]),
+    "mlsh_server_submit": (i32, [vp, C.POINTER(Request), C.POINTER(i64)]),
+    "mlsh_server_poll": (i32, [vp, i64, C.POINTER(RequestResult)]),
+    "mlsh_server_wait": (i32, [vp, i64, C.POINTER(RequestResult)]),
+    "mlsh_server_drain": (i32, [vp]),
+    "mlsh_server_now": (f64, [vp]),
+    "mlsh_server_stats": (i32, [vp, C.POINTER(i64), C.POINTER(i64)]),
+    "mlsh_server_destroy": (i32, [vp]),
 }
 
 _lib = None

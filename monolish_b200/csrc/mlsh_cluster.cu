@@ -1,6 +1,14 @@
-// Cluster-resident CG / BiCGSTAB kernels and their launcher (see
+// Cluster-resident CG / BiCGSTAB kernels and their launchers (see
 // mlsh_cluster.cuh for the design).
+//
+// The per-system solve bodies are device functions used by two kinds of
+// kernel: the queue kernels (single solves and batches: clusters take the
+// next system index from an atomic counter) and the serving kernel
+// (clusters claim records that the host publishes into a ring while the
+// kernel runs -- continuous batching; see mlsh_serve.cu).
 #include <cuda_runtime.h>
+
+#include <cuda/atomic>
 
 #include <algorithm>
 #include <cstring>
@@ -19,314 +27,408 @@ struct ClusterShared {
   double red_warp[32 * 3];
   void *remote_vec[kMaxClusterSize];      // gathered-vector slice of each CTA
   double *remote_slots[kMaxClusterSize];
-  unsigned sys_idx;
+  ClusterSystem sys;                      // serving: this CTA's copy of the record
+  unsigned long long sys_idx;
 };
 
-// Thread's k-th own row (local index) of the CTA's slice.
+// Per-CTA view of the engine (one per kernel).
+struct ClusterEnv {
+  cgs::cluster_group &cl;
+  ClusterShared &sh;
+  unsigned char *dyn;
+  unsigned csize, rank;
+  int shift, rpc, mask;
+  int parity;
+};
+
+struct SolveOut {
+  int status;
+  long long iters;
+  double resid;
+};
+
 #define MLSH_FOR_OWN_ROWS(i, nloc) \
   for (int i = (int)threadIdx.x; i < (nloc); i += kClusterThreads)
 
-template <typename T, bool JAC>
+template <typename T>
 __device__ __forceinline__ void cluster_jacobi_setup(const int *rp, const int *ci, const T *val,
-                                                     T *dinv, int row0, int nloc) {
-  if constexpr (JAC) {
-    MLSH_FOR_OWN_ROWS(i, nloc) {
-      const int row = row0 + i;
-      T d = T(0);
-      for (int j = __ldg(rp + row); j < __ldg(rp + row + 1); ++j)
-        if (__ldg(ci + j) == row) d = __ldg(val + j);
-      dinv[row] = T(1) / d;
-    }
+                                                     T *dinv, int row0, int nloc, bool jac) {
+  if (!jac) return;
+  MLSH_FOR_OWN_ROWS(i, nloc) {
+    const int row = row0 + i;
+    T d = T(0);
+    for (int j = __ldg(rp + row); j < __ldg(rp + row + 1); ++j)
+      if (__ldg(ci + j) == row) d = __ldg(val + j);
+    dinv[row] = T(1) / d;
   }
 }
 
-__device__ __forceinline__ unsigned cluster_next_system(ClusterShared &sh, unsigned *queue,
-                                                        cgs::cluster_group &cl) {
-  if (cl.block_rank() == 0 && threadIdx.x == 0) {
-    const unsigned idx = atomicAdd(queue, 1u);
-    for (unsigned r = 0; r < cl.num_blocks(); ++r) *cl.map_shared_rank(&sh.sys_idx, r) = idx;
-  }
-  cl.sync();
-  return sh.sys_idx;
+template <int NR>
+__device__ __forceinline__ void env_sum(ClusterEnv &E, double (&v)[NR]) {
+  cluster_sum<NR>(v, E.sh.red_warp, E.sh.remote_slots, E.sh.slots, E.parity, E.csize, E.rank,
+                  E.cl);
+  E.parity ^= 1;
 }
 
 // ------------------------------------------------------------------- CG --
-template <typename T, bool JAC>
-__global__ void __launch_bounds__(kClusterThreads, 1) cluster_cg_kernel(const ClusterArgs a) {
-  cgs::cluster_group cl = cgs::this_cluster();
-  const unsigned csize = cl.num_blocks();
-  const unsigned rank = cl.block_rank();
-  const int shift = a.rpc_shift, RPC = 1 << shift, mask = RPC - 1;
-  extern __shared__ __align__(16) unsigned char dyn[];
-  __shared__ ClusterShared sh;
-  T *r = reinterpret_cast<T *>(dyn);
-  T *g = r + RPC;  // p, gathered by the SpMV
+// src/equation/cg.cpp:13-86 on one system; dynamic smem: r, g (= p), q.
+// Inlined into each kernel so that `jac` is a constant where the kernel
+// fixes it.
+template <typename T>
+__device__ __forceinline__ SolveOut cg_system(ClusterEnv &E, const ClusterSystem &S, bool jac,
+                                              unsigned long long budget_ns) {
+  const int RPC = E.rpc;
+  T *r = reinterpret_cast<T *>(E.dyn);
+  T *g = r + RPC;
   T *q = g + RPC;
-  if (threadIdx.x < csize) {
-    sh.remote_vec[threadIdx.x] = cl.map_shared_rank(g, threadIdx.x);
-    sh.remote_slots[threadIdx.x] = cl.map_shared_rank(sh.slots, threadIdx.x);
+  T *const *remote = reinterpret_cast<T *const *>(E.sh.remote_vec);
+  const int rank = (int)E.rank, shift = E.shift, mask = E.mask;
+  const int n = S.n;
+  const int row0 = rank * RPC;
+  const int nloc = max(0, min(RPC, n - row0));
+  const int *rp = S.rp, *ci = S.ci;
+  const T *val = static_cast<const T *>(S.val);
+  const T *b = static_cast<const T *>(S.b);
+  T *x = static_cast<T *>(S.x);
+  T *dinv = static_cast<T *>(S.dinv);
+  const double tol = S.tol;
+  const long long maxiter = S.maxiter, miniter = S.miniter;
+  double *hist = S.hist;
+  const long long hist_cap = S.hist_cap;
+  const uint64_t t0 = global_timer_ns();
+
+  cluster_jacobi_setup<T>(rp, ci, val, dinv, row0, nloc, jac);
+  MLSH_FOR_OWN_ROWS(i, nloc) g[i] = x[row0 + i];
+  E.cl.sync();
+  // r = b - A x0 (cg.cpp:39-40), z = M r, p = z (cg.cpp:43-44)
+  double s2[2] = {0.0, 0.0};
+  MLSH_FOR_OWN_ROWS(i, nloc) {
+    const int row = row0 + i;
+    const T qv = cluster_row_dot<T>(rp, ci, val, row, g, remote, shift, mask, rank);
+    const T ri = b[row] - qv;
+    r[i] = ri;
+    const T zi = jac ? dinv[row] * ri : ri;
+    q[i] = zi;
+    s2[0] += (double)zi * (double)ri;
+    s2[1] += (double)ri * (double)ri;
   }
-  cl.sync();
-  T *const *remote = reinterpret_cast<T *const *>(sh.remote_vec);
-  int parity = 0;
+  env_sum<2>(E, s2);
+  double rz = s2[0], rr = s2[1];
+  MLSH_FOR_OWN_ROWS(i, nloc) g[i] = q[i];
+  long long it = 0;
+  int status = maxiter <= 0 ? MLSH_SOLVER_MAXITER : kRunning;
+  double resid = cl_resid<T>(rr);
+  E.cl.sync();
 
-  while (true) {
-    const unsigned idx = cluster_next_system(sh, a.queue, cl);
-    if (idx >= (unsigned)a.n_systems) break;
-    ClusterSystem &S = a.systems[idx];
-    const int n = S.n;
-    const int row0 = (int)rank * RPC;
-    const int nloc = max(0, min(RPC, n - row0));
-    const int *rp = S.rp, *ci = S.ci;
-    const T *val = static_cast<const T *>(S.val);
-    const T *b = static_cast<const T *>(S.b);
-    T *x = static_cast<T *>(S.x);
-    T *dinv = static_cast<T *>(S.dinv);
-    const double tol = S.tol;
-    const long long maxiter = S.maxiter, miniter = S.miniter;
-    const uint64_t t0 = global_timer_ns();
-
-    cluster_jacobi_setup<T, JAC>(rp, ci, val, dinv, row0, nloc);
-    MLSH_FOR_OWN_ROWS(i, nloc) g[i] = x[row0 + i];
-    cl.sync();
-    // r = b - A x0 (cg.cpp:39-40), z = M r, p = z (cg.cpp:43-44)
-    double acc[3] = {0.0, 0.0, 0.0};
+  while (status == kRunning) {
+    // q = A p, (p, q)
+    double pq[1] = {0.0};
+    MLSH_FOR_OWN_ROWS(i, nloc) {
+      const T qv = cluster_row_dot<T>(rp, ci, val, row0 + i, g, remote, shift, mask, rank);
+      q[i] = qv;
+      pq[0] += (double)g[i] * (double)qv;
+    }
+    env_sum<1>(E, pq);
+    const T alpha = (T)(rz / pq[0]);
+    // x += alpha p; r -= alpha q; (z, r), (r, r); time budget
+    double s3[3] = {0.0, 0.0, 0.0};
     MLSH_FOR_OWN_ROWS(i, nloc) {
       const int row = row0 + i;
-      const T qv = cluster_row_dot<T>(rp, ci, val, row, g, remote, shift, mask, (int)rank);
-      const T ri = b[row] - qv;
+      const T pi = g[i], qi = q[i];
+      x[row] = alpha * pi + x[row];
+      const T ri = -alpha * qi + r[i];
       r[i] = ri;
-      const T zi = JAC ? dinv[row] * ri : ri;
-      q[i] = zi;
-      acc[0] += (double)zi * (double)ri;
-      acc[1] += (double)ri * (double)ri;
+      const T zi = jac ? dinv[row] * ri : ri;
+      s3[0] += (double)zi * (double)ri;
+      s3[1] += (double)ri * (double)ri;
     }
-    {
-      double s2[2] = {acc[0], acc[1]};
-      cluster_sum<2>(s2, sh.red_warp, sh.remote_slots, sh.slots, parity, csize, rank, cl);
-      parity ^= 1;
-      acc[0] = s2[0];
-      acc[1] = s2[1];
+    if (rank == 0 && threadIdx.x == 0 && global_timer_ns() - t0 > budget_ns) s3[2] = 1.0;
+    env_sum<3>(E, s3);
+    rr = s3[1];
+    ++it;
+    resid = cl_resid<T>(rr);
+    if (rank == 0 && threadIdx.x == 0 && hist != nullptr && it <= hist_cap) hist[it - 1] = resid;
+    if (resid < tol && miniter <= it) status = MLSH_SUCCESS;
+    else if (isnan(resid)) status = MLSH_SOLVER_RESIDUAL_NAN;
+    else if (it >= maxiter) status = MLSH_SOLVER_MAXITER;
+    else if (s3[2] > 0.0) status = MLSH_ERR_TIMEOUT;
+    if (status != kRunning) break;
+    const T beta = (T)(s3[0] / rz);
+    rz = s3[0];
+    // p = z + beta p (cg.cpp:59)
+    MLSH_FOR_OWN_ROWS(i, nloc) {
+      const T zi = jac ? dinv[row0 + i] * r[i] : r[i];
+      g[i] = zi + beta * g[i];
     }
-    double rz = acc[0], rr = acc[1];
-    MLSH_FOR_OWN_ROWS(i, nloc) g[i] = q[i];
-    long long it = 0;
-    int status = maxiter <= 0 ? MLSH_SOLVER_MAXITER : kRunning;
-    double resid = cl_resid<T>(rr);
-    cl.sync();
-
-    while (status == kRunning) {
-      // q = A p, (p, q)
-      double pq[1] = {0.0};
-      MLSH_FOR_OWN_ROWS(i, nloc) {
-        const T qv = cluster_row_dot<T>(rp, ci, val, row0 + i, g, remote, shift, mask, (int)rank);
-        q[i] = qv;
-        pq[0] += (double)g[i] * (double)qv;
-      }
-      cluster_sum<1>(pq, sh.red_warp, sh.remote_slots, sh.slots, parity, csize, rank, cl);
-      parity ^= 1;
-      const T alpha = (T)(rz / pq[0]);
-      // x += alpha p; r -= alpha q; (z, r), (r, r); time budget
-      double s3[3] = {0.0, 0.0, 0.0};
-      MLSH_FOR_OWN_ROWS(i, nloc) {
-        const int row = row0 + i;
-        const T pi = g[i], qi = q[i];
-        x[row] = alpha * pi + x[row];
-        const T ri = -alpha * qi + r[i];
-        r[i] = ri;
-        const T zi = JAC ? dinv[row] * ri : ri;
-        s3[0] += (double)zi * (double)ri;
-        s3[1] += (double)ri * (double)ri;
-      }
-      if (rank == 0 && threadIdx.x == 0 && global_timer_ns() - t0 > a.budget_ns) s3[2] = 1.0;
-      cluster_sum<3>(s3, sh.red_warp, sh.remote_slots, sh.slots, parity, csize, rank, cl);
-      parity ^= 1;
-      rr = s3[1];
-      ++it;
-      resid = cl_resid<T>(rr);
-      if (rank == 0 && threadIdx.x == 0 && S.hist != nullptr && it <= S.hist_cap)
-        S.hist[it - 1] = resid;
-      if (resid < tol && miniter <= it) status = MLSH_SUCCESS;
-      else if (isnan(resid)) status = MLSH_SOLVER_RESIDUAL_NAN;
-      else if (it >= maxiter) status = MLSH_SOLVER_MAXITER;
-      else if (s3[2] > 0.0) status = MLSH_ERR_TIMEOUT;
-      if (status != kRunning) break;
-      const T beta = (T)(s3[0] / rz);
-      rz = s3[0];
-      // p = z + beta p (cg.cpp:59)
-      MLSH_FOR_OWN_ROWS(i, nloc) {
-        const T zi = JAC ? dinv[row0 + i] * r[i] : r[i];
-        g[i] = zi + beta * g[i];
-      }
-      cl.sync();
-    }
-    if (rank == 0 && threadIdx.x == 0) {
-      S.status = status;
-      S.iters = it;
-      S.resid = resid;
-    }
+    E.cl.sync();
   }
+  // every x write above precedes the last cluster barrier (inside env_sum)
+  return SolveOut{status, it, resid};
 }
 
 // ------------------------------------------------------------- BiCGSTAB --
-template <typename T, bool JAC>
-__global__ void __launch_bounds__(kClusterThreads, 1)
-    cluster_bicgstab_kernel(const ClusterArgs a) {
-  cgs::cluster_group cl = cgs::this_cluster();
-  const unsigned csize = cl.num_blocks();
-  const unsigned rank = cl.block_rank();
-  const int shift = a.rpc_shift, RPC = 1 << shift, mask = RPC - 1;
-  extern __shared__ __align__(16) unsigned char dyn[];
-  __shared__ ClusterShared sh;
-  T *r = reinterpret_cast<T *>(dyn);
+// src/equation/bicgstab.cpp:13-135 on one system; dynamic smem: r, p, v,
+// s, t, g (= p-hat, then s-hat).
+template <typename T>
+__device__ __forceinline__ SolveOut bicgstab_system(ClusterEnv &E, const ClusterSystem &S,
+                                                    bool jac, unsigned long long budget_ns) {
+  const int RPC = E.rpc;
+  T *r = reinterpret_cast<T *>(E.dyn);
   T *p = r + RPC;
   T *v = p + RPC;
   T *s = v + RPC;
   T *t = s + RPC;
-  T *g = t + RPC;  // p-hat, then s-hat: gathered by the SpMVs
-  if (threadIdx.x < csize) {
-    sh.remote_vec[threadIdx.x] = cl.map_shared_rank(g, threadIdx.x);
+  T *g = t + RPC;
+  T *const *remote = reinterpret_cast<T *const *>(E.sh.remote_vec);
+  const int rank = (int)E.rank, shift = E.shift, mask = E.mask;
+  const int n = S.n;
+  const int row0 = rank * RPC;
+  const int nloc = max(0, min(RPC, n - row0));
+  const int *rp = S.rp, *ci = S.ci;
+  const T *val = static_cast<const T *>(S.val);
+  const T *b = static_cast<const T *>(S.b);
+  T *x = static_cast<T *>(S.x);
+  T *dinv = static_cast<T *>(S.dinv);
+  T *r0 = static_cast<T *>(S.aux);
+  const double tol = S.tol;
+  const long long maxiter = S.maxiter, miniter = S.miniter;
+  double *hist = S.hist;
+  const long long hist_cap = S.hist_cap;
+  const uint64_t t0 = global_timer_ns();
+
+  cluster_jacobi_setup<T>(rp, ci, val, dinv, row0, nloc, jac);
+  MLSH_FOR_OWN_ROWS(i, nloc) g[i] = x[row0 + i];
+  E.cl.sync();
+  // r = b - A x, r0 = r (bicgstab.cpp:47-51)
+  double s2[2] = {0.0, 0.0};
+  MLSH_FOR_OWN_ROWS(i, nloc) {
+    const int row = row0 + i;
+    const T ri = b[row] - cluster_row_dot<T>(rp, ci, val, row, g, remote, shift, mask, rank);
+    r[i] = ri;
+    r0[row] = ri;
+    s2[0] += (double)ri * (double)ri;
+    s2[1] += (double)ri * (double)ri;
+  }
+  env_sum<2>(E, s2);
+  double rho = s2[0], rr = s2[1], rho_old = 1.0, alpha_d = 1.0, omega_d = 1.0;
+  long long it = 0;
+  double resid = cl_resid<T>(rr);
+  int status = kRunning;
+  if (maxiter <= 0) {
+    status = MLSH_SOLVER_MAXITER;
+  } else if (rho == 0.0) {
+    status = MLSH_SOLVER_BREAKDOWN;
+    it = 1;
+  }
+
+  while (status == kRunning) {
+    // p = r + beta (p - omega v) (bicgstab.cpp:66-74); p-hat = M p
+    const T beta = (T)((rho / rho_old) * (alpha_d / omega_d));
+    const T omega_t = (T)omega_d;
+    MLSH_FOR_OWN_ROWS(i, nloc) {
+      T pi;
+      if (it == 0) {
+        pi = r[i];
+      } else {
+        const T tmp = -omega_t * v[i] + p[i];
+        pi = r[i] + beta * tmp;
+      }
+      p[i] = pi;
+      g[i] = jac ? dinv[row0 + i] * pi : pi;
+    }
+    E.cl.sync();
+    // v = A p-hat; alpha = rho / (v, r0)
+    double vr[1] = {0.0};
+    MLSH_FOR_OWN_ROWS(i, nloc) {
+      const int row = row0 + i;
+      const T vv = cluster_row_dot<T>(rp, ci, val, row, g, remote, shift, mask, rank);
+      v[i] = vv;
+      vr[0] += (double)vv * (double)r0[row];
+    }
+    env_sum<1>(E, vr);
+    const T alpha = (T)(rho / vr[0]);
+    alpha_d = (double)alpha;
+    // s = r - alpha v; s-hat = M s
+    MLSH_FOR_OWN_ROWS(i, nloc) {
+      const T si = -alpha * v[i] + r[i];
+      s[i] = si;
+      g[i] = jac ? dinv[row0 + i] * si : si;
+    }
+    E.cl.sync();
+    // t = A s-hat; omega = (t, s) / (t, t)
+    double tw[2] = {0.0, 0.0};
+    MLSH_FOR_OWN_ROWS(i, nloc) {
+      const T tv = cluster_row_dot<T>(rp, ci, val, row0 + i, g, remote, shift, mask, rank);
+      t[i] = tv;
+      tw[0] += (double)tv * (double)s[i];
+      tw[1] += (double)tv * (double)tv;
+    }
+    env_sum<2>(E, tw);
+    const T omega = (T)(tw[0] / tw[1]);
+    if (omega == T(0)) {  // bicgstab.cpp:93-98
+      status = MLSH_SOLVER_BREAKDOWN;
+      ++it;
+      break;
+    }
+    omega_d = (double)omega;
+    // x += alpha p-hat + omega s-hat; r = s - omega t; (r, r0), (r, r)
+    double s3[3] = {0.0, 0.0, 0.0};
+    MLSH_FOR_OWN_ROWS(i, nloc) {
+      const int row = row0 + i;
+      const T di = jac ? dinv[row] : T(1);
+      const T ph = jac ? di * p[i] : p[i];
+      const T shh = jac ? di * s[i] : s[i];
+      T xi = alpha * ph + x[row];
+      xi = omega * shh + xi;
+      x[row] = xi;
+      const T ri = -omega * t[i] + s[i];
+      r[i] = ri;
+      s3[0] += (double)ri * (double)r0[row];
+      s3[1] += (double)ri * (double)ri;
+    }
+    if (rank == 0 && threadIdx.x == 0 && global_timer_ns() - t0 > budget_ns) s3[2] = 1.0;
+    env_sum<3>(E, s3);
+    rr = s3[1];
+    ++it;
+    resid = cl_resid<T>(rr);
+    if (rank == 0 && threadIdx.x == 0 && hist != nullptr && it <= hist_cap) hist[it - 1] = resid;
+    if (resid < tol && miniter <= it) status = MLSH_SUCCESS;
+    else if (isnan(resid)) status = MLSH_SOLVER_RESIDUAL_NAN;
+    else if (it >= maxiter) status = MLSH_SOLVER_MAXITER;
+    else if (s3[2] > 0.0) status = MLSH_ERR_TIMEOUT;
+    if (status != kRunning) break;
+    rho_old = rho;
+    rho = s3[0];
+    if (rho == 0.0) {  // next iteration's breakdown check (bicgstab.cpp:58-63)
+      status = MLSH_SOLVER_BREAKDOWN;
+      ++it;
+    }
+  }
+  // every x write above precedes the last cluster barrier (inside env_sum)
+  return SolveOut{status, it, resid};
+}
+
+// ------------------------------------------------------------- kernels --
+__device__ __forceinline__ void env_init(ClusterEnv &E, void *gathered) {
+  if (threadIdx.x < E.csize) {
+    E.sh.remote_vec[threadIdx.x] = E.cl.map_shared_rank(gathered, threadIdx.x);
+    E.sh.remote_slots[threadIdx.x] = E.cl.map_shared_rank(E.sh.slots, threadIdx.x);
+  }
+  E.cl.sync();
+}
+
+// Next system index from the launch's queue (rank 0 claims, all CTAs see it).
+__device__ __forceinline__ unsigned long long queue_next(ClusterEnv &E, unsigned *queue) {
+  if (E.rank == 0 && threadIdx.x == 0) {
+    const unsigned long long idx = atomicAdd(queue, 1u);
+    for (unsigned r = 0; r < E.csize; ++r) *E.cl.map_shared_rank(&E.sh.sys_idx, r) = idx;
+  }
+  E.cl.sync();
+  return E.sh.sys_idx;
+}
+
+// KIND 0: CG, 1: BiCGSTAB.
+template <typename T, int KIND, bool JAC>
+__global__ void __launch_bounds__(kClusterThreads, 1) cluster_queue_kernel(const ClusterArgs a) {
+  cgs::cluster_group cl = cgs::this_cluster();
+  extern __shared__ __align__(16) unsigned char dyn[];
+  __shared__ ClusterShared sh;
+  ClusterEnv E{cl, sh, dyn, cl.num_blocks(), cl.block_rank(), a.rpc_shift, 1 << a.rpc_shift,
+               (1 << a.rpc_shift) - 1, 0};
+  T *gathered = reinterpret_cast<T *>(dyn) + (KIND == 0 ? 1 : 5) * E.rpc;
+  env_init(E, gathered);
+  while (true) {
+    const unsigned long long idx = queue_next(E, a.queue);
+    if (idx >= (unsigned long long)a.n_systems) break;
+    ClusterSystem &S = a.systems[idx];
+    const SolveOut o = KIND == 0 ? cg_system<T>(E, S, JAC, a.budget_ns)
+                                 : bicgstab_system<T>(E, S, JAC, a.budget_ns);
+    if (E.rank == 0 && threadIdx.x == 0) {
+      S.status = o.status;
+      S.iters = o.iters;
+      S.resid = o.resid;
+    }
+  }
+}
+
+// Serving: claim the next published ring record, copy it into every CTA's
+// shared memory.  Returns false when the cluster should exit (shutdown, or
+// no work for idle_ns).  The wait polls with a bounded sleep.
+__device__ __forceinline__ bool ring_next(ClusterEnv &E, const ServeRing &ring) {
+  if (E.rank == 0 && threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_system> tail(*ring.tail);
+    cuda::atomic_ref<int, cuda::thread_scope_system> stop(*ring.shutdown);
+    unsigned long long claimed = ~0ull;
+    const uint64_t t0 = global_timer_ns();
+    while (true) {
+      const unsigned long long h = atomicAdd(ring.head, 0ull);
+      const unsigned long long t = tail.load(cuda::memory_order_acquire);
+      if (h < t) {
+        if (atomicCAS(ring.head, h, h + 1) == h) {
+          claimed = h;
+          break;
+        }
+        continue;
+      }
+      if (stop.load(cuda::memory_order_relaxed) != 0) break;
+      if (global_timer_ns() - t0 > ring.idle_ns) break;
+      __nanosleep(2000);
+    }
+    ClusterSystem rec;
+    if (claimed != ~0ull) {
+      // uncached word copy of the host-written record
+      const volatile unsigned long long *src = reinterpret_cast<const volatile unsigned long long *>(
+          ring.rec + (claimed & (ring.capacity - 1)));
+      unsigned long long *dst = reinterpret_cast<unsigned long long *>(&rec);
+      for (int w = 0; w < (int)(sizeof(ClusterSystem) / 8); ++w) dst[w] = src[w];
+    }
+    for (unsigned r = 0; r < E.csize; ++r) {
+      *E.cl.map_shared_rank(&E.sh.sys_idx, r) = claimed;
+      if (claimed != ~0ull) *E.cl.map_shared_rank(&E.sh.sys, r) = rec;
+    }
+  }
+  E.cl.sync();
+  return E.sh.sys_idx != ~0ull;
+}
+
+// The serving kernel: FP64, CG or BiCGSTAB per record, Jacobi or none per
+// record; dynamic shared memory for BiCGSTAB's six vectors.
+__global__ void __launch_bounds__(kClusterThreads, 1) cluster_serve_kernel(const ClusterArgs a) {
+  cgs::cluster_group cl = cgs::this_cluster();
+  extern __shared__ __align__(16) unsigned char dyn[];
+  __shared__ ClusterShared sh;
+  ClusterEnv E{cl, sh, dyn, cl.num_blocks(), cl.block_rank(), a.rpc_shift, 1 << a.rpc_shift,
+               (1 << a.rpc_shift) - 1, 0};
+  // CG gathers the second vector, BiCGSTAB the sixth: both are mapped
+  void *g_cg = reinterpret_cast<double *>(dyn) + E.rpc;
+  void *g_bi = reinterpret_cast<double *>(dyn) + 5 * E.rpc;
+  __shared__ void *remote_cg[kMaxClusterSize], *remote_bi[kMaxClusterSize];
+  if (threadIdx.x < E.csize) {
+    remote_cg[threadIdx.x] = cl.map_shared_rank(g_cg, threadIdx.x);
+    remote_bi[threadIdx.x] = cl.map_shared_rank(g_bi, threadIdx.x);
     sh.remote_slots[threadIdx.x] = cl.map_shared_rank(sh.slots, threadIdx.x);
   }
   cl.sync();
-  T *const *remote = reinterpret_cast<T *const *>(sh.remote_vec);
-  int parity = 0;
-
-  while (true) {
-    const unsigned idx = cluster_next_system(sh, a.queue, cl);
-    if (idx >= (unsigned)a.n_systems) break;
-    ClusterSystem &S = a.systems[idx];
-    const int n = S.n;
-    const int row0 = (int)rank * RPC;
-    const int nloc = max(0, min(RPC, n - row0));
-    const int *rp = S.rp, *ci = S.ci;
-    const T *val = static_cast<const T *>(S.val);
-    const T *b = static_cast<const T *>(S.b);
-    T *x = static_cast<T *>(S.x);
-    T *dinv = static_cast<T *>(S.dinv);
-    T *r0 = static_cast<T *>(S.aux);
-    const double tol = S.tol;
-    const long long maxiter = S.maxiter, miniter = S.miniter;
-    const uint64_t t0 = global_timer_ns();
-
-    cluster_jacobi_setup<T, JAC>(rp, ci, val, dinv, row0, nloc);
-    MLSH_FOR_OWN_ROWS(i, nloc) g[i] = x[row0 + i];
+  while (ring_next(E, a.ring)) {
+    const ClusterSystem &S = sh.sys;
+    const bool bicg = (S.flags & kSysBiCGSTAB) != 0;
+    const bool jac = (S.flags & kSysJacobi) != 0;
+    if (threadIdx.x < E.csize)
+      sh.remote_vec[threadIdx.x] = bicg ? remote_bi[threadIdx.x] : remote_cg[threadIdx.x];
+    __syncthreads();
+    const SolveOut o = bicg ? bicgstab_system<double>(E, S, jac, a.budget_ns)
+                            : cg_system<double>(E, S, jac, a.budget_ns);
+    if (E.rank == 0 && threadIdx.x == 0) {
+      ClusterSystem *dst = a.ring.rec + (sh.sys_idx & (a.ring.capacity - 1));
+      volatile ClusterSystem *vd = dst;
+      vd->status = o.status;
+      vd->iters = o.iters;
+      vd->resid = o.resid;
+      cuda::atomic_ref<int, cuda::thread_scope_system> done(dst->done);
+      done.store(1, cuda::memory_order_release);
+    }
+    // every CTA is done with this record before rank 0 overwrites sys
     cl.sync();
-    // r = b - A x, r0 = r (bicgstab.cpp:47-51)
-    double s2[2] = {0.0, 0.0};
-    MLSH_FOR_OWN_ROWS(i, nloc) {
-      const int row = row0 + i;
-      const T ri = b[row] - cluster_row_dot<T>(rp, ci, val, row, g, remote, shift, mask, (int)rank);
-      r[i] = ri;
-      r0[row] = ri;
-      s2[0] += (double)ri * (double)ri;
-      s2[1] += (double)ri * (double)ri;
-    }
-    cluster_sum<2>(s2, sh.red_warp, sh.remote_slots, sh.slots, parity, csize, rank, cl);
-    parity ^= 1;
-    double rho = s2[0], rr = s2[1], rho_old = 1.0, alpha_d = 1.0, omega_d = 1.0;
-    long long it = 0;
-    double resid = cl_resid<T>(rr);
-    int status = kRunning;
-    if (maxiter <= 0) {
-      status = MLSH_SOLVER_MAXITER;
-    } else if (rho == 0.0) {
-      status = MLSH_SOLVER_BREAKDOWN;
-      it = 1;
-    }
-
-    while (status == kRunning) {
-      // p = r + beta (p - omega v) (bicgstab.cpp:66-74); p-hat = M p
-      const T beta = (T)((rho / rho_old) * (alpha_d / omega_d));
-      const T omega_t = (T)omega_d;
-      MLSH_FOR_OWN_ROWS(i, nloc) {
-        T pi;
-        if (it == 0) {
-          pi = r[i];
-        } else {
-          const T tmp = -omega_t * v[i] + p[i];
-          pi = r[i] + beta * tmp;
-        }
-        p[i] = pi;
-        g[i] = JAC ? dinv[row0 + i] * pi : pi;
-      }
-      cl.sync();
-      // v = A p-hat; alpha = rho / (v, r0)
-      double vr[1] = {0.0};
-      MLSH_FOR_OWN_ROWS(i, nloc) {
-        const int row = row0 + i;
-        const T vv = cluster_row_dot<T>(rp, ci, val, row, g, remote, shift, mask, (int)rank);
-        v[i] = vv;
-        vr[0] += (double)vv * (double)r0[row];
-      }
-      cluster_sum<1>(vr, sh.red_warp, sh.remote_slots, sh.slots, parity, csize, rank, cl);
-      parity ^= 1;
-      const T alpha = (T)(rho / vr[0]);
-      alpha_d = (double)alpha;
-      // s = r - alpha v; s-hat = M s
-      MLSH_FOR_OWN_ROWS(i, nloc) {
-        const T si = -alpha * v[i] + r[i];
-        s[i] = si;
-        g[i] = JAC ? dinv[row0 + i] * si : si;
-      }
-      cl.sync();
-      // t = A s-hat; omega = (t, s) / (t, t)
-      double tw[2] = {0.0, 0.0};
-      MLSH_FOR_OWN_ROWS(i, nloc) {
-        const T tv = cluster_row_dot<T>(rp, ci, val, row0 + i, g, remote, shift, mask, (int)rank);
-        t[i] = tv;
-        tw[0] += (double)tv * (double)s[i];
-        tw[1] += (double)tv * (double)tv;
-      }
-      cluster_sum<2>(tw, sh.red_warp, sh.remote_slots, sh.slots, parity, csize, rank, cl);
-      parity ^= 1;
-      const T omega = (T)(tw[0] / tw[1]);
-      if (omega == T(0)) {  // bicgstab.cpp:93-98
-        status = MLSH_SOLVER_BREAKDOWN;
-        ++it;
-        break;
-      }
-      omega_d = (double)omega;
-      // x += alpha p-hat + omega s-hat; r = s - omega t; (r, r0), (r, r)
-      double s3[3] = {0.0, 0.0, 0.0};
-      MLSH_FOR_OWN_ROWS(i, nloc) {
-        const int row = row0 + i;
-        const T di = JAC ? dinv[row] : T(1);
-        const T ph = JAC ? di * p[i] : p[i];
-        const T shh = JAC ? di * s[i] : s[i];
-        T xi = alpha * ph + x[row];
-        xi = omega * shh + xi;
-        x[row] = xi;
-        const T ri = -omega * t[i] + s[i];
-        r[i] = ri;
-        s3[0] += (double)ri * (double)r0[row];
-        s3[1] += (double)ri * (double)ri;
-      }
-      if (rank == 0 && threadIdx.x == 0 && global_timer_ns() - t0 > a.budget_ns) s3[2] = 1.0;
-      cluster_sum<3>(s3, sh.red_warp, sh.remote_slots, sh.slots, parity, csize, rank, cl);
-      parity ^= 1;
-      rr = s3[1];
-      ++it;
-      resid = cl_resid<T>(rr);
-      if (rank == 0 && threadIdx.x == 0 && S.hist != nullptr && it <= S.hist_cap)
-        S.hist[it - 1] = resid;
-      if (resid < tol && miniter <= it) status = MLSH_SUCCESS;
-      else if (isnan(resid)) status = MLSH_SOLVER_RESIDUAL_NAN;
-      else if (it >= maxiter) status = MLSH_SOLVER_MAXITER;
-      else if (s3[2] > 0.0) status = MLSH_ERR_TIMEOUT;
-      if (status != kRunning) break;
-      rho_old = rho;
-      rho = s3[0];
-      if (rho == 0.0) {  // next iteration's breakdown check (bicgstab.cpp:58-63)
-        status = MLSH_SOLVER_BREAKDOWN;
-        ++it;
-      }
-    }
-    if (rank == 0 && threadIdx.x == 0) {
-      S.status = status;
-      S.iters = it;
-      S.resid = resid;
-    }
   }
 }
 
@@ -337,12 +439,13 @@ using KernelFn = void (*)(const ClusterArgs);
 
 KernelFn cluster_kernel(int kind, int dtype, bool jac) {
   if (kind == 0) {
-    if (dtype == MLSH_F64) return jac ? cluster_cg_kernel<double, true> : cluster_cg_kernel<double, false>;
-    return jac ? cluster_cg_kernel<float, true> : cluster_cg_kernel<float, false>;
+    if (dtype == MLSH_F64)
+      return jac ? cluster_queue_kernel<double, 0, true> : cluster_queue_kernel<double, 0, false>;
+    return jac ? cluster_queue_kernel<float, 0, true> : cluster_queue_kernel<float, 0, false>;
   }
   if (dtype == MLSH_F64)
-    return jac ? cluster_bicgstab_kernel<double, true> : cluster_bicgstab_kernel<double, false>;
-  return jac ? cluster_bicgstab_kernel<float, true> : cluster_bicgstab_kernel<float, false>;
+    return jac ? cluster_queue_kernel<double, 1, true> : cluster_queue_kernel<double, 1, false>;
+  return jac ? cluster_queue_kernel<float, 1, true> : cluster_queue_kernel<float, 1, false>;
 }
 
 int cluster_nvec(int kind) { return kind == 0 ? 3 : 6; }
@@ -351,20 +454,37 @@ int set_cluster_attributes() {
   static std::once_flag once;
   static int status = MLSH_SUCCESS;
   std::call_once(once, [] {
+    auto set = [](KernelFn k) {
+      if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kClusterMaxDynSmem) != cudaSuccess ||
+          cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+              cudaSuccess) {
+        cudaGetLastError();
+        status = MLSH_ERR_CUDA;
+      }
+    };
     for (int kind = 0; kind < 2; ++kind)
       for (int dt = 0; dt < 2; ++dt)
-        for (int j = 0; j < 2; ++j) {
-          KernelFn k = cluster_kernel(kind, dt, j != 0);
-          if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   kClusterMaxDynSmem) != cudaSuccess ||
-              cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-                  cudaSuccess) {
-            cudaGetLastError();
-            status = MLSH_ERR_CUDA;
-          }
-        }
+        for (int j = 0; j < 2; ++j) set(cluster_kernel(kind, dt, j != 0));
+    set(cluster_serve_kernel);
   });
   return status;
+}
+
+cudaLaunchConfig_t cluster_config(int csize, int n_clusters, size_t smem, cudaStream_t stream,
+                                  cudaLaunchAttribute *attr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(csize * n_clusters), 1, 1);
+  cfg.blockDim = dim3(kClusterThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)csize;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
 }
 
 }  // namespace
@@ -373,7 +493,6 @@ int cluster_rows_for(int kind, int dtype, int64_t n, int requested) {
   const int esz = dtype_size(dtype);
   int rpc = 1024;
   if (requested > 0) {
-    rpc = 1024;
     while (rpc < requested) rpc <<= 1;
   } else {
     while ((int64_t)rpc * kMaxClusterSize < n) rpc <<= 1;
@@ -386,28 +505,20 @@ int cluster_rows_for(int kind, int dtype, int64_t n, int requested) {
 int cluster_launch(const Handle &h, int kind, int dtype, bool jac, ClusterSystem *d_systems,
                    int n_systems, unsigned *d_queue, int rpc, int csize, int n_clusters,
                    double budget_s, cudaStream_t stream) {
+  (void)h;
   if (set_cluster_attributes() != MLSH_SUCCESS) return MLSH_NOT_IMPL;
   int shift = 0;
   while ((1 << shift) < rpc) ++shift;
-  ClusterArgs a;
+  ClusterArgs a = {};
   a.systems = d_systems;
   a.n_systems = n_systems;
   a.rpc_shift = shift;
   a.queue = d_queue;
   a.budget_ns = (unsigned long long)(budget_s * 1e9);
   a.precond = jac ? MLSH_PRECOND_JACOBI : MLSH_PRECOND_NONE;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(csize * n_clusters), 1, 1);
-  cfg.blockDim = dim3(kClusterThreads, 1, 1);
-  cfg.dynamicSmemBytes = (size_t)cluster_nvec(kind) * rpc * dtype_size(dtype);
-  cfg.stream = stream;
   cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = (unsigned)csize;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cudaLaunchConfig_t cfg = cluster_config(
+      csize, n_clusters, (size_t)cluster_nvec(kind) * rpc * dtype_size(dtype), stream, attr);
   KernelFn k = cluster_kernel(kind, dtype, jac);
   int max_clusters = 0;
   if (cudaOccupancyMaxActiveClusters(&max_clusters, (void *)k, &cfg) != cudaSuccess ||
@@ -425,17 +536,10 @@ int cluster_launch(const Handle &h, int kind, int dtype, bool jac, ClusterSystem
 
 int cluster_max_active(int kind, int dtype, bool jac, int rpc, int csize) {
   if (set_cluster_attributes() != MLSH_SUCCESS) return 0;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)csize, 1, 1);
-  cfg.blockDim = dim3(kClusterThreads, 1, 1);
-  cfg.dynamicSmemBytes = (size_t)cluster_nvec(kind) * rpc * dtype_size(dtype);
   cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = (unsigned)csize;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cudaLaunchConfig_t cfg =
+      cluster_config(csize, 1, (size_t)cluster_nvec(kind) * rpc * dtype_size(dtype), nullptr,
+                     attr);
   int m = 0;
   if (cudaOccupancyMaxActiveClusters(&m, (void *)cluster_kernel(kind, dtype, jac), &cfg) !=
       cudaSuccess) {
@@ -443,6 +547,34 @@ int cluster_max_active(int kind, int dtype, bool jac, int rpc, int csize) {
     return 0;
   }
   return m;
+}
+
+// Serving kernel: FP64, rows per CTA kServeRows (BiCGSTAB's six vectors).
+int cluster_serve_launch(const ServeRing &ring, int csize, int n_clusters, double budget_s,
+                         cudaStream_t stream) {
+  if (set_cluster_attributes() != MLSH_SUCCESS) return MLSH_NOT_IMPL;
+  int shift = 0;
+  while ((1 << shift) < kServeRows) ++shift;
+  ClusterArgs a = {};
+  a.rpc_shift = shift;
+  a.budget_ns = (unsigned long long)(budget_s * 1e9);
+  a.ring = ring;
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg =
+      cluster_config(csize, n_clusters, (size_t)6 * kServeRows * sizeof(double), stream, attr);
+  int max_clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&max_clusters, (void *)cluster_serve_kernel, &cfg) !=
+          cudaSuccess ||
+      max_clusters < 1) {
+    cudaGetLastError();
+    return MLSH_NOT_IMPL;
+  }
+  if (n_clusters > max_clusters) {
+    n_clusters = max_clusters;
+    cfg.gridDim = dim3((unsigned)(csize * n_clusters), 1, 1);
+  }
+  MLSH_CUDA_TRY(cudaLaunchKernelEx(&cfg, cluster_serve_kernel, a));
+  return MLSH_SUCCESS;
 }
 
 }  // namespace mlsh

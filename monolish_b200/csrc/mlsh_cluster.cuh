@@ -17,8 +17,9 @@
 //     (the reference's row loop, crs_matvec.hpp:101-108).
 //   * A wall-clock budget is folded into the per-iteration reduction so a
 //     solve that does not terminate ends with MLSH_ERR_TIMEOUT.
-// The same kernel serves the batched solver: clusters take systems from a
-// queue until it is empty.
+// The same per-system code serves the batched solver (clusters take
+// systems from a queue until it is empty) and the solve server (clusters
+// claim records from a ring that the host fills while the kernel runs).
 #pragma once
 #include <cooperative_groups.h>
 
@@ -37,8 +38,10 @@ constexpr int kClusterMaxDynSmem = 196608;
 constexpr double kClusterBudgetSeconds = 60.0;
 // AUTO engine: longest maxiter sent to the single-launch cluster engine.
 constexpr long long kClusterMaxIterAuto = 2000000;
+// Serving kernel: FP64 rows per CTA (BiCGSTAB's six vectors fit).
+constexpr int kServeRows = 4096;
 
-// One linear system for the cluster engine (device-resident).
+// One linear system for the cluster engine.
 struct ClusterSystem {
   const int *rp;     // row_ptr [n+1] (0-based within the system)
   const int *ci;     // column indices (0-based within the system)
@@ -48,7 +51,7 @@ struct ClusterSystem {
   void *dinv;        // workspace [n]: inverse diagonal (Jacobi)
   void *aux;         // workspace [n]: BiCGSTAB r0
   int n;
-  int pad;
+  int flags;         // serving ring: bit 0 BiCGSTAB, bit 1 Jacobi
   double tol;        // absolute ||r|| threshold
   long long maxiter;
   long long miniter;
@@ -56,10 +59,24 @@ struct ClusterSystem {
   long long hist_cap;
   // results
   int status;
-  int pad2;
+  int done;          // serving ring: set (system scope, release) when final
   long long iters;
   double resid;
 };
+
+constexpr int kSysBiCGSTAB = 1;
+constexpr int kSysJacobi = 2;
+
+// Serving ring: records in host-mapped memory, published by the host.
+struct ServeRing {
+  ClusterSystem *rec;            // [capacity], host memory mapped into the device
+  unsigned long long *tail;      // host-mapped: records published so far
+  unsigned long long *head;      // device: records claimed so far
+  int *shutdown;                 // host-mapped: nonzero asks the kernel to exit
+  unsigned capacity;             // power of two
+  unsigned long long idle_ns;    // clusters exit after this long without work
+};
+static_assert(sizeof(ClusterSystem) % 8 == 0, "records are copied as 8-byte words");
 
 struct ClusterArgs {
   ClusterSystem *systems;
@@ -68,6 +85,7 @@ struct ClusterArgs {
   unsigned *queue;          // next system index (zero before the launch)
   unsigned long long budget_ns;
   int precond;              // MLSH_PRECOND_*
+  ServeRing ring;           // used by the serving kernel only
 };
 
 template <typename T>

@@ -261,7 +261,8 @@ int plan_diag(const CsrPlan &p, void *out, bool invert, cudaStream_t stream) {
 
 int plan_inv_diag(CsrPlan &p, cudaStream_t stream, const void **out) {
   if (!p.inv_diag) {
-    MLSH_CUDA_TRY(cudaMalloc(&p.inv_diag, (size_t)std::max(p.n_rows, 1) * dtype_size(p.dtype)));
+    MLSH_CUDA_TRY(
+        pool_alloc(&p.inv_diag, (size_t)std::max(p.n_rows, 1) * dtype_size(p.dtype), stream));
     p.inv_diag_valid = false;
   }
   if (!p.inv_diag_valid) {
@@ -477,19 +478,22 @@ int mlsh_csr_plan_create(mlsh_handle hs, int n_rows, int n_cols, int nnz,
   p.n_tiles = (int)tiles.size();
   p.n_long = (int)longs.size();
   bool ok = true;
+  cudaStream_t s = h.stream;
   if (p.n_tiles > 0)
-    ok = ok && cudaMalloc(&p.tiles, sizeof(Tile) * tiles.size()) == cudaSuccess &&
-         cudaMemcpy(p.tiles, tiles.data(), sizeof(Tile) * tiles.size(),
-                    cudaMemcpyHostToDevice) == cudaSuccess;
+    ok = ok && pool_alloc(&p.tiles, sizeof(Tile) * tiles.size(), s) == cudaSuccess &&
+         cudaMemcpyAsync(p.tiles, tiles.data(), sizeof(Tile) * tiles.size(),
+                         cudaMemcpyHostToDevice, s) == cudaSuccess;
   if (p.n_long > 0)
-    ok = ok && cudaMalloc(&p.longs, sizeof(LongRow) * longs.size()) == cudaSuccess &&
-         cudaMemcpy(p.longs, longs.data(), sizeof(LongRow) * longs.size(),
-                    cudaMemcpyHostToDevice) == cudaSuccess &&
-         cudaMalloc(&p.chunk_part, sizeof(double) * p.n_chunks) == cudaSuccess &&
-         cudaMalloc(&p.long_cnt, sizeof(unsigned) * p.n_long) == cudaSuccess &&
-         cudaMemset(p.long_cnt, 0, sizeof(unsigned) * p.n_long) == cudaSuccess &&
-         cudaMalloc(&p.long_dot, sizeof(double) * 2 * p.n_long) == cudaSuccess &&
-         cudaMemset(p.long_dot, 0, sizeof(double) * 2 * p.n_long) == cudaSuccess;
+    ok = ok && pool_alloc(&p.longs, sizeof(LongRow) * longs.size(), s) == cudaSuccess &&
+         cudaMemcpyAsync(p.longs, longs.data(), sizeof(LongRow) * longs.size(),
+                         cudaMemcpyHostToDevice, s) == cudaSuccess &&
+         pool_alloc(&p.chunk_part, sizeof(double) * p.n_chunks, s) == cudaSuccess &&
+         pool_alloc(&p.long_cnt, sizeof(unsigned) * p.n_long, s) == cudaSuccess &&
+         cudaMemsetAsync(p.long_cnt, 0, sizeof(unsigned) * p.n_long, s) == cudaSuccess &&
+         pool_alloc(&p.long_dot, sizeof(double) * 2 * p.n_long, s) == cudaSuccess &&
+         cudaMemsetAsync(p.long_dot, 0, sizeof(double) * 2 * p.n_long, s) == cudaSuccess;
+  // the plan may be used on any stream from here on
+  ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
   if (!ok) {
     mlsh_csr_plan_destroy(ps);
     return MLSH_ERR_OOM;
@@ -506,16 +510,13 @@ int mlsh_csr_plan_create(mlsh_handle hs, int n_rows, int n_cols, int nnz,
 int mlsh_csr_plan_destroy(mlsh_csr_plan ps) {
   if (!ps) return MLSH_ERR_INVALID_ARG;
   CsrPlan &p = ps->p;
-  if (p.handle) cudaStreamSynchronize(p.handle->stream);
-  cudaFree(p.tiles);
-  cudaFree(p.longs);
-  cudaFree(p.chunk_part);
-  cudaFree(p.long_cnt);
-  cudaFree(p.long_dot);
-  cudaFree(p.inv_diag);
-  cudaFree(p.col16);
-  cudaFree(p.tile_base);
+  cudaStream_t s = p.handle ? p.handle->stream : nullptr;
+  if (p.handle) cudaStreamSynchronize(s);
   release_plan_extras(p);
+  for (void *d : {(void *)p.tiles, (void *)p.longs, (void *)p.chunk_part, (void *)p.long_cnt,
+                  (void *)p.long_dot, p.inv_diag, (void *)p.col16, (void *)p.tile_base})
+    pool_free(d, s);
+  if (p.handle) cudaStreamSynchronize(s);
   delete ps;
   return MLSH_SUCCESS;
 }

@@ -35,6 +35,11 @@ int cluster_launch(const Handle &h, int kind, int dtype, bool jac, ClusterSystem
                    int n_systems, unsigned *d_queue, int rpc, int csize, int n_clusters,
                    double budget_s, cudaStream_t stream);
 int cluster_max_active(int kind, int dtype, bool jac, int rpc, int csize);
+struct ServeRing;
+// The serving kernel (FP64, kServeRows rows per CTA) on n_clusters
+// clusters of csize CTAs, fed from `ring`.
+int cluster_serve_launch(const ServeRing &ring, int csize, int n_clusters, double budget_s,
+                         cudaStream_t stream);
 
 // Mixed-precision data kept with an FP64 plan (mlsh_mixed.cu).
 void mixed_release(CsrPlan &p);

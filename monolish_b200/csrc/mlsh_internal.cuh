@@ -144,6 +144,18 @@ void set_last_error(const char *where, cudaError_t e);
     }                                               \
   } while (0)
 
+// Plan- and handle-owned buffers come from the stream-ordered pool of the
+// stream that uses them: no device-wide synchronization on allocation or
+// release, so plans can be built and destroyed while kernels of other
+// streams (a persistent serving kernel, say) keep running.
+template <typename P>
+inline cudaError_t pool_alloc(P **ptr, size_t bytes, cudaStream_t s) {
+  return cudaMallocAsync(reinterpret_cast<void **>(ptr), bytes, s);
+}
+inline void pool_free(void *ptr, cudaStream_t s) {
+  if (ptr) cudaFreeAsync(ptr, s);
+}
+
 inline int dtype_size(int dtype) {
   return dtype == MLSH_F64 ? 8 : (dtype == MLSH_F32 ? 4 : 0);
 }

@@ -560,11 +560,11 @@ int ensure_ws(Handle &h, size_t bytes) {
   if (h.ws) {
     cudaStreamSynchronize(h.stream);
     purge_graphs(h, nullptr, h.ws);
-    cudaFree(h.ws);
+    pool_free(h.ws, h.stream);
     h.ws = nullptr;
     h.ws_bytes = 0;
   }
-  if (cudaMalloc(&h.ws, bytes) != cudaSuccess) {
+  if (pool_alloc(&h.ws, bytes, h.stream) != cudaSuccess) {
     cudaGetLastError();
     return MLSH_ERR_OOM;
   }
@@ -591,10 +591,11 @@ int cluster_solve_one(Kind kind, Handle &h, CsrPlan &p, const void *b, void *x,
   unsigned *d_queue = reinterpret_cast<unsigned *>(ws + 256);
   const bool want_hist = opts->history != nullptr && opts->history_len > 0;
   if (want_hist && h.hist_cap < opts->history_len) {
-    if (h.hist) cudaFree(h.hist);
+    pool_free(h.hist, h.stream);
     h.hist = nullptr;
     h.hist_cap = 0;
-    if (cudaMalloc(&h.hist, sizeof(double) * (size_t)opts->history_len) != cudaSuccess) {
+    if (pool_alloc(&h.hist, sizeof(double) * (size_t)opts->history_len, h.stream) !=
+        cudaSuccess) {
       cudaGetLastError();
       return MLSH_ERR_OOM;
     }
@@ -707,10 +708,11 @@ int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, voi
   const bool want_hist = opts->history != nullptr && opts->history_len > 0;
   if (want_hist) {
     if (h.hist_cap < opts->history_len) {
-      if (h.hist) cudaFree(h.hist);
+      pool_free(h.hist, h.stream);
       h.hist = nullptr;
       h.hist_cap = 0;
-      if (cudaMalloc(&h.hist, sizeof(double) * (size_t)opts->history_len) != cudaSuccess) {
+      if (pool_alloc(&h.hist, sizeof(double) * (size_t)opts->history_len, h.stream) !=
+          cudaSuccess) {
         cudaGetLastError();
         h.hist = nullptr;
         return MLSH_ERR_OOM;
@@ -777,10 +779,12 @@ void release_solver_graphs(Handle &h) {
     delete static_cast<GraphCache *>(h.graph_cache);
     h.graph_cache = nullptr;
   }
-  if (h.ws) cudaFree(h.ws);
+  cudaStreamSynchronize(h.stream);
+  pool_free(h.ws, h.stream);
   h.ws = nullptr;
   h.ws_bytes = 0;
-  if (h.hist) cudaFree(h.hist);
+  pool_free(h.hist, h.stream);
+  cudaStreamSynchronize(h.stream);
   h.hist = nullptr;
   h.hist_cap = 0;
 }

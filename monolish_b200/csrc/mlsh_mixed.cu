@@ -103,31 +103,31 @@ __global__ void tile_col16(const Tile *tiles, const int *col, const int *base, u
 int build_col16(CsrPlan &q, cudaStream_t s) {
   if (q.n_tiles == 0 || q.nnz == 0) return MLSH_SUCCESS;
   int *tmin = nullptr, *tmax = nullptr;
-  MLSH_CUDA_TRY(cudaMalloc(&tmin, sizeof(int) * q.n_tiles));
-  MLSH_CUDA_TRY(cudaMalloc(&tmax, sizeof(int) * q.n_tiles));
+  MLSH_CUDA_TRY(pool_alloc(&tmin, sizeof(int) * q.n_tiles, s));
+  MLSH_CUDA_TRY(pool_alloc(&tmax, sizeof(int) * q.n_tiles, s));
   tile_col_range<<<q.n_tiles, 256, 0, s>>>(q.tiles, q.col_ind, tmin, tmax);
   std::vector<int> lo(q.n_tiles), hi(q.n_tiles);
   cudaMemcpyAsync(lo.data(), tmin, sizeof(int) * q.n_tiles, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hi.data(), tmax, sizeof(int) * q.n_tiles, cudaMemcpyDeviceToHost, s);
   const cudaError_t e = cudaStreamSynchronize(s);
-  cudaFree(tmax);
+  pool_free(tmax, s);
   if (e != cudaSuccess) {
-    cudaFree(tmin);
+    pool_free(tmin, s);
     set_last_error("tile column ranges", e);
     return MLSH_ERR_CUDA;
   }
   for (int t = 0; t < q.n_tiles; ++t) {
     if (lo[t] > hi[t]) lo[t] = 0;  // empty tile
     if ((int64_t)hi[t] - lo[t] >= 65536) {
-      cudaFree(tmin);
+      pool_free(tmin, s);
       return MLSH_SUCCESS;  // not compressible: keep 32-bit columns
     }
   }
   cudaMemcpyAsync(tmin, lo.data(), sizeof(int) * q.n_tiles, cudaMemcpyHostToDevice, s);
   uint16_t *c16 = nullptr;
-  if (cudaMalloc(&c16, sizeof(uint16_t) * (size_t)q.nnz) != cudaSuccess) {
+  if (pool_alloc(&c16, sizeof(uint16_t) * (size_t)q.nnz, s) != cudaSuccess) {
     cudaGetLastError();
-    cudaFree(tmin);
+    pool_free(tmin, s);
     return MLSH_SUCCESS;  // no room: keep 32-bit columns
   }
   tile_col16<<<q.n_tiles, 256, 0, s>>>(q.tiles, q.col_ind, tmin, c16);
@@ -137,13 +137,12 @@ int build_col16(CsrPlan &q, cudaStream_t s) {
   return MLSH_SUCCESS;
 }
 
-void free_extras(MixedExtras *m) {
+void free_extras(MixedExtras *m, cudaStream_t s) {
   if (!m) return;
   if (m->plan32) mlsh_csr_plan_destroy(m->plan32);
-  cudaFree(m->val32);
-  cudaFree(m->r64);
-  cudaFree(m->r32);
-  cudaFree(m->d32);
+  cudaStreamSynchronize(s);
+  for (void *d : {(void *)m->val32, (void *)m->r64, (void *)m->r32, (void *)m->d32})
+    pool_free(d, s);
   m->plan32 = nullptr;
   m->val32 = nullptr;
   m->r64 = nullptr;
@@ -164,15 +163,15 @@ int ensure_extras(mlsh_handle hs, CsrPlan &p, MixedExtras **out) {
     *out = m;
     return MLSH_SUCCESS;
   }
-  free_extras(m);
+  free_extras(m, h.stream);
   const size_t n = (size_t)std::max(p.n_rows, 1);
   const size_t nnz = (size_t)std::max(p.nnz, 1);
-  if (cudaMalloc(&m->val32, sizeof(float) * nnz) != cudaSuccess ||
-      cudaMalloc(&m->r64, sizeof(double) * n) != cudaSuccess ||
-      cudaMalloc(&m->r32, sizeof(float) * n) != cudaSuccess ||
-      cudaMalloc(&m->d32, sizeof(float) * n) != cudaSuccess) {
+  if (pool_alloc(&m->val32, sizeof(float) * nnz, h.stream) != cudaSuccess ||
+      pool_alloc(&m->r64, sizeof(double) * n, h.stream) != cudaSuccess ||
+      pool_alloc(&m->r32, sizeof(float) * n, h.stream) != cudaSuccess ||
+      pool_alloc(&m->d32, sizeof(float) * n, h.stream) != cudaSuccess) {
     cudaGetLastError();
-    free_extras(m);
+    free_extras(m, h.stream);
     return MLSH_ERR_OOM;
   }
   if (p.nnz > 0) {
@@ -200,7 +199,7 @@ int ensure_extras(mlsh_handle hs, CsrPlan &p, MixedExtras **out) {
 void mixed_release(CsrPlan &p) {
   MixedExtras *m = static_cast<MixedExtras *>(p.extras);
   if (m) {
-    free_extras(m);
+    free_extras(m, p.handle ? p.handle->stream : nullptr);
     delete m;
     p.extras = nullptr;
   }
@@ -210,7 +209,7 @@ void mixed_invalidate(CsrPlan &p) {
   MixedExtras *m = static_cast<MixedExtras *>(p.extras);
   if (m && m->plan32) {
     // values changed: the FP32 copy is rebuilt at the next mixed solve
-    free_extras(m);
+    free_extras(m, p.handle ? p.handle->stream : nullptr);
   }
 }
 

@@ -299,3 +299,100 @@ def cg_solve(A: Crs, b, x, tol, maxiter, **kw) -> SolveResult:
 
 def bicgstab_solve(A: Crs, b, x, tol, maxiter, **kw) -> SolveResult:
     return _solve(A.lib.mlsh_bicgstab_solve, A, b, x, tol, maxiter, **kw)
+
+
+@dataclass
+class ServeResult:
+    status: int
+    path: int          # 0 cluster ring, 1 worker lane
+    iters: int
+    resid: float
+    t_submit: float
+    t_admit: float
+    t_done: float
+    x: np.ndarray
+
+
+class Server:
+    """Solve server over mlsh_server_*: requests (host CRS + right-hand
+    side) are submitted while others run and come back with their
+    solution and timestamps on the server's clock."""
+
+    def __init__(self, memory_budget=8 << 30, n_lanes=2):
+        self.lib = _abi.load()
+        s = C.c_void_p()
+        _abi.check(self.lib.mlsh_server_create(int(memory_budget), int(n_lanes), C.byref(s)),
+                   "server_create")
+        self.s = s
+        self._live = {}  # request id -> host arrays kept alive until done
+
+    def submit(self, kind, row_ptr, col_ind, val, b, tol, maxiter, x0=None,
+               precond=_abi.PRECOND_JACOBI, precision="fp64", inner_tol=1e-4) -> int:
+        rp = np.ascontiguousarray(row_ptr, np.int32)
+        ci = np.ascontiguousarray(col_ind, np.int32)
+        v = np.ascontiguousarray(val, np.float64)
+        bb = np.ascontiguousarray(b, np.float64)
+        x0a = None if x0 is None else np.ascontiguousarray(x0, np.float64)
+        n = len(rp) - 1
+        xo = np.zeros(n, np.float64)
+        r = _abi.Request()
+        r.kind = 0 if kind == "cg" else 1
+        r.precision = 0 if precision == "fp64" else 1
+        r.precond = precond
+        r.n = n
+        r.nnz = int(rp[-1])
+        r.row_ptr = rp.ctypes.data
+        r.col_ind = ci.ctypes.data if len(ci) else None
+        r.val = v.ctypes.data if len(v) else None
+        r.b = bb.ctypes.data if n else None
+        r.x0 = None if x0a is None else x0a.ctypes.data
+        r.x_out = xo.ctypes.data if n else None
+        r.tol = float(tol)
+        r.maxiter = int(maxiter)
+        r.inner_tol = float(inner_tol)
+        rid = C.c_int64()
+        _abi.check(self.lib.mlsh_server_submit(self.s, C.byref(r), C.byref(rid)), "server_submit")
+        self._live[rid.value] = (rp, ci, v, bb, x0a, xo)
+        return rid.value
+
+    def _result(self, rid, res):
+        arrays = self._live.pop(rid)
+        return ServeResult(res.status, res.path, res.iters, res.resid, res.t_submit,
+                           res.t_admit, res.t_done, arrays[5])
+
+    def poll(self, rid):
+        """The result if request `rid` has finished, else None."""
+        res = _abi.RequestResult()
+        st = self.lib.mlsh_server_poll(self.s, rid, C.byref(res))
+        if st == _abi.PENDING:
+            return None
+        _abi.check(st, "server_poll")
+        return self._result(rid, res)
+
+    def wait(self, rid) -> ServeResult:
+        res = _abi.RequestResult()
+        _abi.check(self.lib.mlsh_server_wait(self.s, rid, C.byref(res)), "server_wait")
+        return self._result(rid, res)
+
+    def drain(self):
+        _abi.check(self.lib.mlsh_server_drain(self.s), "server_drain")
+
+    def now(self) -> float:
+        return self.lib.mlsh_server_now(self.s)
+
+    def stats(self):
+        """(serving-kernel launches, lane solves) since creation."""
+        a, b = C.c_int64(), C.c_int64()
+        _abi.check(self.lib.mlsh_server_stats(self.s, C.byref(a), C.byref(b)), "server_stats")
+        return a.value, b.value
+
+    def close(self):
+        if self.s:
+            self.lib.mlsh_server_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
