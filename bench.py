@@ -56,6 +56,8 @@ WORKLOADS = {
     "cg_poisson2d": dict(kind="cg", matrix="poisson2d", m=128, dtype="f64"),
     "bicgstab_convdiff": dict(kind="bicgstab", matrix="convdiff3d", m=160, dtype="f64"),
     "batch_cg": dict(kind="batch", matrix="diffusion_batch", count=2048, dtype="f64"),
+    "serve_stream": dict(kind="serve", matrix="serve", count=200, budget=8 << 30,
+                         dtype="f64"),
 }
 METRIC_BATCH = "solves/s at 1e-8 rel. residual, 2,048-system batch"
 
@@ -186,6 +188,22 @@ def profile_traffic(workload):
         return None
 
 
+# ------------------------------------------------------ host-side inputs
+def host_matvec(rp, ci, v, x):
+    """y = A x on the host in FP64 (scipy CSR): builds right-hand sides and
+    checks true residuals; never on a timed path."""
+    import scipy.sparse as sp
+    n = len(rp) - 1
+    A = sp.csr_matrix((np.asarray(v, np.float64), ci, rp), shape=(n, len(x)))
+    return A @ np.asarray(x, np.float64)
+
+
+def true_relres(rp, ci, v, b, x):
+    r = b - host_matvec(rp, ci, v, x)
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(r)) / (nb if nb > 0 else 1.0)
+
+
 # ------------------------------------------------------------- CPU leg
 def cpu_reference_spmv(rp, ci, v, x, reps, threads):
     """The reference's CPU SpMV (oracle/_ref build, OpenMP row loop)."""
@@ -290,7 +308,7 @@ def run_spmv(args, wl, rank, world, local):
     else:
         hy.copy_(dy)
 
-    # correctness spot check against the oracle on a sample of rows
+    # correctness spot check: FP64 numpy row dots on a sample of rows
     y = hy.numpy()
     rows = np.linspace(0, n - 1, 2048).astype(np.int64)
     ref_rows = np.array([np.dot(v[rp[i]:rp[i + 1]].astype(np.float64),
@@ -353,12 +371,10 @@ def run_solve(args, wl, rank, world, local):
     import torch
     import torch.distributed as dist
     from monolish_b200 import device as D
-    import oracle
 
     torch.cuda.set_device(local)
     n, rp, ci, v, xt = make_matrix(wl)
-    port = oracle.restatement()
-    b = port.spmv(rp, ci, v, xt)
+    b = host_matvec(rp, ci, v, xt)
     tol = 1e-10 * float(np.linalg.norm(b))
     h = D.Handle()
     A = D.Crs(h, n, n, rp, ci, v, validate=False)
@@ -394,7 +410,7 @@ def run_solve(args, wl, rank, world, local):
         p1.record(stream)
         torch.cuda.synchronize()
         plain_ms = p0.elapsed_time(p1) / args.steps
-        plain_rel = port.true_relres(rp, ci, v, b, dx.cpu().numpy())
+        plain_rel = true_relres(rp, ci, v, b, dx.cpu().numpy())
     for _ in range(args.warmup):
         dx.zero_()
         r = fn(A, db, dx, tol, 20000)
@@ -413,7 +429,7 @@ def run_solve(args, wl, rank, world, local):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     cl = clocks.stop()
-    rel = port.true_relres(rp, ci, v, b, dx.cpu().numpy())
+    rel = true_relres(rp, ci, v, b, dx.cpu().numpy())
     # end to end: b from pinned host memory, x back to host, per solve
     hb = torch.from_numpy(b).pin_memory()
     hx = torch.empty(n, dtype=torch.float64).pin_memory()
@@ -468,6 +484,7 @@ def run_solve(args, wl, rank, world, local):
                                      "speedup_of_mixed": round(plain_ms / (ms / args.steps),
                                                                3)}
         if world == 1 and not args.no_cpu:
+            import oracle
             ref = oracle.reference_or_none()
             if ref is not None:
                 ref.set_threads(os.cpu_count() or 1)
@@ -487,12 +504,10 @@ def run_solve(args, wl, rank, world, local):
 def batch_inputs(wl):
     """Systems, right-hand sides b = A x_true (x_true ~ U[-1,1], seed 3 + k)
     and per-system absolute tolerances 1e-8 * ||b_k||."""
-    import oracle
     from monolish_b200 import workloads as W
     count = wl.get("size") or wl["count"]
     systems = W.diffusion_batch(count, seed=3)
-    port = oracle.restatement()
-    bs = [port.spmv(rp, ci, v, W.uniform_mt(len(rp) - 1, -1.0, 1.0, 3 + k))
+    bs = [host_matvec(rp, ci, v, W.uniform_mt(len(rp) - 1, -1.0, 1.0, 3 + k))
           for k, (rp, ci, v) in enumerate(systems)]
     tol = np.array([1e-8 * np.linalg.norm(b) for b in bs])
     return systems, bs, tol
@@ -519,7 +534,6 @@ def cpu_reference_batch(systems, bs, tol, every, threads):
 def run_batch(args, wl, rank, world, local):
     import torch
     import torch.distributed as dist
-    import oracle
     from monolish_b200 import device as D
 
     torch.cuda.set_device(local)
@@ -589,10 +603,9 @@ def run_batch(args, wl, rank, world, local):
         ms, e2e_ms = float(t[0]), float(t[1])
     out = None
     if rank == 0:
-        port = oracle.restatement()
         xs = np.split(x_all, np.cumsum([len(b) for b in bs])[:-1])
         sample = list(range(0, count, max(1, count // 32)))
-        worst = max(port.true_relres(*systems[k], bs[k], xs[k]) for k in sample)
+        worst = max(true_relres(*systems[k], bs[k], xs[k]) for k in sample)
         per_step_s = ms / 1e3 / args.steps
         value = world * count / per_step_s
         rows = int(sum(len(b) for b in bs))
@@ -647,10 +660,251 @@ def run_batch(args, wl, rank, world, local):
     return out
 
 
+# ---------------------------------------------------------- serving leg
+METRIC_SERVE = "served solves/s (open-loop Poisson arrivals), p50/p99 latency"
+
+
+def serve_requests(count, seed=4, lo=1e3, hi=2e6):
+    """The request stream: per request a family (CG on 2D or 3D
+    variable-coefficient diffusion, or BiCGSTAB on upwind
+    convection-diffusion with Peclet ~ U[0,20]), a size log-uniform in
+    [lo, hi], tol 1e-8 or 1e-10 (relative to ||b||) and plain FP64 or mixed
+    precision, each chosen uniformly (numpy PCG64(seed)); b = A x_true with
+    x_true ~ U[-1,1]."""
+    from monolish_b200 import workloads as W
+    rng = np.random.default_rng(seed)
+    sizes = W.loguniform_sizes(count, lo, hi, seed)
+    reqs = []
+    for k in range(count):
+        fam = int(rng.integers(3))
+        rel = (1e-8, 1e-10)[int(rng.integers(2))]
+        prec = ("fp64", "mixed")[int(rng.integers(2))]
+        pe = float(rng.uniform(0.0, 20.0))
+        n = int(sizes[k])
+        if fam == 0:
+            nx, ny = W.grid2d_for(n)
+            _, rp, ci, v = W.vardiff2d(nx, ny, seed, k)
+            kind = "cg"
+        elif fam == 1:
+            m = max(2, int(round(n ** (1.0 / 3.0))))
+            nz = max(1, -(-n // (m * m)))
+            _, rp, ci, v = W.vardiff3d(m, m, nz, seed, k)
+            kind = "cg"
+        else:
+            m = max(2, int(round(n ** (1.0 / 3.0))))
+            _, rp, ci, v = W.convdiff3d(m, peclet=pe)
+            kind = "bicgstab"
+        xt = W.uniform_fast(len(rp) - 1, -1.0, 1.0, 1000 * seed + k)
+        b = host_matvec(rp, ci, v, xt)
+        reqs.append(dict(kind=kind, family=("cg2d", "cg3d", "bicgstab")[fam], precision=prec,
+                         rel=rel, rp=rp, ci=ci, v=v, b=b,
+                         tol=rel * float(np.linalg.norm(b))))
+    return reqs
+
+
+def serve_stream(D, reqs, rate, budget, lanes, seed, maxiter):
+    """Submit `reqs` at Poisson arrival times (rate req/s) from a producer
+    thread; returns per-request results and (serving-kernel launches, lane
+    solves) during the stream."""
+    import threading
+    srv = D.Server(budget, lanes)
+    # warm-up: the smallest request of each kind and precision (serving
+    # kernels, lanes, their first launches); not part of the stream
+    warm = {}
+    for q in sorted(reqs, key=lambda q: len(q["b"])):
+        warm.setdefault((q["kind"], q["precision"]), q)
+    for q in warm.values():
+        srv.wait(srv.submit(q["kind"], q["rp"], q["ci"], q["v"], q["b"], q["tol"], maxiter,
+                            precision=q["precision"], inner_tol=1e-4))
+    gaps = np.random.default_rng(seed).exponential(1.0 / rate, len(reqs))
+    arrivals = np.cumsum(gaps) - gaps[0]
+    ids = [None] * len(reqs)
+
+    def producer():
+        t0 = time.perf_counter()
+        for k, q in enumerate(reqs):
+            dt = t0 + arrivals[k] - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            ids[k] = srv.submit(q["kind"], q["rp"], q["ci"], q["v"], q["b"], q["tol"], maxiter,
+                                precision=q["precision"], inner_tol=1e-4)
+
+    l0, s0 = srv.stats()
+    th = threading.Thread(target=producer)
+    th.start()
+    th.join()
+    res = [srv.wait(i) for i in ids]
+    l1, s1 = srv.stats()
+    srv.close()
+    return res, (l1 - l0, s1 - s0)
+
+
+def serve_loop_of_single_solves(D, h, reqs, maxiter):
+    """The comparison: requests one after another through the single-solve
+    entry points (upload, plan, plain FP64 solve, download); wall time."""
+    import torch
+    t0 = time.perf_counter()
+    iters = []
+    for q in reqs:
+        n = len(q["b"])
+        A = D.Crs(h, n, n, q["rp"], q["ci"], q["v"], validate=False)
+        db = torch.from_numpy(q["b"]).cuda()
+        dx = torch.zeros_like(db)
+        fn = D.cg_solve if q["kind"] == "cg" else D.bicgstab_solve
+        r = fn(A, db, dx, q["tol"], maxiter)
+        dx.cpu()
+        A.close()
+        iters.append(r.iters)
+    return time.perf_counter() - t0, iters
+
+
+def solve_bytes(q, iters):
+    """Algorithmic HBM bytes of a Jacobi-CG / BiCGSTAB solve (fused minimum
+    per iteration: one SpMV pass (two for BiCGSTAB) plus the vector traffic)."""
+    n = len(q["b"])
+    nnz = int(q["rp"][-1])
+    sp = nnz * 12 + (n + 1) * 4
+    return iters * (sp + 13 * n * 8 if q["kind"] == "cg" else 2 * sp + 22 * n * 8)
+
+
+def run_serve(args, wl, rank, world, local):
+    import torch
+    from monolish_b200 import device as D
+    torch.cuda.set_device(local)
+    count = args.size or wl["count"]
+    reqs = serve_requests(count, seed=4)
+    rates = [float(r) for r in args.rates.split(",")]
+    budget, lanes, maxiter = int(wl["budget"]), args.lanes, 100000
+    h = D.Handle()
+    sweep = []
+    clocks = ClockSampler(local)
+    head = None
+    for k, rate in enumerate(rates):
+        if k == len(rates) - 1:
+            clocks.start()
+        res, (launches, lane_solves) = serve_stream(D, reqs, rate, budget, lanes, 40 + k,
+                                                    maxiter)
+        lat = np.array([r.t_done - r.t_submit for r in res])
+        span = max(r.t_done for r in res) - min(r.t_submit for r in res)
+        entry = {"rate_req_s": rate, "solves_per_s": round(len(res) / span, 2),
+                 "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
+                 "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
+                 "makespan_s": round(span, 3),
+                 "all_converged": all(r.status == 0 for r in res),
+                 "ring_requests": sum(1 for r in res if r.path == 0),
+                 "lane_requests": sum(1 for r in res if r.path == 1)}
+        sweep.append(entry)
+        head = (res, span, launches, lane_solves, entry)
+    cl = clocks.stop()
+    res, span, launches, lane_solves, entry = head
+    loop_s = None
+    if not args.quick:
+        loop_s, _ = serve_loop_of_single_solves(D, h, reqs, maxiter)
+    h.close()
+    # true residual of every request, recomputed on the host in FP64
+    worst = max(true_relres(q["rp"], q["ci"], q["v"], q["b"], r.x) / q["rel"]
+                for q, r in zip(reqs, res))
+    peak, peak_kind = measured_peak()
+    bytes_all = float(sum(solve_bytes(q, r.iters) for q, r in zip(reqs, res)
+                          if q["precision"] == "fp64"))
+    h2d = int(sum(q["rp"].nbytes + q["ci"].nbytes + q["v"].nbytes + q["b"].nbytes
+                  for q in reqs))
+    d2h = int(sum(q["b"].nbytes for q in reqs))
+    value = len(res) / span
+    fam = {f: sum(1 for q in reqs if q["family"] == f) for f in ("cg2d", "cg3d", "bicgstab")}
+    out = {
+        "metric": METRIC_SERVE, "value": round(value, 2), "unit": "solves/s",
+        "n_gpus": world, "steps": 1, "warmup": args.warmup,
+        "ms_per_step": round(span * 1e3, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 / f32-inner mixed",
+        "data": "synthetic (seeded generators)",
+        "config": {"workload": f"open-loop stream of {count} requests (seed 4): CG on 2D/3D "
+                               "variable-coefficient diffusion or BiCGSTAB on convection-"
+                               "diffusion (Peclet U[0,20]), n log-uniform in [1e3, 2e6], tol "
+                               "1e-8 or 1e-10, FP64 or mixed, Poisson arrivals",
+                   "requests": count, "families": fam,
+                   "mixed_requests": sum(1 for q in reqs if q["precision"] == "mixed"),
+                   "rows_total": int(sum(len(q["b"]) for q in reqs)),
+                   "memory_budget_bytes": budget, "lanes": lanes,
+                   "headline_rate_req_s": rates[-1],
+                   "p50_ms": entry["p50_ms"], "p99_ms": entry["p99_ms"],
+                   "worst_true_rel_residual_over_tol": worst,
+                   "all_converged": entry["all_converged"],
+                   "l2": "no flush: each request's matrix is uploaded from the host",
+                   "parallelism": "one GPU: serving-kernel rings + worker lanes"},
+        "sweep": sweep,
+        "e2e": {"value": round(value, 2), "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "note": "the served stream is end to end: host CRS and b in, x out"},
+        "roofline": {"bound": "hbm", "achieved": round(bytes_all / span / 1e9, 1),
+                     "peak": peak, "unit": "GB/s",
+                     "frac": round(bytes_all / span / 1e9 / peak, 4), "peak_kind": peak_kind,
+                     "traffic": None,
+                     "note": "algorithmic solve bytes of the FP64 requests only / makespan"},
+        "gpu_launches": int(launches + lane_solves),
+        "gpu_launches_note": "serving-kernel launches + lane solves (a lower bound: each "
+                             "lane solve launches one graph or cluster kernel at least)",
+    }
+    if loop_s is not None:
+        out["loop_of_single_solves"] = {
+            "value": round(count / loop_s, 2), "unit": "solves/s",
+            "speedup_of_server": round(value / (count / loop_s), 2),
+            "note": "same requests one at a time, plain FP64, wall time"}
+    if not args.no_cpu:
+        cb = cpu_reference_serve(reqs, seconds=20.0)
+        if cb:
+            out["cpu_baseline"] = cb
+    if cl:
+        out["clocks"] = cl
+    return out
+
+
+def cpu_reference_serve(reqs, seconds):
+    """The reference's CPU CG / BiCGSTAB (Jacobi, plain FP64) on requests
+    taken in a seeded random order until `seconds` of solve time; solves/s
+    = solved / their summed time."""
+    import oracle
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    ref = oracle.reference_or_none()
+    if ref is None:
+        return None
+    threads = os.cpu_count() or 1
+    ref.set_threads(threads)
+    order = np.random.default_rng(99).permutation(len(reqs))
+    total, done = 0.0, 0
+    for k in order:
+        q = reqs[k]
+        st, it, res, x, sec = getattr(ref, q["kind"])(q["rp"], q["ci"], q["v"], q["b"],
+                                                      np.zeros(len(q["b"])), q["tol"], 100000)
+        total += sec
+        done += 1
+        if total > seconds:
+            break
+    return {"value": round(done / total, 3), "unit": "solves/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"{done} of {len(reqs)} requests in seeded random order, plain FP64 "
+                      f"(the reference has no mixed form), {total:.1f} s of solves"}
+
+
 # ---------------------------------------------------------- reference arm
 def run_reference(args, wl, rank, world):
     if rank != 0:
         return None
+    if wl["kind"] == "serve":
+        reqs = serve_requests(args.size or wl["count"], seed=4)
+        cb = cpu_reference_serve(reqs, seconds=60.0)
+        if cb is None:
+            return {"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) "
+                                                        "not present"}
+        return {"metric": METRIC_SERVE, "value": cb["value"], "unit": "solves/s",
+                "n_gpus": world, "steps": 1, "warmup": 0, "ms_per_step": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic (seeded generators)", "impl": "reference",
+                "config": {"workload": f"{len(reqs)}-request serving stream, solved one "
+                                       "after another on the host"},
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
     if wl["kind"] == "batch":
         threads = os.cpu_count() or 1
         systems, bs, tol = batch_inputs(wl)
@@ -701,8 +955,7 @@ def run_reference(args, wl, rank, world):
                                  "sample": f"{args.steps} full SpMVs (mean), {threads} threads"},
                 "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
-    port = oracle.restatement()
-    b = port.spmv(rp, ci, v, x)
+    b = host_matvec(rp, ci, v, x)
     tol = 1e-10 * float(np.linalg.norm(b))
     if ref is None:
         raise SystemExit("reference CPU build missing")
@@ -742,6 +995,9 @@ def main():
                     help="cluster engine: rows per CTA (0 = auto)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="SpMV kernel variant (default: autotuned per matrix)")
+    ap.add_argument("--rates", default="100,500,2000,5000",
+                    help="serve_stream: arrival rates (req/s); the last one is the headline")
+    ap.add_argument("--lanes", type=int, default=4, help="serve_stream: worker lanes")
     ap.add_argument("--quick", action="store_true",
                     help="timed steps only: no clock soak, no e2e, no CPU leg (profiling)")
     args = ap.parse_args()
@@ -769,6 +1025,8 @@ def main():
             out = run_spmv(args, wl, rank, world, local)
         elif wl["kind"] == "batch":
             out = run_batch(args, wl, rank, world, local)
+        elif wl["kind"] == "serve":
+            out = run_serve(args, wl, rank, world, local)
         else:
             out = run_solve(args, wl, rank, world, local)
     finally:
