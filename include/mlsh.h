@@ -142,6 +142,41 @@ int mlsh_spmv(mlsh_handle handle, mlsh_csr_plan plan, double alpha,
  * CRS::diag (src/utils/getvec/crs_getvec.cpp:8-55). */
 int mlsh_csr_diag(mlsh_handle handle, mlsh_csr_plan plan, void *d_diag);
 
+/* y = alpha*A^T*x + beta*y for the plan's n_rows x n_cols matrix (x has
+ * n_rows entries, y n_cols).  Replaces blas::matvec_T(CRS,x,y)
+ * (src/blas/matrix/matvec/crs_matvec.hpp:88-98; the reference's OSS path
+ * ignores alpha and beta, so parity uses alpha = 1, beta = 0).  The first
+ * call builds A^T on the device and keeps it with the plan;
+ * mlsh_csr_plan_values_changed refreshes its values. */
+int mlsh_spmv_transpose(mlsh_handle handle, mlsh_csr_plan plan, double alpha,
+                        const void *d_x, double beta, void *d_y);
+
+/* ------------------------------------------------------ matrix set-up -- */
+/* Sorts device COO arrays in place by (row, col), entries with equal
+ * (row, col) keeping their input order.  With merge != 0 each such run
+ * collapses to one entry holding the run's last value, and *new_nnz is the
+ * count left.  Replaces COO::sort(merge)
+ * (src/utils/at_insert_sort/at_insert_sort_coo.cpp:119-145), whose
+ * quicksort leaves the order of duplicates unspecified.  Indices outside
+ * [0,n_rows) x [0,n_cols) give MLSH_ERR_INVALID_ARG. */
+int mlsh_coo_sort(mlsh_handle handle, int n_rows, int n_cols, int64_t nnz, int *d_row,
+                  int *d_col, void *d_val, int dtype, int merge, int64_t *new_nnz);
+
+/* d_row_ptr[n_rows+1] of the CRS holding a row-sorted COO (its column and
+ * value arrays are the CRS's as they are).  Replaces the row-pointer pass of
+ * CRS::convert(COO&) (src/utils/convert/convert_crs.cpp:9-43).  Rows out of
+ * order or out of range give MLSH_ERR_INVALID_CSR. */
+int mlsh_coo_to_csr(mlsh_handle handle, int n_rows, int64_t nnz, const int *d_row,
+                    int *d_row_ptr);
+
+/* The transpose of an n_rows x n_cols CRS as an n_cols x n_rows CRS
+ * (d_rp_t[n_cols+1], d_ci_t[nnz], d_val_t[nnz]); each of its rows lists
+ * the entries of one column of A in row order.  No reference counterpart
+ * as a function (the reference transposes inside matvec_T). */
+int mlsh_csr_transpose(mlsh_handle handle, int n_rows, int n_cols, int nnz, const int *d_rp,
+                       const int *d_ci, const void *d_val, int dtype, int *d_rp_t,
+                       int *d_ci_t, void *d_val_t);
+
 /* ------------------------------------------------------ vector BLAS ----- */
 /* Results returned to host memory, like blas::dot/nrm2 on the reference GPU
  * path (src/blas/vector/dot.hpp:6-41, nrm2.hpp:6-36); synchronous. */

@@ -87,6 +87,10 @@ SIGNATURES = {
     "mlsh_csr_plan_get_variant": (i32, [vp, C.POINTER(i32), C.POINTER(i32)]),
     "mlsh_spmv": (i32, [vp, vp, f64, vp, f64, vp]),
     "mlsh_csr_diag": (i32, [vp, vp, vp]),
+    "mlsh_spmv_transpose": (i32, [vp, vp, f64, vp, f64, vp]),
+    "mlsh_coo_sort": (i32, [vp, i32, i32, i64, vp, vp, vp, i32, i32, C.POINTER(i64)]),
+    "mlsh_coo_to_csr": (i32, [vp, i32, i64, vp, vp]),
+    "mlsh_csr_transpose": (i32, [vp, i32, i32, i32, vp, vp, vp, i32, vp, vp, vp]),
     "mlsh_dot": (i32, [vp, i32, i64, vp, vp, C.POINTER(f64)]),
     "mlsh_nrm2": (i32, [vp, i32, i64, vp, C.POINTER(f64)]),
     "mlsh_dot_device": (i32, [vp, i32, i64, vp, vp, vp]),

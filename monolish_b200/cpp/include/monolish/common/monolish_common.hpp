@@ -237,7 +237,8 @@ template <typename Float> class COO {
     col_index.push_back(static_cast<int>(n));
     val.push_back(value);
   }
-  // stable sort by (row, col); duplicate entries are summed when merge
+  // sort by (row, col), equal (row, col) in input order; with merge each
+  // run of equal (row, col) becomes one entry holding the run's last value
   void sort(bool merge);
   [[nodiscard]] size_t get_row() const { return rowN; }
   [[nodiscard]] size_t get_col() const { return colN; }

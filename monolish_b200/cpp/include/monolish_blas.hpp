@@ -3,6 +3,7 @@
 //
 //   matvec  include/monolish/blas/monolish_matvec_blas.hpp:3972 (CRS x vector),
 //           alpha/beta overload src/blas/matrix/matvec/matvec_blas.cpp:3853
+//   matvec_T (CRS^T x vector)
 //   dot, nrm2, axpy, xpay, axpyz, copy
 //           include/monolish/blas/monolish_vector_blas.hpp
 #pragma once
@@ -17,6 +18,11 @@ void matvec(const double &a, const matrix::CRS<double> &A, const vector<double> 
             const double &b, vector<double> &y);
 void matvec(const float &a, const matrix::CRS<float> &A, const vector<float> &x,
             const float &b, vector<float> &y);
+
+// y = A^T x  (include/monolish/blas/monolish_matvec_blas.hpp:4283,
+// src/blas/matrix/matvec/crs_matvec.hpp:88-98)
+void matvec_T(const matrix::CRS<double> &A, const vector<double> &x, vector<double> &y);
+void matvec_T(const matrix::CRS<float> &A, const vector<float> &x, vector<float> &y);
 
 double dot(const vector<double> &x, const vector<double> &y);
 float dot(const vector<float> &x, const vector<float> &y);

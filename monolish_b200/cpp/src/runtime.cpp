@@ -195,38 +195,48 @@ template <typename Float> void COO<Float>::input_mm(const std::string filename) 
   }
 }
 
+// COO::sort (src/utils/at_insert_sort/at_insert_sort_coo.cpp:119-145) on
+// the device: the entries are copied up, sorted by (row, col) -- equal
+// (row, col) keeping their input order -- and, with merge, each such run
+// collapses to one entry with the run's last value; then copied back.
 template <typename Float> void COO<Float>::sort(bool merge) {
   const size_t n = val.size();
-  std::vector<size_t> perm(n);
-  std::iota(perm.begin(), perm.end(), 0);
-  std::stable_sort(perm.begin(), perm.end(), [&](size_t a, size_t b) {
-    return row_index[a] != row_index[b] ? row_index[a] < row_index[b]
-                                        : col_index[a] < col_index[b];
-  });
-  std::vector<int> r, c;
-  std::vector<Float> v;
-  r.reserve(n);
-  c.reserve(n);
-  v.reserve(n);
-  for (size_t k : perm) {
-    if (merge && !r.empty() && r.back() == row_index[k] && c.back() == col_index[k]) {
-      v.back() += val[k];
-    } else {
-      r.push_back(row_index[k]);
-      c.push_back(col_index[k]);
-      v.push_back(val[k]);
-    }
+  if (n == 0) return;
+  void *d_r = internal::dalloc(sizeof(int) * n);
+  void *d_c = internal::dalloc(sizeof(int) * n);
+  void *d_v = internal::dalloc(sizeof(Float) * n);
+  int64_t kept = 0;
+  try {
+    internal::h2d(d_r, row_index.data(), sizeof(int) * n);
+    internal::h2d(d_c, col_index.data(), sizeof(int) * n);
+    internal::h2d(d_v, val.data(), sizeof(Float) * n);
+    internal::check(mlsh_coo_sort(internal::handle(), (int)rowN, (int)colN, (int64_t)n,
+                                  static_cast<int *>(d_r), static_cast<int *>(d_c), d_v,
+                                  internal::dtype<Float>(), merge ? 1 : 0, &kept),
+                    "COO::sort");
+    row_index.resize((size_t)kept);
+    col_index.resize((size_t)kept);
+    val.resize((size_t)kept);
+    internal::d2h(row_index.data(), d_r, sizeof(int) * (size_t)kept);
+    internal::d2h(col_index.data(), d_c, sizeof(int) * (size_t)kept);
+    internal::d2h(val.data(), d_v, sizeof(Float) * (size_t)kept);
+  } catch (...) {
+    internal::dfree(d_r);
+    internal::dfree(d_c);
+    internal::dfree(d_v);
+    throw;
   }
-  row_index.swap(r);
-  col_index.swap(c);
-  val.swap(v);
+  internal::dfree(d_r);
+  internal::dfree(d_c);
+  internal::dfree(d_v);
 }
 
 template class COO<double>;
 template class COO<float>;
 
 // CRS from COO (src/utils/convert/convert_crs.cpp:9-43): entries must be
-// ordered by row; within a row their order is kept.
+// ordered by row (a COO that is not gets sorted first); within a row their
+// order is kept.  The row pointer is computed on the device.
 template <typename Float> void CRS<Float>::convert(COO<Float> &coo) {
   rowN = coo.get_row();
   colN = coo.get_col();
@@ -239,11 +249,22 @@ template <typename Float> void CRS<Float>::convert(COO<Float> &coo) {
   row_ptr.assign(rowN + 1, 0);
   col_ind.assign(coo.col_index.begin(), coo.col_index.end());
   alloc_val(n);
-  for (size_t k = 0; k < n; ++k) {
-    row_ptr[(size_t)coo.row_index[k] + 1]++;
-    val.get()[k] = coo.val[k];
+  std::copy(coo.val.begin(), coo.val.end(), val.get());
+  void *d_r = internal::dalloc(sizeof(int) * std::max<size_t>(n, 1));
+  void *d_p = internal::dalloc(sizeof(int) * (rowN + 1));
+  try {
+    if (n) internal::h2d(d_r, coo.row_index.data(), sizeof(int) * n);
+    internal::check(mlsh_coo_to_csr(internal::handle(), (int)rowN, (int64_t)n,
+                                    static_cast<const int *>(d_r), static_cast<int *>(d_p)),
+                    "CRS::convert");
+    internal::d2h(row_ptr.data(), d_p, sizeof(int) * (rowN + 1));
+  } catch (...) {
+    internal::dfree(d_r);
+    internal::dfree(d_p);
+    throw;
   }
-  for (size_t i = 0; i < rowN; ++i) row_ptr[i + 1] += row_ptr[i];
+  internal::dfree(d_r);
+  internal::dfree(d_p);
   gpu_status = std::make_shared<bool>(false);
   dev.reset();
 }
@@ -275,6 +296,18 @@ void matvec_t(double a, const matrix::CRS<T> &A, const vector<T> &x, double b, v
                   "matvec");
 }
 
+template <typename T>
+void matvec_tr(const matrix::CRS<T> &A, const vector<T> &x, vector<T> &y) {
+  need_device(A, "matvec_T");
+  need_device(x, "matvec_T");
+  need_device(y, "matvec_T");
+  if (A.get_row() != x.size() || A.get_col() != y.size())
+    throw std::runtime_error("error, matvec_T: size");
+  internal::check(mlsh_spmv_transpose(internal::handle(), A.device_plan(), 1.0,
+                                      x.device_data(), 0.0, y.device_data()),
+                  "matvec_T");
+}
+
 template <typename T> T dot_t(const vector<T> &x, const vector<T> &y) {
   need_device(x, "dot");
   need_device(y, "dot");
@@ -297,6 +330,12 @@ template <typename T> T nrm2_t(const vector<T> &x) {
 }  // namespace
 
 namespace blas {
+void matvec_T(const matrix::CRS<double> &A, const vector<double> &x, vector<double> &y) {
+  matvec_tr<double>(A, x, y);
+}
+void matvec_T(const matrix::CRS<float> &A, const vector<float> &x, vector<float> &y) {
+  matvec_tr<float>(A, x, y);
+}
 void matvec(const matrix::CRS<double> &A, const vector<double> &x, vector<double> &y) {
   matvec_t<double>(1.0, A, x, 0.0, y);
 }

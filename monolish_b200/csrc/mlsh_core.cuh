@@ -45,6 +45,10 @@ int cluster_serve_launch(const ServeRing &ring, int csize, int n_clusters, doubl
 void mixed_release(CsrPlan &p);
 void mixed_invalidate(CsrPlan &p);
 
+// The cached transpose of a plan (mlsh_sort.cu).
+void transpose_release(CsrPlan &p);
+void transpose_invalidate(CsrPlan &p);
+
 // Solver-side resources kept on the handle / plan (mlsh_krylov.cu).
 void release_solver_graphs(Handle &h);
 void release_plan_extras(CsrPlan &p);

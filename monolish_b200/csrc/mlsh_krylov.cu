@@ -792,9 +792,13 @@ void release_solver_graphs(Handle &h) {
 void release_plan_extras(CsrPlan &p) {
   if (p.handle) purge_graphs(*p.handle, &p, nullptr);
   mixed_release(p);
+  transpose_release(p);
 }
 
-void invalidate_plan_extras(CsrPlan &p) { mixed_invalidate(p); }
+void invalidate_plan_extras(CsrPlan &p) {
+  mixed_invalidate(p);
+  transpose_invalidate(p);
+}
 
 }  // namespace mlsh
 

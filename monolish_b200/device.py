@@ -172,6 +172,47 @@ class Crs:
     def diag(self, out):
         _abi.check(self.lib.mlsh_csr_diag(self.handle.h, self.plan, ptr(out)), "diag")
 
+    def matvec_t(self, x, y, alpha=1.0, beta=0.0):
+        """y = alpha A^T x + beta y (blas::matvec_T)."""
+        _abi.check(self.lib.mlsh_spmv_transpose(self.handle.h, self.plan, alpha, ptr(x), beta,
+                                                ptr(y)), "spmv_transpose")
+
+    def values_changed(self):
+        _abi.check(self.lib.mlsh_csr_plan_values_changed(self.plan), "values_changed")
+
+
+def coo_sort(handle: Handle, n_rows, n_cols, d_row, d_col, d_val, merge=True):
+    """Sort device COO tensors in place by (row, col); returns the entry
+    count (after merging duplicates when `merge`)."""
+    k = C.c_int64()
+    _abi.check(handle.lib.mlsh_coo_sort(
+        handle.h, int(n_rows), int(n_cols), int(d_row.numel()), ptr(d_row), ptr(d_col),
+        ptr(d_val), _dtype_code(np.dtype(str(d_val.dtype).replace("torch.", ""))), int(merge),
+        C.byref(k)), "coo_sort")
+    return k.value
+
+
+def coo_to_csr(handle: Handle, n_rows, d_row, nnz=None):
+    """Row pointer (device int32 tensor) of a row-sorted device COO."""
+    nnz = int(d_row.numel()) if nnz is None else int(nnz)
+    rp = torch.empty(n_rows + 1, dtype=torch.int32, device=d_row.device)
+    _abi.check(handle.lib.mlsh_coo_to_csr(handle.h, int(n_rows), nnz, ptr(d_row), ptr(rp)),
+               "coo_to_csr")
+    return rp
+
+
+def csr_transpose(handle: Handle, n_rows, n_cols, d_rp, d_ci, d_val):
+    """(rp_t, ci_t, val_t) device tensors of A^T."""
+    nnz = int(d_ci.numel())
+    rp_t = torch.empty(n_cols + 1, dtype=torch.int32, device=d_rp.device)
+    ci_t = torch.empty(max(nnz, 1), dtype=torch.int32, device=d_rp.device)
+    v_t = torch.empty(max(nnz, 1), dtype=d_val.dtype, device=d_rp.device)
+    _abi.check(handle.lib.mlsh_csr_transpose(
+        handle.h, int(n_rows), int(n_cols), nnz, ptr(d_rp), ptr(d_ci), ptr(d_val),
+        _dtype_code(np.dtype(str(d_val.dtype).replace("torch.", ""))), ptr(rp_t), ptr(ci_t),
+        ptr(v_t)), "csr_transpose")
+    return rp_t, ci_t[:nnz], v_t[:nnz]
+
 
 @dataclass
 class SolveResult:

@@ -43,6 +43,12 @@ class Restatement:
         for nm in ("oracle_spmv_d", "oracle_spmv_s"):
             getattr(lib, nm).argtypes = [I, P, P, P, P, P]
         lib.oracle_spmv_ab_d.argtypes = [I, P, P, P, D, P, D, P]
+        for nm in ("oracle_spmv_t_d", "oracle_spmv_t_s"):
+            getattr(lib, nm).argtypes = [I, I, P, P, P, P, P]
+        lib.oracle_coo_sort_d.argtypes = [L, P, P, P, I]
+        lib.oracle_coo_sort_d.restype = L
+        lib.oracle_coo_rowptr.argtypes = [I, L, P, P]
+        lib.oracle_csr_transpose_d.argtypes = [I, I, P, P, P, P, P, P]
         lib.oracle_dot_d.argtypes = [L, P, P]
         lib.oracle_dot_d.restype = D
         lib.oracle_nrm2_d.argtypes = [L, P]
@@ -65,6 +71,35 @@ class Restatement:
         y = y.copy()
         self.lib.oracle_spmv_ab_d(len(rp) - 1, _p(rp), _p(ci), _p(v), alpha, _p(x), beta, _p(y))
         return y
+
+    def spmv_t(self, rp, ci, v, x, n_cols):
+        """y = A^T x (the reference's serial row loop)."""
+        y = np.zeros(n_cols, v.dtype)
+        fn = self.lib.oracle_spmv_t_d if v.dtype == np.float64 else self.lib.oracle_spmv_t_s
+        fn(len(rp) - 1, n_cols, _p(rp), _p(ci), _p(v), _p(x), _p(y))
+        return y
+
+    def coo_sort(self, row, col, val, merge):
+        r = np.array(row, np.int32)
+        c = np.array(col, np.int32)
+        v = np.array(val, np.float64)
+        k = self.lib.oracle_coo_sort_d(len(r), _p(r), _p(c), _p(v), int(merge))
+        return r[:k].copy(), c[:k].copy(), v[:k].copy()
+
+    def coo_rowptr(self, n_rows, row):
+        row = np.ascontiguousarray(row, np.int32)
+        rp = np.zeros(n_rows + 1, np.int32)
+        self.lib.oracle_coo_rowptr(n_rows, len(row), _p(row), _p(rp))
+        return rp
+
+    def csr_transpose(self, rp, ci, v, n_cols):
+        nnz = int(rp[-1])
+        rp_t = np.zeros(n_cols + 1, np.int32)
+        ci_t = np.zeros(nnz, np.int32)
+        v_t = np.zeros(nnz, np.float64)
+        self.lib.oracle_csr_transpose_d(len(rp) - 1, n_cols, _p(rp), _p(ci), _p(v), _p(rp_t),
+                                        _p(ci_t), _p(v_t))
+        return rp_t, ci_t, v_t
 
     def dot(self, x, y):
         return self.lib.oracle_dot_d(len(x), _p(x), _p(y))
@@ -120,6 +155,12 @@ class Reference:
         lib.ref_random_vector_d.argtypes = [L, D, D, C.c_uint, P]
         lib.ref_laplacian_2d5p_d.argtypes = [I, I, P, P, P]
         lib.ref_laplacian_2d5p_d.restype = L
+        lib.ref_spmv_t_d.argtypes = [I, I, I, P, P, P, P, P]
+        lib.ref_spmv_t_d.restype = I
+        lib.ref_coo_sort_d.argtypes = [I, I, L, P, P, P, I]
+        lib.ref_coo_sort_d.restype = L
+        lib.ref_coo_to_crs_d.argtypes = [I, I, L, P, P, P, P]
+        lib.ref_coo_to_crs_d.restype = I
 
     def threads(self):
         return self.lib.ref_max_threads()
@@ -134,6 +175,27 @@ class Reference:
         fn = self.lib.ref_spmv_d if v.dtype == np.float64 else self.lib.ref_spmv_s
         fn(n, int(rp[-1]), _p(rp), _p(ci), _p(v), _p(x), _p(y), reps, _p(sec))
         return y, float(sec[0]), float(sec[1])
+
+    def spmv_t(self, rp, ci, v, x, n_cols):
+        y = np.zeros(n_cols, np.float64)
+        self.lib.ref_spmv_t_d(len(rp) - 1, n_cols, int(rp[-1]), _p(rp), _p(ci), _p(v), _p(x),
+                              _p(y))
+        return y
+
+    def coo_sort(self, n_rows, n_cols, row, col, val, merge):
+        r = np.array(row, np.int32)
+        c = np.array(col, np.int32)
+        v = np.array(val, np.float64)
+        k = self.lib.ref_coo_sort_d(n_rows, n_cols, len(r), _p(r), _p(c), _p(v), int(merge))
+        return r[:k].copy(), c[:k].copy(), v[:k].copy()
+
+    def coo_rowptr(self, n_rows, n_cols, row, col, val):
+        row = np.ascontiguousarray(row, np.int32)
+        col = np.ascontiguousarray(col, np.int32)
+        val = np.ascontiguousarray(val, np.float64)
+        rp = np.zeros(n_rows + 1, np.int32)
+        self.lib.ref_coo_to_crs_d(n_rows, n_cols, len(row), _p(row), _p(col), _p(val), _p(rp))
+        return rp
 
     def _solve(self, name, rp, ci, v, b, x0, tol, maxiter, precond=1):
         sfx = "d" if v.dtype == np.float64 else "s"

@@ -62,6 +62,86 @@ void oracle_spmv_ab_d(int n, const int *rp, const int *ci, const double *v,
   }
 }
 
+/* ------------------------------------------------------ transposed SpMV --- */
+void oracle_spmv_t_d(int n_rows, int n_cols, const int *rp, const int *ci,
+                     const double *v, const double *x, double *y) {
+  for (int j = 0; j < n_cols; j++) y[j] = 0.0;
+  for (int i = 0; i < n_rows; i++)
+    for (int k = rp[i]; k < rp[i + 1]; k++) y[ci[k]] += v[k] * x[i];
+}
+
+void oracle_spmv_t_s(int n_rows, int n_cols, const int *rp, const int *ci,
+                     const float *v, const float *x, float *y) {
+  for (int j = 0; j < n_cols; j++) y[j] = 0.0f;
+  for (int i = 0; i < n_rows; i++)
+    for (int k = rp[i]; k < rp[i + 1]; k++) y[ci[k]] += v[k] * x[i];
+}
+
+/* ------------------------------------------------------ COO / transpose --- */
+typedef struct {
+  int row, col;
+  long idx;
+} coo_key;
+
+static int coo_key_cmp(const void *a, const void *b) {
+  const coo_key *p = (const coo_key *)a, *q = (const coo_key *)b;
+  if (p->row != q->row) return p->row < q->row ? -1 : 1;
+  if (p->col != q->col) return p->col < q->col ? -1 : 1;
+  return p->idx < q->idx ? -1 : (p->idx > q->idx ? 1 : 0);
+}
+
+long oracle_coo_sort_d(long nnz, int *row, int *col, double *val, int merge) {
+  if (nnz <= 0) return 0;
+  coo_key *k = (coo_key *)malloc(sizeof(coo_key) * (size_t)nnz);
+  double *v = (double *)malloc(sizeof(double) * (size_t)nnz);
+  for (long i = 0; i < nnz; i++) {
+    k[i].row = row[i];
+    k[i].col = col[i];
+    k[i].idx = i;
+    v[i] = val[i];
+  }
+  qsort(k, (size_t)nnz, sizeof(coo_key), coo_key_cmp);
+  long out = 0;
+  for (long i = 0; i < nnz; i++) {
+    if (merge && out > 0 && row[out - 1] == k[i].row && col[out - 1] == k[i].col) {
+      val[out - 1] = v[k[i].idx]; /* the run keeps its last value */
+      continue;
+    }
+    row[out] = k[i].row;
+    col[out] = k[i].col;
+    val[out] = v[k[i].idx];
+    out++;
+  }
+  free(k);
+  free(v);
+  return out;
+}
+
+void oracle_coo_rowptr(int n_rows, long nnz, const int *row, int *rp) {
+  /* rp[i] = number of entries with row < i */
+  long k = 0;
+  for (int i = 0; i <= n_rows; i++) {
+    while (k < nnz && row[k] < i) k++;
+    rp[i] = (int)k;
+  }
+}
+
+void oracle_csr_transpose_d(int n_rows, int n_cols, const int *rp, const int *ci,
+                            const double *v, int *rp_t, int *ci_t, double *v_t) {
+  for (int j = 0; j <= n_cols; j++) rp_t[j] = 0;
+  for (int k = 0; k < rp[n_rows]; k++) rp_t[ci[k] + 1]++;
+  for (int j = 0; j < n_cols; j++) rp_t[j + 1] += rp_t[j];
+  int *fill = (int *)malloc(sizeof(int) * (size_t)(n_cols > 0 ? n_cols : 1));
+  for (int j = 0; j < n_cols; j++) fill[j] = rp_t[j];
+  for (int i = 0; i < n_rows; i++)
+    for (int k = rp[i]; k < rp[i + 1]; k++) {
+      const int p = fill[ci[k]]++;
+      ci_t[p] = i;
+      v_t[p] = v[k];
+    }
+  free(fill);
+}
+
 /* ---------------------------------------------------------- reductions --- */
 double oracle_dot_d(long n, const double *x, const double *y) {
   double s = 0.0;

@@ -29,6 +29,26 @@ void oracle_spmv_s(int n, const int *rp, const int *ci, const float *v,
 void oracle_spmv_ab_d(int n, const int *rp, const int *ci, const double *v,
                       double alpha, const double *x, double beta, double *y);
 
+/* y = A^T x for an n_rows x n_cols CRS A: y zeroed, then rows in order,
+ * y[col] += val * x[row] (src/blas/matrix/matvec/crs_matvec.hpp:88-98). */
+void oracle_spmv_t_d(int n_rows, int n_cols, const int *rp, const int *ci,
+                     const double *v, const double *x, double *y);
+void oracle_spmv_t_s(int n_rows, int n_cols, const int *rp, const int *ci,
+                     const float *v, const float *x, float *y);
+
+/* COO::sort (src/utils/at_insert_sort/at_insert_sort_coo.cpp:119-145):
+ * entries ordered by (row, col); with `merge`, each run of equal (row,
+ * col) collapses to one entry holding the run's last value.  Ties keep
+ * input order (the reference's quicksort leaves it unspecified).  Returns
+ * the entry count after merging; arrays are rewritten in place. */
+long oracle_coo_sort_d(long nnz, int *row, int *col, double *val, int merge);
+/* CRS::convert(COO) row pointer (src/utils/convert/convert_crs.cpp:9-43)
+ * for entries sorted by row. */
+void oracle_coo_rowptr(int n_rows, long nnz, const int *row, int *rp);
+/* The transpose as CRS: entries of each column in row order. */
+void oracle_csr_transpose_d(int n_rows, int n_cols, const int *rp, const int *ci,
+                            const double *v, int *rp_t, int *ci_t, double *v_t);
+
 double oracle_dot_d(long n, const double *x, const double *y);
 double oracle_nrm2_d(long n, const double *x);
 double oracle_dot_s(long n, const float *x, const float *y);

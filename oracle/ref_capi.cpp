@@ -12,6 +12,7 @@
 //   - equation::CG::solve: src/equation/cg.cpp:13-116
 //   - equation::BiCGSTAB::solve: src/equation/bicgstab.cpp:13-166
 //   - equation::Jacobi as preconditioner: src/equation/jacobi.cpp:12-61
+//   - blas::matvec_T, COO::sort, CRS(COO&): see the entry points below
 // Nothing in the product links against this file.
 #include <chrono>
 #include <cstdint>
@@ -96,6 +97,42 @@ int solve_impl(int n, int nnz, const int *rp, const int *ci, const T *v,
 } // namespace
 
 extern "C" {
+
+// y = A^T x through blas::matvec_T (src/blas/matrix/matvec/crs_matvec.hpp:88-98
+// for the OSS path) on an n_rows x n_cols CRS<double>.
+int ref_spmv_t_d(int n_rows, int n_cols, int nnz, const int *rp, const int *ci,
+                 const double *v, const double *x, double *y) {
+  monolish::matrix::CRS<double> A(n_rows, n_cols, nnz, rp, ci, v);
+  monolish::vector<double> xv(x, x + n_rows);
+  monolish::vector<double> yv(n_cols, 0.0);
+  monolish::blas::matvec_T(A, xv, yv);
+  std::memcpy(y, yv.data(), sizeof(double) * n_cols);
+  return 0;
+}
+
+// COO<double>::sort(merge) (src/utils/at_insert_sort/at_insert_sort_coo.cpp:119-145)
+// on a COO built from raw arrays; the sorted entries are written back and
+// their count returned.
+long ref_coo_sort_d(int n_rows, int n_cols, long nnz, int *row, int *col, double *val,
+                    int merge) {
+  monolish::matrix::COO<double> A(n_rows, n_cols, nnz, row, col, val);
+  A.sort(merge != 0);
+  const long out = (long)A.get_nnz();
+  std::memcpy(row, A.row_index.data(), sizeof(int) * out);
+  std::memcpy(col, A.col_index.data(), sizeof(int) * out);
+  std::memcpy(val, A.data(), sizeof(double) * out);
+  return out;
+}
+
+// CRS<double>(COO&) (src/utils/convert/convert_crs.cpp:9-43): the row
+// pointer built from a row-sorted COO.
+int ref_coo_to_crs_d(int n_rows, int n_cols, long nnz, const int *row, const int *col,
+                     const double *val, int *rp) {
+  monolish::matrix::COO<double> A(n_rows, n_cols, nnz, row, col, val);
+  monolish::matrix::CRS<double> B(A);
+  std::memcpy(rp, B.row_ptr.data(), sizeof(int) * (n_rows + 1));
+  return 0;
+}
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
 void ref_set_threads(int n) { omp_set_num_threads(n); }

@@ -88,6 +88,32 @@ template <typename T> bool run(size_t n, double tol, double mv_tol) {
   u.recv();
   ok &= check_vec("matvec", u, mv, mv_tol);
 
+  // COO -> CRS on the device from unsorted entries with one repeated
+  // (row, col) (COO::sort keeps its last value), then matvec_T
+  {
+    const size_t m = 7, nc = 5;
+    const std::vector<int> r = {3, 0, 6, 2, 0, 3, 5, 1, 4, 6};
+    const std::vector<int> c = {1, 4, 0, 2, 1, 1, 3, 0, 4, 2};
+    const std::vector<T> vals = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10};
+    matrix::COO<T> C(m, nc, r.size(), r.data(), c.data(), vals.data());
+    C.sort(true);
+    ok &= C.get_nnz() == 9;
+    for (size_t k = 1; k < C.get_nnz(); ++k)
+      ok &= C.row_index[k - 1] < C.row_index[k] ||
+            (C.row_index[k - 1] == C.row_index[k] && C.col_index[k - 1] < C.col_index[k]);
+    std::vector<double> dense(m * nc, 0.0);
+    for (size_t k = 0; k < r.size(); ++k) dense[(size_t)r[k] * nc + (size_t)c[k]] = vals[k];
+    matrix::CRS<T> B(C);
+    vector<T> xr(m, -1.0, 1.0, 3u), yr(nc, 0.0);
+    std::vector<double> yt(nc, 0.0);
+    for (size_t i = 0; i < m; ++i)
+      for (size_t j = 0; j < nc; ++j) yt[j] += dense[i * nc + j] * (double)xr.data()[i];
+    util::send(B, xr, yr);
+    blas::matvec_T(B, xr, yr);
+    yr.recv();
+    ok &= check_vec("matvec_T", yr, yt, mv_tol);
+  }
+
   // diag + Jacobi create/apply
   vector<T> dg(A.get_row(), 0.0);
   dg.send();

@@ -24,6 +24,14 @@ Cases (all small, so the CPU restatement replays them in seconds):
                four rows exceed one 1,792-nonzero SpMV tile), double and
                float.
   blas1        dot/nrm2/axpy/xpay/axpyz on n = 1,000.
+  setup        blas::matvec_T on a 1,500 x 1,000 Zipf(2) matrix and on
+               the 16x16 Poisson matrix; COO::sort(merge) of a shuffled
+               COO (400 x 300, 3,000 distinct entries) with the CRS(COO&)
+               row pointer; the (row, col) sequence COO::sort leaves when
+               600 duplicates are added (their kept values depend on the
+               reference's quicksort order and are not stored).
+
+    python tests/golden/make_golden.py setup   # that case only
 """
 import os
 import sys
@@ -45,9 +53,43 @@ def tridiag3():
     return 3, rp, ci, v
 
 
-def main():
+def setup_case(ref):
+    out = {}
+    n, rp, ci, v = W.zipf(1500, seed=3, maxlen=600, ncols=1000)
+    x = W.uniform_mt(n, -1.0, 1.0, 31)
+    out.update(zipf_rp=rp, zipf_ci=ci, zipf_v=v, zipf_x=x,
+               zipf_yt=ref.spmv_t(rp, ci, v, x, 1000))
+    n, rp, ci, v = W.poisson2d(16)
+    x = W.uniform_mt(n, -1.0, 1.0, 32)
+    out.update(pois_x=x, pois_yt=ref.spmv_t(rp, ci, v, x, n))
+    rng = np.random.default_rng(33)
+    m, k, cols = 400, 3000, 300
+    lin = rng.choice(m * cols, k, replace=False)
+    row, col = (lin // cols).astype(np.int32), (lin % cols).astype(np.int32)
+    val = rng.uniform(-1.0, 1.0, k)
+    sr, sc, sv = ref.coo_sort(m, cols, row, col, val, True)
+    out.update(coo_row=row, coo_col=col, coo_val=val, sorted_row=sr, sorted_col=sc,
+               sorted_val=sv, rowptr=ref.coo_rowptr(m, cols, sr, sc, sv))
+    d = rng.integers(0, k, 600)
+    row2, col2 = np.concatenate([row, row[d]]), np.concatenate([col, col[d]])
+    val2 = np.concatenate([val, rng.uniform(-1.0, 1.0, 600)])
+    dr, dc, _ = ref.coo_sort(m, cols, row2, col2, val2, True)
+    nr, nc, _ = ref.coo_sort(m, cols, row2, col2, val2, False)
+    out.update(dup_row=row2, dup_col=col2, dup_val=val2, dup_merged_row=dr, dup_merged_col=dc,
+               dup_all_row=nr, dup_all_col=nc)
+    return out
+
+
+def main(only=None):
     ref = oracle.Reference()
     out = {}
+    if only == "setup":
+        out["setup"] = setup_case(ref)
+        for name, case in out.items():
+            path = os.path.join(HERE, f"{name}.npz")
+            np.savez_compressed(path, **case)
+            print("wrote", path, os.path.getsize(path), "bytes")
+        return
 
     # ---- tridiag3 (reference test/test.mtx) ----
     n, rp, ci, v = tridiag3()
@@ -105,6 +147,8 @@ def main():
                         axpy=ref.axpy(0.75, a, c), xpay=ref.xpay(0.75, a, c),
                         axpyz=ref.axpyz(0.75, a, c))
 
+    out["setup"] = setup_case(ref)
+
     for name, case in out.items():
         path = os.path.join(HERE, f"{name}.npz")
         np.savez_compressed(path, **case)
@@ -112,4 +156,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else None)

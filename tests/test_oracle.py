@@ -122,3 +122,45 @@ def test_status_codes_match_reference(restatement, reference):
     a = restatement.cg(rp, ci, v, b, np.zeros(n), 1e-30, 5)
     r = reference.cg(rp, ci, v, b, np.zeros(n), 1e-30, 5)
     assert a[0] == r[0] == -2 and a[1] == r[1] == 5
+
+
+def test_setup_routines_match_reference_golden(restatement):
+    """Transposed SpMV, COO sort/merge and the COO -> CRS row pointer of the
+    restatement against the reference's blas::matvec_T, COO::sort and
+    CRS(COO&) outputs."""
+    g = golden("setup")
+    yt = restatement.spmv_t(g["zipf_rp"], g["zipf_ci"], g["zipf_v"], g["zipf_x"], 1000)
+    assert np.array_equal(yt, g["zipf_yt"])  # same serial loop: identical bits
+    n, rp, ci, v = W.poisson2d(16)
+    assert np.array_equal(restatement.spmv_t(rp, ci, v, g["pois_x"], n), g["pois_yt"])
+    sr, sc, sv = restatement.coo_sort(g["coo_row"], g["coo_col"], g["coo_val"], True)
+    assert np.array_equal(sr, g["sorted_row"]) and np.array_equal(sc, g["sorted_col"])
+    assert np.array_equal(sv, g["sorted_val"])
+    assert np.array_equal(restatement.coo_rowptr(400, sr), g["rowptr"])
+    dr, dc, _ = restatement.coo_sort(g["dup_row"], g["dup_col"], g["dup_val"], True)
+    assert np.array_equal(dr, g["dup_merged_row"]) and np.array_equal(dc, g["dup_merged_col"])
+    nr, nc, _ = restatement.coo_sort(g["dup_row"], g["dup_col"], g["dup_val"], False)
+    assert np.array_equal(nr, g["dup_all_row"]) and np.array_equal(nc, g["dup_all_col"])
+    # the restatement's transpose is scipy's CSR transpose with sorted indices
+    import scipy.sparse as sp
+    rp_t, ci_t, v_t = restatement.csr_transpose(g["zipf_rp"], g["zipf_ci"], g["zipf_v"], 1000)
+    At = sp.csr_matrix((g["zipf_v"], g["zipf_ci"], g["zipf_rp"]), shape=(1500, 1000)).T.tocsr()
+    At.sort_indices()
+    assert np.array_equal(rp_t, At.indptr) and np.array_equal(ci_t, At.indices)
+    assert np.array_equal(v_t, At.data)
+
+
+def test_setup_routines_match_reference_live(restatement, reference):
+    n, rp, ci, v = W.zipf(5000, seed=9, maxlen=3000, ncols=3500)
+    x = W.uniform_mt(n, -1.0, 1.0, 41)
+    assert np.array_equal(restatement.spmv_t(rp, ci, v, x, 3500),
+                          reference.spmv_t(rp, ci, v, x, 3500))
+    rng = np.random.default_rng(42)
+    lin = rng.choice(900 * 700, 20000, replace=False)
+    row, col = (lin // 700).astype(np.int32), (lin % 700).astype(np.int32)
+    val = rng.uniform(-1, 1, 20000)
+    a = restatement.coo_sort(row, col, val, True)
+    b = reference.coo_sort(900, 700, row, col, val, True)
+    assert all(np.array_equal(p, q) for p, q in zip(a, b))
+    assert np.array_equal(restatement.coo_rowptr(900, a[0]),
+                          reference.coo_rowptr(900, 700, *b))
