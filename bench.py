@@ -386,11 +386,12 @@ def run_solve(args, wl, rank, world, local):
 
     def plain_fn(A_, b_, x_, tol_, maxiter_):
         return base_fn(A_, b_, x_, tol_, maxiter_, engine=engine,
-                       cluster_rows=args.cluster_rows)
+                       cluster_rows=args.cluster_rows, use_graph=not args.eager)
 
     def fn(A_, b_, x_, tol_, maxiter_):
         if args.precision == "mixed":
-            return mixed_fn(A_, b_, x_, tol_, maxiter_, inner_tol=1e-4, engine=engine)
+            return mixed_fn(A_, b_, x_, tol_, maxiter_, inner_tol=1e-4, engine=engine,
+                            use_graph=not args.eager)
         return plain_fn(A_, b_, x_, tol_, maxiter_)
 
     stream = torch.cuda.current_stream()
@@ -998,6 +999,9 @@ def main():
     ap.add_argument("--rates", default="100,500,2000,5000",
                     help="serve_stream: arrival rates (req/s); the last one is the headline")
     ap.add_argument("--lanes", type=int, default=4, help="serve_stream: worker lanes")
+    ap.add_argument("--eager", action="store_true",
+                    help="solver workloads: launch iterations one by one instead of a graph "
+                         "(kernel-level profiling)")
     ap.add_argument("--quick", action="store_true",
                     help="timed steps only: no clock soak, no e2e, no CPU leg (profiling)")
     args = ap.parse_args()

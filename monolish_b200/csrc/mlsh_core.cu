@@ -41,21 +41,22 @@ void build_tiles(const int *rp, int n_rows, std::vector<Tile> &tiles,
       for (int c = 0; c < nch; ++c) {
         const int b = rp[r] + c * kTileNnz;
         const int e = std::min(b + kTileNnz, rp[r + 1]);
-        tiles.push_back(Tile{r, -(li + 1), b, e});
+        tiles.push_back(Tile{r, -(li + 1), b, e, 0, {0, 0, 0}});
       }
       n_chunks += nch;
       ++r;
       continue;
     }
     const int rb = r;
-    int nnz = 0;
+    int nnz = 0, longest = 0;
     while (r < n_rows && r - rb < kTileRows) {
       const int l = rp[r + 1] - rp[r];
       if (l > kTileNnz || nnz + l > kTileNnz) break;
       nnz += l;
+      longest = std::max(longest, l);
       ++r;
     }
-    tiles.push_back(Tile{rb, r, rp[rb], rp[r]});
+    tiles.push_back(Tile{rb, r, rp[rb], rp[r], longest <= kShortRow ? 1 : 0, {0, 0, 0}});
   }
 }
 

@@ -49,6 +49,12 @@ void mixed_invalidate(CsrPlan &p);
 void transpose_release(CsrPlan &p);
 void transpose_invalidate(CsrPlan &p);
 
+// Mixed-precision BiCGSTAB with reliable updates on the kernel engine
+// (mlsh_krylov.cu): p FP64, p32 its FP32 copy, r64 an FP64 work vector.
+int mixed_bicgstab_kernels(Handle &h, CsrPlan &p, CsrPlan &p32, double *r64, const void *b,
+                           void *x, const mlsh_solver_opts *opts, double inner_tol,
+                           mlsh_solver_result *res);
+
 // Solver-side resources kept on the handle / plan (mlsh_krylov.cu).
 void release_solver_graphs(Handle &h);
 void release_plan_extras(CsrPlan &p);

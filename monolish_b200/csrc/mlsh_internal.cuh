@@ -22,7 +22,7 @@ constexpr int kTileNnz = 1792;  // = 256 rows x 7 nonzeros (7-point stencil)
 constexpr int kConsumers = 256;  // consumer threads per CTA (8 warps)
 constexpr int kSpmvThreads = kConsumers + 32;  // + one producer warp
 constexpr int kShortRow = 8;     // rows up to this length: thread-per-row sum
-constexpr int kDefaultSpmvVariant = 1;  // until the plan is autotuned
+constexpr int kDefaultSpmvVariant = 2;  // until the plan is autotuned
 
 // Elementwise / reduction kernels.
 constexpr int kVecThreads = 256;
@@ -39,11 +39,14 @@ constexpr int kRunning = 1;
 // --------------------------------------------------------- tile record ---
 // Normal tile: rows [row_begin, row_end), nonzeros [nnz_begin, nnz_end).
 // Chunk of a long row: row_begin = row, row_end = -(long_index + 1).
-struct Tile {
+// short_only: every row of a normal tile has at most kShortRow entries.
+struct __align__(16) Tile {
   int row_begin;
   int row_end;
   int nnz_begin;
   int nnz_end;
+  int short_only;
+  int pad[3];
 };
 
 struct LongRow {
@@ -81,6 +84,17 @@ struct SolverState {
   int pad1;
   double *hist;    // optional residual history (device), hist_cap entries
   long long hist_cap;
+  // mixed precision with reliable updates: FP32 iteration vectors hold the
+  // FP64 quantities divided by `scale`; x and the true residual are FP64
+  double scale;
+  double rr64;      // ||b - A x||^2 of the last FP64 residual
+  double rel_true;  // true ||r|| at the last update
+  double delta;     // update once the iterated ||r|| < delta * rel_true
+  long long outer;  // FP64 residual evaluations after the first
+  int upd;          // 1: the update kernels run at the start of the next pass
+  int noupd;        // 1 - upd (the update kernels' skip flag)
+  int first;        // 1: the next iteration starts a fresh Krylov space
+  int pending;      // status the iteration ended with, applied after the update
 };
 
 // ------------------------------------------------------------- objects ---

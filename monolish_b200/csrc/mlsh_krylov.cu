@@ -278,6 +278,219 @@ struct BiXRBody : NoPrep {  // omega = (t,s)/(t,t); x += a phat + w shat; r = s 
   }
 };
 
+// ------------------------------------------ mixed precision, BiCGSTAB --
+// FP32 BiCGSTAB iterations on A32 with reliable updates (Sleijpen & van der
+// Vorst, "Reliable updated residuals in hybrid Bi-CG methods", Computing
+// 56 (1996); the mixed-precision form of Clark et al., Comput. Phys. Commun.
+// 181 (2010)): the FP32 iterate x32 holds the correction since the last
+// update; whenever the iterated residual has dropped by `delta` since the
+// last true residual (or the iteration ends), x += scale * x32 in FP64, the
+// true residual b - A x is formed with the FP64 matrix, and the FP32
+// iteration continues from it without restarting its Krylov space.  The
+// stopping test is on the true FP64 residual.
+
+// Initial pass: r32 = r64 / s, r0 = r32, x32 = 0 with s = ||r64||.
+struct MixInitBody {
+  const double *r64;
+  float *r32;
+  float *r0;
+  float *x32;
+  SolverState *st;
+  CondRef cond;
+  double inv;
+  __device__ void prepare() { inv = st->rr64 > 0.0 ? 1.0 / sqrt(st->rr64) : 1.0; }
+  __device__ void operator()(int64_t i, double *acc) const {
+    const float r = (float)(r64[i] * inv);
+    r32[i] = r;
+    r0[i] = r;
+    x32[i] = 0.0f;
+    acc[0] += (double)r * (double)r;
+    acc[1] += (double)r * (double)r;
+  }
+  __device__ void finish(const double *s) {
+    const double tr = sqrt(st->rr64);
+    st->scale = tr > 0.0 ? tr : 1.0;
+    st->rel_true = tr;
+    st->resid = tr;
+    st->outer = 0;
+    if (st->hist != nullptr && st->hist_cap > 0) st->hist[0] = tr;
+    st->rho = s[0];
+    st->rr = s[1];
+    st->rho_old = st->alpha = st->omega = 1.0;
+    st->first = 1;
+    st->upd = 0;
+    st->noupd = 1;
+    st->pending = kRunning;
+    if (st->maxiter <= 0) {
+      st->status = MLSH_SOLVER_MAXITER;
+      st->done = 1;
+    } else if (tr < st->tol && st->miniter <= 0) {
+      st->status = MLSH_SUCCESS;
+      st->done = 1;
+    } else if (isnan(tr)) {
+      st->status = MLSH_SOLVER_RESIDUAL_NAN;
+      st->done = 1;
+    }
+    cond.set(st->done ? 0 : 1);
+  }
+};
+
+// Update, part 1: x += s * x32 (FP64), x32 = 0.
+struct MixXUpdBody : NoPrep {
+  double *x64;
+  float *x32;
+  SolverState *st;
+  double s;
+  __device__ void prepare() { s = st->scale; }
+  __device__ void operator()(int64_t i, double *) const {
+    x64[i] = s * (double)x32[i] + x64[i];
+    x32[i] = 0.0f;
+  }
+};
+
+// Update, part 3 (after r64 = b - A x in FP64): r32 = r64 / s; a fresh
+// Krylov space also restarts the shadow residual r0 = r32.
+struct MixRUpdBody {
+  const double *r64;
+  float *r32;
+  float *r0;
+  SolverState *st;
+  CondRef cond;
+  double inv;
+  int fresh;
+  __device__ void prepare() {
+    inv = 1.0 / st->scale;
+    fresh = st->first;
+  }
+  __device__ void operator()(int64_t i, double *acc) const {
+    const float r = (float)(r64[i] * inv);
+    r32[i] = r;
+    float z;
+    if (fresh) {
+      r0[i] = r;
+      z = r;
+    } else {
+      z = r0[i];
+    }
+    acc[0] += (double)r * (double)z;
+    acc[1] += (double)r * (double)r;
+  }
+  __device__ void finish(const double *s) {
+    const double tr = sqrt(st->rr64);
+    const long long o = st->outer + 1;
+    st->outer = o;
+    if (st->hist != nullptr && o < st->hist_cap) st->hist[o] = tr;
+    st->resid = tr;
+    st->rel_true = tr;
+    st->upd = 0;
+    st->noupd = 1;
+    if (tr < st->tol && st->miniter <= st->iter) {
+      st->status = MLSH_SUCCESS;
+      st->done = 1;
+    } else if (isnan(tr)) {
+      st->status = MLSH_SOLVER_RESIDUAL_NAN;
+      st->done = 1;
+    } else if (st->pending != kRunning) {
+      st->status = st->pending;
+      st->done = 1;
+    } else {
+      st->rho = s[0];
+      st->rr = s[1];
+      if (s[0] == 0.0) {  // r orthogonal to r0: nothing to continue from
+        st->status = MLSH_SOLVER_BREAKDOWN;
+        st->done = 1;
+      }
+    }
+    cond.set(st->done ? 0 : 1);
+  }
+};
+
+template <bool JAC>
+struct MixPBody {  // p = r + beta (p - omega v) (or p = r on a fresh start); phat = M p
+  const float *r;
+  float *p;
+  const float *v;
+  float *phat;
+  const float *d;
+  SolverState *st;
+  float beta, omega;
+  int first;
+  __device__ void prepare() {
+    first = st->first;
+    omega = (float)st->omega;
+    beta = (float)((st->rho / st->rho_old) * (st->alpha / st->omega));
+  }
+  __device__ void operator()(int64_t i, double *) const {
+    float pi;
+    if (first) {
+      pi = r[i];
+    } else {
+      const float t = -omega * v[i] + p[i];
+      pi = r[i] + beta * t;
+    }
+    p[i] = pi;
+    if (JAC) phat[i] = d[i] * pi;
+  }
+  __device__ void finish(const double *) { st->first = 0; }
+};
+
+struct MixXRBody : NoPrep {  // x32 += a phat + w shat; r = s - w t; decide on an update
+  float *x;
+  float *r;
+  const float *r0;
+  const float *phat;
+  const float *shat;
+  const float *s;
+  const float *t;
+  SolverState *st;
+  float alpha, omega;
+  int brk;
+  __device__ void prepare() {
+    omega = (float)(st->ts / st->tt);
+    alpha = (float)st->alpha;
+    brk = (omega == 0.0f);
+  }
+  __device__ void operator()(int64_t i, double *acc) const {
+    if (brk) return;
+    float xi = alpha * phat[i] + x[i];
+    xi = omega * shat[i] + xi;
+    x[i] = xi;
+    const float ri = -omega * t[i] + s[i];
+    r[i] = ri;
+    acc[0] += (double)ri * (double)r0[i];
+    acc[1] += (double)ri * (double)ri;
+  }
+  __device__ void finish(const double *sums) {
+    const long long it = st->iter + 1;
+    st->iter = it;
+    int upd = 0;
+    if (brk) {
+      // omega = 0: apply the correction so far and restart the Krylov space
+      st->first = 1;
+      upd = 1;
+    } else {
+      st->omega = (double)omega;
+      st->rho_old = st->rho;
+      st->rho = sums[0];
+      st->rr = sums[1];
+      const double res = (double)sqrtf((float)sums[1]) * st->scale;
+      if (isnan(res)) {
+        st->pending = MLSH_SOLVER_RESIDUAL_NAN;
+        upd = 1;
+      } else if (res < st->delta * st->rel_true || res < st->tol) {
+        upd = 1;
+      } else if (sums[0] == 0.0) {
+        st->first = 1;
+        upd = 1;
+      }
+    }
+    if (!upd && it >= st->maxiter) upd = 1;
+    if (it >= st->maxiter && st->pending == kRunning) st->pending = MLSH_SOLVER_MAXITER;
+    st->upd = upd;
+    st->noupd = 1 - upd;
+  }
+};
+
 // --------------------------------------------------------------- driver --
 namespace {
 
@@ -289,7 +502,7 @@ cudaError_t run_body(const Handle &h, int64_t n, const Body &b, const int *done,
   return cudaGetLastError();
 }
 
-enum Kind { kCG = 0, kBiCGSTAB = 1 };
+enum Kind { kCG = 0, kBiCGSTAB = 1, kMixedBiCGSTAB = 3 };
 
 struct SolveCtx {
   Kind kind;
@@ -303,6 +516,9 @@ struct SolveCtx {
   void *ws;       // work vectors, `stride` elements apart
   int64_t n;
   int64_t stride;
+  // mixed kinds: `plan` is the FP32 copy, `b`/`x` are FP64, and
+  const CsrPlan *plan64 = nullptr;  // the FP64 matrix
+  double *r64 = nullptr;            // FP64 residual vector
 };
 
 template <typename T>
@@ -383,10 +599,74 @@ cudaError_t bi_iter(const SolveCtx &c, cudaStream_t s, CondRef cond) {
   return run_body<2, true>(*c.h, c.n, xb, done, s);
 }
 
+// ---- mixed BiCGSTAB: ws (FP32) = r, r0, p, v, s, t, phat, shat, x32
+template <bool JAC>
+cudaError_t mixbi_init(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  SolverState *st = c.h->state;
+  cudaError_t e = launch_spmv_t<double, kDotSelf, kDotNone>(
+      *c.plan64, *c.h, -1.0, static_cast<const double *>(c.x), 1.0,
+      static_cast<const double *>(c.b), c.r64, nullptr, nullptr, &st->rr64, nullptr, s);
+  if (e != cudaSuccess) return e;
+  MixInitBody ib;
+  ib.r64 = c.r64; ib.r32 = wsv<float>(c, 0); ib.r0 = wsv<float>(c, 1);
+  ib.x32 = wsv<float>(c, 8); ib.st = st; ib.cond = cond;
+  return run_body<2, true>(*c.h, c.n, ib, nullptr, s);
+}
+
+template <bool JAC>
+cudaError_t mixbi_iter(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  float *r = wsv<float>(c, 0), *r0 = wsv<float>(c, 1), *p = wsv<float>(c, 2);
+  float *v = wsv<float>(c, 3), *sv = wsv<float>(c, 4), *t = wsv<float>(c, 5);
+  float *phat = JAC ? wsv<float>(c, 6) : p;
+  float *shat = JAC ? wsv<float>(c, 7) : sv;
+  float *x32 = wsv<float>(c, 8);
+  const float *d = static_cast<const float *>(c.d);
+  SolverState *st = c.h->state;
+  const int *done = &st->done;
+  const int *noupd = &st->noupd;
+  // reliable update, when the previous pass asked for one
+  MixXUpdBody ub;
+  ub.x64 = static_cast<double *>(c.x); ub.x32 = x32; ub.st = st;
+  cudaError_t e = run_body<0, false>(*c.h, c.n, ub, noupd, s);
+  if (e != cudaSuccess) return e;
+  e = launch_spmv_t<double, kDotSelf, kDotNone>(
+      *c.plan64, *c.h, -1.0, static_cast<const double *>(c.x), 1.0,
+      static_cast<const double *>(c.b), c.r64, nullptr, nullptr, &st->rr64, noupd, s);
+  if (e != cudaSuccess) return e;
+  MixRUpdBody rb;
+  rb.r64 = c.r64; rb.r32 = r; rb.r0 = r0; rb.st = st; rb.cond = cond;
+  e = run_body<2, true>(*c.h, c.n, rb, noupd, s);
+  if (e != cudaSuccess) return e;
+  // one FP32 BiCGSTAB iteration
+  MixPBody<JAC> pb;
+  pb.r = r; pb.p = p; pb.v = v; pb.phat = phat; pb.d = d; pb.st = st;
+  e = run_body<0, true>(*c.h, c.n, pb, done, s);
+  if (e != cudaSuccess) return e;
+  e = launch_spmv_t<float, kDotW, kDotNone>(*c.plan, *c.h, 1.0, phat, 0.0, nullptr, v, r0,
+                                            nullptr, &st->vr0, done, s);
+  if (e != cudaSuccess) return e;
+  BiSBody<float, JAC> sb;
+  sb.r = r; sb.v = v; sb.s = sv; sb.shat = shat; sb.d = d; sb.st = st;
+  e = run_body<0, true>(*c.h, c.n, sb, done, s);
+  if (e != cudaSuccess) return e;
+  e = launch_spmv_t<float, kDotW, kDotSelf>(*c.plan, *c.h, 1.0, shat, 0.0, nullptr, t, sv,
+                                            nullptr, &st->ts, done, s);
+  if (e != cudaSuccess) return e;
+  MixXRBody xb;
+  xb.x = x32; xb.r = r; xb.r0 = r0; xb.phat = phat; xb.shat = shat; xb.s = sv; xb.t = t;
+  xb.st = st;
+  return run_body<2, true>(*c.h, c.n, xb, done, s);
+}
+
 using StepFn = cudaError_t (*)(const SolveCtx &, cudaStream_t, CondRef);
 
 void pick_steps(const SolveCtx &c, StepFn *init, StepFn *iter) {
   const bool f64 = c.dtype == MLSH_F64;
+  if (c.kind == kMixedBiCGSTAB) {
+    *init = c.jac ? mixbi_init<true> : mixbi_init<false>;
+    *iter = c.jac ? mixbi_iter<true> : mixbi_iter<false>;
+    return;
+  }
   if (c.kind == kCG) {
     if (f64) {
       *init = c.jac ? cg_init<double, true> : cg_init<double, false>;
@@ -772,6 +1052,106 @@ int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, voi
 
 }  // namespace
 
+// Mixed-precision BiCGSTAB with reliable updates on the kernel engine (see
+// MixInitBody): p is the FP64 matrix, p32 its FP32 copy, r64 an n-vector.
+int mixed_bicgstab_kernels(Handle &h, CsrPlan &p, CsrPlan &p32, double *r64, const void *b,
+                           void *x, const mlsh_solver_opts *opts, double inner_tol,
+                           mlsh_solver_result *res) {
+  const int64_t n = p.n_rows;
+  SolveCtx c;
+  c.kind = kMixedBiCGSTAB;
+  c.dtype = MLSH_F32;
+  c.jac = opts->precond == MLSH_PRECOND_JACOBI;
+  c.plan = &p32;
+  c.plan64 = &p;
+  c.r64 = r64;
+  c.h = &h;
+  c.b = b;
+  c.x = x;
+  c.d = nullptr;
+  c.n = n;
+  if (c.jac) {
+    const int st = plan_inv_diag(p32, h.stream, &c.d);
+    if (st != MLSH_SUCCESS) return st;
+  }
+  const int64_t n_al = (int64_t)(((size_t)n * 4 + 255) / 256 * 256 / 4);
+  int st = ensure_ws(h, (size_t)9 * (size_t)n_al * 4);
+  if (st != MLSH_SUCCESS) return st;
+  c.ws = h.ws;
+  c.stride = n_al;
+
+  SolverState *hst = h.host_state;
+  std::memset(hst, 0, sizeof(SolverState));
+  hst->tol = opts->tol;
+  hst->maxiter = opts->maxiter;
+  hst->miniter = opts->miniter;
+  hst->delta = inner_tol;
+  hst->status = kRunning;
+  hst->done = 0;
+  const bool want_hist = opts->history != nullptr && opts->history_len > 0;
+  if (want_hist) {
+    if (h.hist_cap < opts->history_len) {
+      pool_free(h.hist, h.stream);
+      h.hist = nullptr;
+      h.hist_cap = 0;
+      if (pool_alloc(&h.hist, sizeof(double) * (size_t)opts->history_len, h.stream) !=
+          cudaSuccess) {
+        cudaGetLastError();
+        return MLSH_ERR_OOM;
+      }
+      h.hist_cap = opts->history_len;
+    }
+    hst->hist = h.hist;
+    hst->hist_cap = opts->history_len;
+  }
+  MLSH_CUDA_TRY(cudaMemcpyAsync(h.state, hst, sizeof(SolverState), cudaMemcpyHostToDevice,
+                                h.stream));
+  MLSH_CUDA_TRY(cudaMemsetAsync(h.err_flag, 0, sizeof(int), h.stream));
+  bool graph_ok = false;
+  if (opts->use_graph) {
+    cudaGraphExec_t ex = nullptr;
+    if (get_graph(c, h, &ex) == MLSH_SUCCESS) {
+      MLSH_CUDA_TRY(cudaGraphLaunch(ex, h.stream));
+      graph_ok = true;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  if (!graph_ok) {
+    StepFn init, iter;
+    pick_steps(c, &init, &iter);
+    CondRef none{0, 0};
+    MLSH_CUDA_TRY(init(c, h.stream, none));
+    const int every = opts->check_every > 0 ? opts->check_every : 16;
+    while (true) {
+      MLSH_CUDA_TRY(cudaMemcpyAsync(hst, h.state, sizeof(SolverState), cudaMemcpyDeviceToHost,
+                                    h.stream));
+      MLSH_CUDA_TRY(cudaStreamSynchronize(h.stream));
+      if (hst->done) break;
+      for (int k = 0; k < every; ++k) MLSH_CUDA_TRY(iter(c, h.stream, none));
+    }
+  }
+  MLSH_CUDA_TRY(cudaMemcpyAsync(hst, h.state, sizeof(SolverState), cudaMemcpyDeviceToHost,
+                                h.stream));
+  MLSH_CUDA_TRY(cudaMemcpyAsync(&h.host_scalars[7], h.err_flag, sizeof(int),
+                                cudaMemcpyDeviceToHost, h.stream));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  int err = 0;
+  std::memcpy(&err, &h.host_scalars[7], sizeof(int));
+  if (err != 0) return err;
+  res->status = hst->status;
+  res->iters = hst->iter;
+  res->final_resid = hst->resid;
+  res->outer_iters = (int)hst->outer;
+  if (want_hist) {
+    const int64_t k = std::min<int64_t>(hst->outer + 1, opts->history_len);
+    if (k > 0)
+      MLSH_CUDA_TRY(cudaMemcpy(opts->history, h.hist, sizeof(double) * (size_t)k,
+                               cudaMemcpyDeviceToHost));
+  }
+  return res->status;
+}
+
 void release_solver_graphs(Handle &h) {
   if (h.graph_cache) {
     GraphCache &gc = cache_of(h);
@@ -796,6 +1176,7 @@ void release_plan_extras(CsrPlan &p) {
 }
 
 void invalidate_plan_extras(CsrPlan &p) {
+  if (p.handle) purge_graphs(*p.handle, &p, nullptr);
   mixed_invalidate(p);
   transpose_invalidate(p);
 }

@@ -25,6 +25,7 @@
 #include <new>
 #include <vector>
 
+#include "mlsh_cluster.cuh"
 #include "mlsh_core.cuh"
 
 namespace mlsh {
@@ -233,6 +234,18 @@ int mixed_solve(int kind, mlsh_handle hs, mlsh_csr_plan ps, const void *d_b, voi
   MixedExtras *m = nullptr;
   int st = ensure_extras(hs, p, &m);
   if (st != MLSH_SUCCESS) return st;
+  // Large systems (the FP32 iteration on the kernel engine): BiCGSTAB with
+  // reliable updates in one graph.  Systems that fit a thread-block cluster
+  // keep the restarted refinement below, whose inner solves run on it.
+  const bool inner_on_cluster =
+      opts->engine == MLSH_ENGINE_CLUSTER ||
+      (opts->engine == MLSH_ENGINE_AUTO && opts->maxiter <= kClusterMaxIterAuto &&
+       cluster_rows_for(kind, MLSH_F32, n, opts->cluster_rows) != 0);
+  if (kind == 1 && !inner_on_cluster) {
+    if (opts->precond != MLSH_PRECOND_NONE && opts->precond != MLSH_PRECOND_JACOBI)
+      return MLSH_ERR_INVALID_ARG;
+    return mixed_bicgstab_kernels(h, p, m->plan32->p, m->r64, d_b, d_x, opts, inner_tol, res);
+  }
 
   mlsh_solver_opts in = *opts;
   in.tol = inner_tol;

@@ -110,6 +110,17 @@ constexpr int kFlagLast = 3;
 constexpr int kFlagWarpSeg = 4;  // 8 per-warp segment counts (4..11)
 
 template <typename T>
+__device__ __forceinline__ T spmv_mul_rn(T a, T b) {
+  if constexpr (sizeof(T) == 8) return __dmul_rn(a, b);
+  else return __fmul_rn(a, b);
+}
+template <typename T>
+__device__ __forceinline__ T spmv_add_rn(T a, T b) {
+  if constexpr (sizeof(T) == 8) return __dadd_rn(a, b);
+  else return __fadd_rn(a, b);
+}
+
+template <typename T>
 __device__ __forceinline__ int head_elems(const T *base, int idx) {
   return (int)(((uintptr_t)(base + idx) & 15u) / sizeof(T));
 }
@@ -183,7 +194,7 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(full0 + 8 * s, 1);
-      mbar_init(empty0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, kConsumers / 32);  // one arrival per consumer warp
     }
     for (int f = 0; f < 16; ++f) flags[f] = 0;
     fence_mbar_init();
@@ -198,6 +209,7 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
     bool aborted = false;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++k) {
       const int s = k % STAGES;
+      const Tile tl = a.tiles[t];  // issued before the wait for a free stage
       if (k >= STAGES) {
         int ok = 1;
         if (lane == 0) {
@@ -216,7 +228,6 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (!ok) { aborted = true; break; }
       }
-      const Tile tl = a.tiles[t];
       unsigned char *st = smem + s * L::kStageBytes;
       VT *sv = reinterpret_cast<VT *>(st);
       const uint32_t bar = full0 + 8 * s;
@@ -290,20 +301,40 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
   const double alpha = a.alpha, beta = a.beta;
   constexpr int kPer = kTileNnz / kConsumers;  // 7 products per thread
 
+  // Per-tile values each thread needs besides the staged val/col: the tile
+  // record, its row bounds, the 16-bit column base and the fused dot's
+  // w0 entry.  They are fetched one tile ahead (the record two steps
+  // ahead), so their latency hides behind the current tile's gathers.
+  Tile tl_c = {0, 0, 0, 0};
+  int g0c = 0, g1c = 0, cbc = 0;
+  XT w0c = XT(0);
+  {
+    const int t0 = blockIdx.x;
+    if (t0 < a.n_tiles) {
+      tl_c = a.tiles[t0];
+      const int nr = tl_c.row_end >= 0 ? tl_c.row_end - tl_c.row_begin : 0;
+      if (ct < nr) {
+        g0c = __ldg(a.row_ptr + tl_c.row_begin + ct);
+        g1c = __ldg(a.row_ptr + tl_c.row_begin + ct + 1);
+        if constexpr (M0 == kDotW) w0c = a.w0[tl_c.row_begin + ct];
+      }
+      if constexpr (C16) cbc = __ldg(a.tile_base + t0);
+    }
+  }
+
   int k = 0;
   for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++k) {
     const int s = k % STAGES;
-    const Tile tl = a.tiles[t];
+    const Tile tl = tl_c;
     const bool normal = tl.row_end >= 0;
     const int rb = tl.row_begin;
     const int nrows = normal ? tl.row_end - tl.row_begin : 0;
-    // row bounds of this thread's row, issued before the stage wait
-    int g0 = 0, g1 = 0;
-    if (ct < nrows) {
-      g0 = __ldg(a.row_ptr + rb + ct);
-      g1 = __ldg(a.row_ptr + rb + ct + 1);
-    }
-    const int col_base = C16 ? __ldg(a.tile_base + t) : 0;
+    const int g0 = g0c, g1 = g1c;
+    const int col_base = cbc;
+    const XT w0v = w0c;
+    const int tn = t + (int)gridDim.x;
+    Tile tl_n = {0, -1, 0, 0};
+    if (tn < a.n_tiles) tl_n = a.tiles[tn];
     if (ct == 0) {
       if (!mbar_wait_bounded(full0 + 8 * s, (uint32_t)((k / STAGES) & 1), kWaitLimitNs)) {
         flags[kFlagConsAbort] = 1;
@@ -316,6 +347,63 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
     const int nb = tl.nnz_begin, ne = tl.nnz_end, nt = ne - nb;
     unsigned char *st = smem + s * L::kStageBytes;
     VT *v = reinterpret_cast<VT *>(st) + head_elems(a.val, nb);
+
+    if (normal && tl.short_only) {
+      // ---------------------------------------------- direct: short rows
+      // Every row has <= kShortRow entries: each thread gathers and sums
+      // its own row in row order with separately rounded products (the
+      // reference's loop, as passes A+B compute it), with no exchange
+      // through shared memory and no barrier before the stage is released.
+      VT sum = VT(0);
+      if (ct < nrows) {
+        const int s0 = g0 - nb, len = g1 - g0;
+        XT xx[kShortRow];
+        if constexpr (C16) {
+          const uint16_t *c = reinterpret_cast<const uint16_t *>(st + L::kValBytes) +
+                              head_elems(a.col16, nb);
+#pragma unroll
+          for (int u = 0; u < kShortRow; ++u)
+            if (u < len) xx[u] = __ldg(a.x + col_base + (int)c[s0 + u]);
+        } else {
+          const int *c = reinterpret_cast<const int *>(st + L::kValBytes) + head_elems(a.col, nb);
+#pragma unroll
+          for (int u = 0; u < kShortRow; ++u)
+            if (u < len) xx[u] = __ldg(a.x + c[s0 + u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kShortRow; ++u)
+          if (u < len) sum = spmv_add_rn(sum, spmv_mul_rn(v[s0 + u], (VT)xx[u]));
+      }
+      // this warp is done with the stage
+      __syncwarp();
+      if (lane == 0) mbar_arrive(empty0 + 8 * s);
+      if (ct == 0) flags[kFlagConsumed] = k + 1;
+      if (ct < nrows) {
+        const int r = rb + ct;
+        const double dsum = (double)sum;
+        const XT out = (beta == 0.0) ? (XT)(alpha * dsum)
+                                     : (XT)(alpha * dsum + beta * (double)a.y_in[r]);
+        a.y_out[r] = out;
+        if constexpr (M0 == kDotW) acc[0] += (double)w0v * (double)out;
+        if constexpr (M0 == kDotSelf) acc[0] += (double)out * (double)out;
+        if constexpr (M1 == kDotW) acc[1] += (double)a.w1[r] * (double)out;
+        if constexpr (M1 == kDotSelf) acc[1] += (double)out * (double)out;
+      }
+      // prefetch the next tile's per-thread values
+      g0c = g1c = cbc = 0;
+      w0c = XT(0);
+      if (tn < a.n_tiles) {
+        const int nr = tl_n.row_end >= 0 ? tl_n.row_end - tl_n.row_begin : 0;
+        if (ct < nr) {
+          g0c = __ldg(a.row_ptr + tl_n.row_begin + ct);
+          g1c = __ldg(a.row_ptr + tl_n.row_begin + ct + 1);
+          if constexpr (M0 == kDotW) w0c = a.w0[tl_n.row_begin + ct];
+        }
+        if constexpr (C16) cbc = __ldg(a.tile_base + tn);
+      }
+      tl_c = tl_n;
+      continue;
+    }
 
     // pass A: products in place
     {
@@ -349,6 +437,19 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
       }
     }
     named_sync(1, kConsumers);
+    // prefetch the next tile's per-thread values
+    g0c = g1c = cbc = 0;
+    w0c = XT(0);
+    if (tn < a.n_tiles) {
+      const int nr = tl_n.row_end >= 0 ? tl_n.row_end - tl_n.row_begin : 0;
+      if (ct < nr) {
+        g0c = __ldg(a.row_ptr + tl_n.row_begin + ct);
+        g1c = __ldg(a.row_ptr + tl_n.row_begin + ct + 1);
+        if constexpr (M0 == kDotW) w0c = a.w0[tl_n.row_begin + ct];
+      }
+      if constexpr (C16) cbc = __ldg(a.tile_base + tn);
+    }
+    tl_c = tl_n;
 
     if (normal) {
       // ------------------------------------------------ pass B: short rows
@@ -407,10 +508,8 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
         }
       }
       // all reads of the stage are done (the last barrier above)
-      if (ct == 0) {
-        mbar_arrive(empty0 + 8 * s);
-        flags[kFlagConsumed] = k + 1;
-      }
+      if (lane == 0) mbar_arrive(empty0 + 8 * s);
+      if (ct == 0) flags[kFlagConsumed] = k + 1;
       // ----------------------------------------------------- pass D: y
       if (ct < nrows) {
         const int r = rb + ct;
@@ -418,7 +517,7 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
         const XT out = (beta == 0.0) ? (XT)(alpha * sum)
                                      : (XT)(alpha * sum + beta * (double)a.y_in[r]);
         a.y_out[r] = out;
-        if constexpr (M0 == kDotW) acc[0] += (double)a.w0[r] * (double)out;
+        if constexpr (M0 == kDotW) acc[0] += (double)w0v * (double)out;
         if constexpr (M0 == kDotSelf) acc[0] += (double)out * (double)out;
         if constexpr (M1 == kDotW) acc[1] += (double)a.w1[r] * (double)out;
         if constexpr (M1 == kDotSelf) acc[1] += (double)out * (double)out;
@@ -430,8 +529,8 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
       part = warp_sum(part);
       if (lane == 0) red[warp] = (double)part;
       named_sync(1, kConsumers);
+      if (lane == 0) mbar_arrive(empty0 + 8 * s);
       if (ct == 0) {
-        mbar_arrive(empty0 + 8 * s);
         flags[kFlagConsumed] = k + 1;
         double tot = 0.0;
         for (int w = 0; w < kConsumers / 32; ++w) tot += red[w];

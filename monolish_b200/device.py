@@ -250,8 +250,9 @@ def _solve(fn, A: Crs, b, x, tol, maxiter, miniter=0, precond=_abi.PRECOND_JACOB
 
 
 def _solve_mixed(fn, A: Crs, b, x, tol, maxiter, inner_tol=1e-4, miniter=0,
-                 precond=_abi.PRECOND_JACOBI, engine=_abi.ENGINE_AUTO, history=None):
-    o = _opts(tol, maxiter, miniter, precond, True, 0, engine, 0)
+                 precond=_abi.PRECOND_JACOBI, engine=_abi.ENGINE_AUTO, history=None,
+                 use_graph=True):
+    o = _opts(tol, maxiter, miniter, precond, use_graph, 0, engine, 0)
     if history is not None:
         o.history = history.ctypes.data_as(C.POINTER(C.c_double))
         o.history_len = len(history)

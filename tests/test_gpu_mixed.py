@@ -14,7 +14,7 @@ from monolish_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 
-def solve_both(handle, restatement, kind, n, rp, ci, v, seed):
+def solve_both(handle, restatement, kind, n, rp, ci, v, seed, engine=_abi.ENGINE_AUTO):
     import torch
     from monolish_b200 import device as D
     xt = W.uniform_mt(n, -1, 1, seed)
@@ -26,7 +26,7 @@ def solve_both(handle, restatement, kind, n, rp, ci, v, seed):
     mixed = D.cg_solve_mixed if kind == "cg" else D.bicgstab_solve_mixed
     plain = D.cg_solve if kind == "cg" else D.bicgstab_solve
     hist = np.full(100, np.nan)
-    rm = mixed(A, db, dx, tol, 20000, inner_tol=1e-4, history=hist)
+    rm = mixed(A, db, dx, tol, 20000, inner_tol=1e-4, history=hist, engine=engine)
     xm = dx.cpu().numpy()
     dx.zero_()
     rpl = plain(A, db, dx, tol, 20000)
@@ -35,12 +35,17 @@ def solve_both(handle, restatement, kind, n, rp, ci, v, seed):
     return rm, xm, rpl, st, it, xo, b, hist
 
 
+@pytest.mark.parametrize("engine", [_abi.ENGINE_AUTO, _abi.ENGINE_KERNELS],
+                         ids=["auto", "kernels"])
 @pytest.mark.parametrize("case", ["convdiff40", "convdiff64_pe2"])
-def test_mixed_bicgstab_convdiff(handle, restatement, case):
+def test_mixed_bicgstab_convdiff(handle, restatement, case, engine):
+    """AUTO runs these sizes' FP32 iterations on the cluster engine
+    (restarted refinement); KERNELS on the kernel engine (reliable
+    updates, the path large systems take)."""
     m, pe = (40, 10.0) if case == "convdiff40" else (64, 2.0)
     n, rp, ci, v = W.convdiff3d(m, peclet=pe)
     rm, xm, rpl, st, it, xo, b, hist = solve_both(handle, restatement, "bicgstab", n, rp, ci,
-                                                  v, 2)
+                                                  v, 2, engine)
     assert rm.status == 0 and st == 0 and rpl.status == 0
     assert rm.outer >= 2
     assert restatement.true_relres(rp, ci, v, b, xm) < 1e-10
@@ -91,3 +96,49 @@ def test_mixed_rejects_fp32_plan(handle):
     with pytest.raises(_abi.MlshError):
         D.cg_solve_mixed(A, d, d, 1e-8, 10)
     A.close()
+
+
+def test_mixed_bicgstab_reliable_updates_eager_equals_graph(handle, restatement):
+    """The reliable-update engine gives the same result launched as one graph
+    or iteration by iteration, and takes about as many FP32 iterations as the
+    plain FP64 solve takes FP64 ones."""
+    import torch
+    from monolish_b200 import device as D
+    n, rp, ci, v = W.convdiff3d(48, peclet=5.0)
+    xt = W.uniform_mt(n, -1, 1, 4)
+    b = restatement.spmv(rp, ci, v, xt)
+    tol = 1e-10 * np.linalg.norm(b)
+    A = D.Crs(handle, n, n, rp, ci, v)
+    db = torch.from_numpy(b).cuda()
+    xs, rs = [], []
+    for use_graph in (True, False):
+        dx = torch.zeros(n, dtype=torch.float64, device="cuda")
+        r = D.bicgstab_solve_mixed(A, db, dx, tol, 20000, inner_tol=1e-4,
+                                   engine=_abi.ENGINE_KERNELS, use_graph=use_graph)
+        xs.append(dx.cpu().numpy())
+        rs.append(r)
+    A.close()
+    assert rs[0].status == 0 and (rs[0].iters, rs[0].outer) == (rs[1].iters, rs[1].outer)
+    assert np.array_equal(xs[0], xs[1])
+    st, it, _, _ = restatement.bicgstab(rp, ci, v, b, np.zeros(n), tol, 20000)
+    assert rs[0].iters <= 1.25 * it + 10
+    assert restatement.true_relres(rp, ci, v, b, xs[0]) < 1e-10
+
+
+def test_mixed_bicgstab_reliable_updates_maxiter(handle, restatement):
+    """Stopped by maxiter: the correction so far is applied and the status is
+    MAXITER with the true residual."""
+    import torch
+    from monolish_b200 import device as D
+    n, rp, ci, v = W.convdiff3d(40, peclet=10.0)
+    xt = W.uniform_mt(n, -1, 1, 5)
+    b = restatement.spmv(rp, ci, v, xt)
+    A = D.Crs(handle, n, n, rp, ci, v)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.zeros(n, dtype=torch.float64, device="cuda")
+    r = D.bicgstab_solve_mixed(A, db, dx, 1e-10 * np.linalg.norm(b), 7, inner_tol=1e-4,
+                               engine=_abi.ENGINE_KERNELS)
+    A.close()
+    assert r.status == _abi.SOLVER_MAXITER and r.iters == 7
+    rel = restatement.true_relres(rp, ci, v, b, dx.cpu().numpy())
+    assert rel < 1.0 and abs(r.resid / np.linalg.norm(b) - rel) <= 1e-6 * rel
