@@ -50,9 +50,11 @@ void transpose_release(CsrPlan &p);
 void transpose_invalidate(CsrPlan &p);
 
 // Mixed-precision BiCGSTAB with reliable updates on the kernel engine
-// (mlsh_krylov.cu): p FP64, p32 its FP32 copy, r64 an FP64 work vector.
-int mixed_bicgstab_kernels(Handle &h, CsrPlan &p, CsrPlan &p32, double *r64, const void *b,
-                           void *x, const mlsh_solver_opts *opts, double inner_tol,
+// (mlsh_krylov.cu): p FP64, p32 its FP32 copy (holding A D^-1 when dinv64,
+// the FP64 inverse diagonal, is given for Jacobi), r64 an FP64 work vector.
+int mixed_bicgstab_kernels(Handle &h, CsrPlan &p, CsrPlan &p32, double *r64,
+                           const double *dinv64, const void *b, void *x,
+                           const mlsh_solver_opts *opts, double inner_tol,
                            mlsh_solver_result *res);
 
 // Solver-side resources kept on the handle / plan (mlsh_krylov.cu).

@@ -103,15 +103,25 @@ struct CgXRBody : NoPrep {  // x += a p; r -= a q; sums (z,r), (r,r)
   const T *d;
   SolverState *st;
   T alpha;
+  using elem = T;
+  bool aligned() const { return al16(x) && al16(r) && al16(p) && al16(q) && (!JAC || al16(d)); }
   __device__ void prepare() { alpha = (T)(st->rz / st->pq); }
-  __device__ void operator()(int64_t i, double *acc) const {
-    const T pi = p[i], qi = q[i];
-    x[i] = alpha * pi + x[i];
-    const T ri = -alpha * qi + r[i];
-    r[i] = ri;
-    const T zi = JAC ? d[i] * ri : ri;
-    acc[0] += (double)zi * (double)ri;
-    acc[1] += (double)ri * (double)ri;
+  template <int W>
+  __device__ void step(int64_t i, double *acc) const {
+    const Pack<T, W> pp = ldp<W>(p, i), qq = ldp<W>(q, i);
+    Pack<T, W> xx = ldp<W>(x, i), rr = ldp<W>(r, i), dd;
+    if (JAC) dd = ldp<W>(d, i);
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      xx.v[k] = alpha * pp.v[k] + xx.v[k];
+      const T ri = -alpha * qq.v[k] + rr.v[k];
+      rr.v[k] = ri;
+      const T zi = JAC ? dd.v[k] * ri : ri;
+      acc[0] += (double)zi * (double)ri;
+      acc[1] += (double)ri * (double)ri;
+    }
+    stp<W>(x, i, xx);
+    stp<W>(r, i, rr);
   }
   __device__ void finish(const double *s) {
     st->rz_new = s[0];
@@ -127,11 +137,20 @@ struct CgPBody : NoPrep {  // p = z + b p; stopping test
   SolverState *st;
   CondRef cond;
   T beta;
+  using elem = T;
+  bool aligned() const { return al16(p) && al16(r) && (!JAC || al16(d)); }
   __device__ void prepare() { beta = (T)(st->rz_new / st->rz); }
-  __device__ void operator()(int64_t i, double *) const {
-    const T ri = r[i];
-    const T zi = JAC ? d[i] * ri : ri;
-    p[i] = zi + beta * p[i];
+  template <int W>
+  __device__ void step(int64_t i, double *) const {
+    const Pack<T, W> rr = ldp<W>(r, i);
+    Pack<T, W> pp = ldp<W>(p, i), dd;
+    if (JAC) dd = ldp<W>(d, i);
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const T zi = JAC ? dd.v[k] * rr.v[k] : rr.v[k];
+      pp.v[k] = zi + beta * pp.v[k];
+    }
+    stp<W>(p, i, pp);
   }
   __device__ void finish(const double *) {
     st->rz = st->rz_new;
@@ -191,21 +210,35 @@ struct BiPBody : NoPrep {  // p = r + beta (p - omega v); phat = M p
   SolverState *st;
   T beta, omega;
   int first;
+  using elem = T;
+  bool aligned() const { return al16(r) && al16(p) && al16(v) && al16(phat) && (!JAC || al16(d)); }
   __device__ void prepare() {
     first = st->iter == 0;
     omega = (T)st->omega;
     beta = (T)((st->rho / st->rho_old) * (st->alpha / st->omega));
   }
-  __device__ void operator()(int64_t i, double *) const {
-    T pi;
+  template <int W>
+  __device__ void step(int64_t i, double *) const {
+    const Pack<T, W> rr = ldp<W>(r, i);
+    Pack<T, W> pp;
     if (first) {
-      pi = r[i];
+      pp = rr;
     } else {
-      const T t = -omega * v[i] + p[i];
-      pi = r[i] + beta * t;
+      const Pack<T, W> vv = ldp<W>(v, i);
+      pp = ldp<W>(p, i);
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        const T t = -omega * vv.v[k] + pp.v[k];
+        pp.v[k] = rr.v[k] + beta * t;
+      }
     }
-    p[i] = pi;
-    if (JAC) phat[i] = d[i] * pi;
+    stp<W>(p, i, pp);
+    if (JAC) {
+      Pack<T, W> dd = ldp<W>(d, i);
+#pragma unroll
+      for (int k = 0; k < W; ++k) dd.v[k] = dd.v[k] * pp.v[k];
+      stp<W>(phat, i, dd);
+    }
   }
 };
 
@@ -219,14 +252,25 @@ struct BiSBody : NoPrep {  // alpha = rho/(v,r0); s = r - alpha v; shat = M s
   SolverState *st;
   T alpha;
   double alpha_d;
+  using elem = T;
+  bool aligned() const { return al16(r) && al16(v) && al16(s) && al16(shat) && (!JAC || al16(d)); }
   __device__ void prepare() {
     alpha_d = st->rho / st->vr0;
     alpha = (T)alpha_d;
   }
-  __device__ void operator()(int64_t i, double *) const {
-    const T si = -alpha * v[i] + r[i];
-    s[i] = si;
-    if (JAC) shat[i] = d[i] * si;
+  template <int W>
+  __device__ void step(int64_t i, double *) const {
+    const Pack<T, W> vv = ldp<W>(v, i), rr = ldp<W>(r, i);
+    Pack<T, W> ss;
+#pragma unroll
+    for (int k = 0; k < W; ++k) ss.v[k] = -alpha * vv.v[k] + rr.v[k];
+    stp<W>(s, i, ss);
+    if (JAC) {
+      Pack<T, W> dd = ldp<W>(d, i);
+#pragma unroll
+      for (int k = 0; k < W; ++k) dd.v[k] = dd.v[k] * ss.v[k];
+      stp<W>(shat, i, dd);
+    }
   }
   __device__ void finish(const double *) { st->alpha = (double)alpha; }
 };
@@ -244,20 +288,32 @@ struct BiXRBody : NoPrep {  // omega = (t,s)/(t,t); x += a phat + w shat; r = s 
   CondRef cond;
   T alpha, omega;
   int brk;
+  using elem = T;
+  bool aligned() const {
+    return al16(x) && al16(r) && al16(r0) && al16(phat) && al16(shat) && al16(s) && al16(t);
+  }
   __device__ void prepare() {
     omega = (T)(st->ts / st->tt);
     alpha = (T)st->alpha;
     brk = (omega == T(0));
   }
-  __device__ void operator()(int64_t i, double *acc) const {
+  template <int W>
+  __device__ void step(int64_t i, double *acc) const {
     if (brk) return;
-    T xi = alpha * phat[i] + x[i];
-    xi = omega * shat[i] + xi;
-    x[i] = xi;
-    const T ri = -omega * t[i] + s[i];
-    r[i] = ri;
-    acc[0] += (double)ri * (double)r0[i];
-    acc[1] += (double)ri * (double)ri;
+    const Pack<T, W> ph = ldp<W>(phat, i), sh = ldp<W>(shat, i), tt = ldp<W>(t, i),
+                     ss = ldp<W>(s, i), rz = ldp<W>(r0, i);
+    Pack<T, W> xx = ldp<W>(x, i), rr;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      T xi = alpha * ph.v[k] + xx.v[k];
+      xx.v[k] = omega * sh.v[k] + xi;
+      const T ri = -omega * tt.v[k] + ss.v[k];
+      rr.v[k] = ri;
+      acc[0] += (double)ri * (double)rz.v[k];
+      acc[1] += (double)ri * (double)ri;
+    }
+    stp<W>(x, i, xx);
+    stp<W>(r, i, rr);
   }
   __device__ void finish(const double *sums) {
     if (brk) {
@@ -335,15 +391,17 @@ struct MixInitBody {
   }
 };
 
-// Update, part 1: x += s * x32 (FP64), x32 = 0.
+// Update, part 1: x += s * D^-1 x32 (FP64; D^-1 = 1 without Jacobi), x32 = 0.
 struct MixXUpdBody : NoPrep {
   double *x64;
   float *x32;
+  const double *dinv;  // Jacobi: the FP32 iteration runs on A D^-1 (right scaling)
   SolverState *st;
   double s;
   __device__ void prepare() { s = st->scale; }
   __device__ void operator()(int64_t i, double *) const {
-    x64[i] = s * (double)x32[i] + x64[i];
+    const double c = dinv != nullptr ? s * dinv[i] : s;
+    x64[i] = c * (double)x32[i] + x64[i];
     x32[i] = 0.0f;
   }
 };
@@ -415,21 +473,35 @@ struct MixPBody {  // p = r + beta (p - omega v) (or p = r on a fresh start); ph
   SolverState *st;
   float beta, omega;
   int first;
+  using elem = float;
+  bool aligned() const { return al16(r) && al16(p) && al16(v) && al16(phat) && (!JAC || al16(d)); }
   __device__ void prepare() {
     first = st->first;
     omega = (float)st->omega;
     beta = (float)((st->rho / st->rho_old) * (st->alpha / st->omega));
   }
-  __device__ void operator()(int64_t i, double *) const {
-    float pi;
+  template <int W>
+  __device__ void step(int64_t i, double *) const {
+    const Pack<float, W> rr = ldp<W>(r, i);
+    Pack<float, W> pp;
     if (first) {
-      pi = r[i];
+      pp = rr;
     } else {
-      const float t = -omega * v[i] + p[i];
-      pi = r[i] + beta * t;
+      const Pack<float, W> vv = ldp<W>(v, i);
+      pp = ldp<W>(p, i);
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        const float t = -omega * vv.v[k] + pp.v[k];
+        pp.v[k] = rr.v[k] + beta * t;
+      }
     }
-    p[i] = pi;
-    if (JAC) phat[i] = d[i] * pi;
+    stp<W>(p, i, pp);
+    if (JAC) {
+      Pack<float, W> dd = ldp<W>(d, i);
+#pragma unroll
+      for (int k = 0; k < W; ++k) dd.v[k] = dd.v[k] * pp.v[k];
+      stp<W>(phat, i, dd);
+    }
   }
   __device__ void finish(const double *) { st->first = 0; }
 };
@@ -443,22 +515,35 @@ struct MixXRBody : NoPrep {  // x32 += a phat + w shat; r = s - w t; decide on a
   const float *s;
   const float *t;
   SolverState *st;
+  CondRef upd_cond;
   float alpha, omega;
   int brk;
+  using elem = float;
+  bool aligned() const {
+    return al16(x) && al16(r) && al16(r0) && al16(phat) && al16(shat) && al16(s) && al16(t);
+  }
   __device__ void prepare() {
     omega = (float)(st->ts / st->tt);
     alpha = (float)st->alpha;
     brk = (omega == 0.0f);
   }
-  __device__ void operator()(int64_t i, double *acc) const {
+  template <int W>
+  __device__ void step(int64_t i, double *acc) const {
     if (brk) return;
-    float xi = alpha * phat[i] + x[i];
-    xi = omega * shat[i] + xi;
-    x[i] = xi;
-    const float ri = -omega * t[i] + s[i];
-    r[i] = ri;
-    acc[0] += (double)ri * (double)r0[i];
-    acc[1] += (double)ri * (double)ri;
+    const Pack<float, W> ph = ldp<W>(phat, i), sh = ldp<W>(shat, i), tt = ldp<W>(t, i),
+                     ss = ldp<W>(s, i), rz = ldp<W>(r0, i);
+    Pack<float, W> xx = ldp<W>(x, i), rr;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      float xi = alpha * ph.v[k] + xx.v[k];
+      xx.v[k] = omega * sh.v[k] + xi;
+      const float ri = -omega * tt.v[k] + ss.v[k];
+      rr.v[k] = ri;
+      acc[0] += (double)ri * (double)rz.v[k];
+      acc[1] += (double)ri * (double)ri;
+    }
+    stp<W>(x, i, xx);
+    stp<W>(r, i, rr);
   }
   __device__ void finish(const double *sums) {
     const long long it = st->iter + 1;
@@ -488,6 +573,7 @@ struct MixXRBody : NoPrep {  // x32 += a phat + w shat; r = s - w t; decide on a
     if (it >= st->maxiter && st->pending == kRunning) st->pending = MLSH_SOLVER_MAXITER;
     st->upd = upd;
     st->noupd = 1 - upd;
+    upd_cond.set(upd);
   }
 };
 
@@ -498,7 +584,16 @@ template <int NR, bool FIN, typename Body>
 cudaError_t run_body(const Handle &h, int64_t n, const Body &b, const int *done,
                      cudaStream_t s) {
   RedArgs ra{h.partials, h.counters, done};
-  vec_kernel<NR, FIN, Body><<<vec_grid(n, h.num_sms), kVecThreads, 0, s>>>(n, b, ra);
+  const int g = vec_grid(n, h.num_sms);
+  if constexpr (has_step<Body>::value) {
+    constexpr int W = 16 / (int)sizeof(typename Body::elem);
+    if (b.aligned())
+      vec_pack_kernel<NR, FIN, W, Body><<<g, kVecThreads, 0, s>>>(n, b, ra);
+    else
+      vec_pack_kernel<NR, FIN, 1, Body><<<g, kVecThreads, 0, s>>>(n, b, ra);
+  } else {
+    vec_kernel<NR, FIN, Body><<<g, kVecThreads, 0, s>>>(n, b, ra);
+  }
   return cudaGetLastError();
 }
 
@@ -519,6 +614,7 @@ struct SolveCtx {
   // mixed kinds: `plan` is the FP32 copy, `b`/`x` are FP64, and
   const CsrPlan *plan64 = nullptr;  // the FP64 matrix
   double *r64 = nullptr;            // FP64 residual vector
+  CondRef upd_cond = {0, 0};        // graph: the IF node that runs the update
 };
 
 template <typename T>
@@ -599,8 +695,10 @@ cudaError_t bi_iter(const SolveCtx &c, cudaStream_t s, CondRef cond) {
   return run_body<2, true>(*c.h, c.n, xb, done, s);
 }
 
-// ---- mixed BiCGSTAB: ws (FP32) = r, r0, p, v, s, t, phat, shat, x32
-template <bool JAC>
+// ---- mixed BiCGSTAB: ws (FP32) = r, r0, p, v, s, t, x32.  With Jacobi the
+// FP32 matrix holds A D^-1 (right preconditioning folded into the values),
+// so the FP32 iteration itself is unpreconditioned and c.d is the FP64
+// inverse diagonal the update applies.
 cudaError_t mixbi_init(const SolveCtx &c, cudaStream_t s, CondRef cond) {
   SolverState *st = c.h->state;
   cudaError_t e = launch_spmv_t<double, kDotSelf, kDotNone>(
@@ -609,53 +707,64 @@ cudaError_t mixbi_init(const SolveCtx &c, cudaStream_t s, CondRef cond) {
   if (e != cudaSuccess) return e;
   MixInitBody ib;
   ib.r64 = c.r64; ib.r32 = wsv<float>(c, 0); ib.r0 = wsv<float>(c, 1);
-  ib.x32 = wsv<float>(c, 8); ib.st = st; ib.cond = cond;
+  ib.x32 = wsv<float>(c, 6); ib.st = st; ib.cond = cond;
   return run_body<2, true>(*c.h, c.n, ib, nullptr, s);
 }
 
-template <bool JAC>
-cudaError_t mixbi_iter(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+// One FP32 BiCGSTAB iteration; its last kernel decides whether an update
+// follows.
+cudaError_t mixbi_main(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  (void)cond;
   float *r = wsv<float>(c, 0), *r0 = wsv<float>(c, 1), *p = wsv<float>(c, 2);
   float *v = wsv<float>(c, 3), *sv = wsv<float>(c, 4), *t = wsv<float>(c, 5);
-  float *phat = JAC ? wsv<float>(c, 6) : p;
-  float *shat = JAC ? wsv<float>(c, 7) : sv;
-  float *x32 = wsv<float>(c, 8);
-  const float *d = static_cast<const float *>(c.d);
+  float *x32 = wsv<float>(c, 6);
   SolverState *st = c.h->state;
   const int *done = &st->done;
-  const int *noupd = &st->noupd;
-  // reliable update, when the previous pass asked for one
-  MixXUpdBody ub;
-  ub.x64 = static_cast<double *>(c.x); ub.x32 = x32; ub.st = st;
-  cudaError_t e = run_body<0, false>(*c.h, c.n, ub, noupd, s);
+  MixPBody<false> pb;
+  pb.r = r; pb.p = p; pb.v = v; pb.phat = p; pb.d = nullptr; pb.st = st;
+  cudaError_t e = run_body<0, true>(*c.h, c.n, pb, done, s);
   if (e != cudaSuccess) return e;
-  e = launch_spmv_t<double, kDotSelf, kDotNone>(
-      *c.plan64, *c.h, -1.0, static_cast<const double *>(c.x), 1.0,
-      static_cast<const double *>(c.b), c.r64, nullptr, nullptr, &st->rr64, noupd, s);
-  if (e != cudaSuccess) return e;
-  MixRUpdBody rb;
-  rb.r64 = c.r64; rb.r32 = r; rb.r0 = r0; rb.st = st; rb.cond = cond;
-  e = run_body<2, true>(*c.h, c.n, rb, noupd, s);
-  if (e != cudaSuccess) return e;
-  // one FP32 BiCGSTAB iteration
-  MixPBody<JAC> pb;
-  pb.r = r; pb.p = p; pb.v = v; pb.phat = phat; pb.d = d; pb.st = st;
-  e = run_body<0, true>(*c.h, c.n, pb, done, s);
-  if (e != cudaSuccess) return e;
-  e = launch_spmv_t<float, kDotW, kDotNone>(*c.plan, *c.h, 1.0, phat, 0.0, nullptr, v, r0,
+  e = launch_spmv_t<float, kDotW, kDotNone>(*c.plan, *c.h, 1.0, p, 0.0, nullptr, v, r0,
                                             nullptr, &st->vr0, done, s);
   if (e != cudaSuccess) return e;
-  BiSBody<float, JAC> sb;
-  sb.r = r; sb.v = v; sb.s = sv; sb.shat = shat; sb.d = d; sb.st = st;
+  BiSBody<float, false> sb;
+  sb.r = r; sb.v = v; sb.s = sv; sb.shat = sv; sb.d = nullptr; sb.st = st;
   e = run_body<0, true>(*c.h, c.n, sb, done, s);
   if (e != cudaSuccess) return e;
-  e = launch_spmv_t<float, kDotW, kDotSelf>(*c.plan, *c.h, 1.0, shat, 0.0, nullptr, t, sv,
+  e = launch_spmv_t<float, kDotW, kDotSelf>(*c.plan, *c.h, 1.0, sv, 0.0, nullptr, t, sv,
                                             nullptr, &st->ts, done, s);
   if (e != cudaSuccess) return e;
   MixXRBody xb;
-  xb.x = x32; xb.r = r; xb.r0 = r0; xb.phat = phat; xb.shat = shat; xb.s = sv; xb.t = t;
-  xb.st = st;
+  xb.x = x32; xb.r = r; xb.r0 = r0; xb.phat = p; xb.shat = sv; xb.s = sv; xb.t = t;
+  xb.st = st; xb.upd_cond = c.upd_cond;
   return run_body<2, true>(*c.h, c.n, xb, done, s);
+}
+
+// The reliable update: x += s D^-1 x32, r64 = b - A x (FP64), r32 = r64 / s.
+// In a graph it sits under an IF node; launched one by one, each kernel
+// skips itself unless an update is pending.
+cudaError_t mixbi_update(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  float *r = wsv<float>(c, 0), *r0 = wsv<float>(c, 1), *x32 = wsv<float>(c, 6);
+  SolverState *st = c.h->state;
+  const int *skip = c.upd_cond.enabled ? nullptr : &st->noupd;
+  MixXUpdBody ub;
+  ub.x64 = static_cast<double *>(c.x); ub.x32 = x32;
+  ub.dinv = static_cast<const double *>(c.d); ub.st = st;
+  cudaError_t e = run_body<0, false>(*c.h, c.n, ub, skip, s);
+  if (e != cudaSuccess) return e;
+  e = launch_spmv_t<double, kDotSelf, kDotNone>(
+      *c.plan64, *c.h, -1.0, static_cast<const double *>(c.x), 1.0,
+      static_cast<const double *>(c.b), c.r64, nullptr, nullptr, &st->rr64, skip, s);
+  if (e != cudaSuccess) return e;
+  MixRUpdBody rb;
+  rb.r64 = c.r64; rb.r32 = r; rb.r0 = r0; rb.st = st; rb.cond = cond;
+  return run_body<2, true>(*c.h, c.n, rb, skip, s);
+}
+
+cudaError_t mixbi_iter(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  cudaError_t e = mixbi_main(c, s, cond);
+  if (e != cudaSuccess) return e;
+  return mixbi_update(c, s, cond);
 }
 
 using StepFn = cudaError_t (*)(const SolveCtx &, cudaStream_t, CondRef);
@@ -663,8 +772,8 @@ using StepFn = cudaError_t (*)(const SolveCtx &, cudaStream_t, CondRef);
 void pick_steps(const SolveCtx &c, StepFn *init, StepFn *iter) {
   const bool f64 = c.dtype == MLSH_F64;
   if (c.kind == kMixedBiCGSTAB) {
-    *init = c.jac ? mixbi_init<true> : mixbi_init<false>;
-    *iter = c.jac ? mixbi_iter<true> : mixbi_iter<false>;
+    *init = mixbi_init;
+    *iter = mixbi_iter;
     return;
   }
   if (c.kind == kCG) {
@@ -769,13 +878,45 @@ int build_graph(const SolveCtx &c, Handle &h, GraphEntry &out) {
     return MLSH_ERR_CUDA;
   }
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  e = cudaStreamBeginCaptureToGraph(h.capture_stream, body, nullptr, nullptr, 0,
-                                    cudaStreamCaptureModeThreadLocal);
-  if (e == cudaSuccess) {
-    cudaError_t e2 = iter(c, h.capture_stream, cr);
-    cudaGraph_t bb = nullptr;
-    e = cudaStreamEndCapture(h.capture_stream, &bb);
-    if (e == cudaSuccess) e = e2;
+  auto capture = [&](cudaGraph_t into, StepFn fn, const SolveCtx &cc) {
+    cudaError_t ce = cudaStreamBeginCaptureToGraph(h.capture_stream, into, nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+      cudaError_t e2 = fn(cc, h.capture_stream, cr);
+      cudaGraph_t bb = nullptr;
+      ce = cudaStreamEndCapture(h.capture_stream, &bb);
+      if (ce == cudaSuccess) ce = e2;
+    }
+    return ce;
+  };
+  if (c.kind == kMixedBiCGSTAB) {
+    // body = one FP32 iteration, then IF (update pending) { reliable update }
+    cudaGraphConditionalHandle hif;
+    e = cudaGraphConditionalHandleCreate(&hif, body, 0, cudaGraphCondAssignDefault);
+    SolveCtx c2 = c;
+    c2.upd_cond = CondRef{hif, 1};
+    if (e == cudaSuccess) e = capture(body, mixbi_main, c2);
+    if (e == cudaSuccess) {
+      size_t bn = 0;
+      cudaGraphGetNodes(body, nullptr, &bn);
+      std::vector<cudaGraphNode_t> bnodes(bn), bleaves;
+      cudaGraphGetNodes(body, bnodes.data(), &bn);
+      for (auto nd : bnodes) {
+        size_t nd_out = 0;
+        cudaGraphNodeGetDependentNodes(nd, nullptr, &nd_out);
+        if (nd_out == 0) bleaves.push_back(nd);
+      }
+      cudaGraphNodeParams ip = {};
+      ip.type = cudaGraphNodeTypeConditional;
+      ip.conditional.handle = hif;
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      cudaGraphNode_t inode;
+      e = cudaGraphAddNode(&inode, body, bleaves.data(), bleaves.size(), &ip);
+      if (e == cudaSuccess) e = capture(ip.conditional.phGraph_out[0], mixbi_update, c2);
+    }
+  } else {
+    e = capture(body, iter, c);
   }
   if (e != cudaSuccess) {
     cudaGraphDestroy(g);
@@ -1054,28 +1195,25 @@ int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, voi
 
 // Mixed-precision BiCGSTAB with reliable updates on the kernel engine (see
 // MixInitBody): p is the FP64 matrix, p32 its FP32 copy, r64 an n-vector.
-int mixed_bicgstab_kernels(Handle &h, CsrPlan &p, CsrPlan &p32, double *r64, const void *b,
-                           void *x, const mlsh_solver_opts *opts, double inner_tol,
+int mixed_bicgstab_kernels(Handle &h, CsrPlan &p, CsrPlan &p32, double *r64,
+                           const double *dinv64, const void *b, void *x,
+                           const mlsh_solver_opts *opts, double inner_tol,
                            mlsh_solver_result *res) {
   const int64_t n = p.n_rows;
   SolveCtx c;
   c.kind = kMixedBiCGSTAB;
   c.dtype = MLSH_F32;
-  c.jac = opts->precond == MLSH_PRECOND_JACOBI;
+  c.jac = dinv64 != nullptr;
   c.plan = &p32;
   c.plan64 = &p;
   c.r64 = r64;
   c.h = &h;
   c.b = b;
   c.x = x;
-  c.d = nullptr;
+  c.d = dinv64;
   c.n = n;
-  if (c.jac) {
-    const int st = plan_inv_diag(p32, h.stream, &c.d);
-    if (st != MLSH_SUCCESS) return st;
-  }
   const int64_t n_al = (int64_t)(((size_t)n * 4 + 255) / 256 * 256 / 4);
-  int st = ensure_ws(h, (size_t)9 * (size_t)n_al * 4);
+  int st = ensure_ws(h, (size_t)7 * (size_t)n_al * 4);
   if (st != MLSH_SUCCESS) return st;
   c.ws = h.ws;
   c.stride = n_al;

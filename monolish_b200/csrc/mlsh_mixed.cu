@@ -37,6 +37,7 @@ struct MixedExtras {
   float *r32 = nullptr;
   float *d32 = nullptr;
   bool valid = false;
+  int scaled = 0;  // val32 holds A D^-1 (Jacobi folded in) rather than A
 };
 
 namespace {
@@ -54,6 +55,36 @@ struct AddScaledBody : NoPrep {  // x += s * d (FP64)
   double s;
   __device__ void operator()(int64_t i, double *) const { x[i] = s * (double)d[i] + x[i]; }
 };
+
+// val32[j] = val[j] / A(col[j], col[j]): A D^-1 rounded once to FP32.
+__global__ void to_f32_right_scaled(const double *val, const int *col, const double *dinv,
+                                    int64_t nnz, float *out) {
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nnz;
+       j += (int64_t)gridDim.x * blockDim.x)
+    out[j] = (float)(val[j] * dinv[col[j]]);
+}
+
+// The FP32 values of the extras in the requested form.
+int fill_val32(Handle &h, CsrPlan &p, MixedExtras *m, const double *dinv) {
+  if (p.nnz <= 0) return MLSH_SUCCESS;
+  if (dinv) {
+    const int64_t nnz = p.nnz;
+    const unsigned g = (unsigned)std::min<int64_t>((nnz + 255) / 256, (int64_t)h.num_sms * 16);
+    to_f32_right_scaled<<<g, 256, 0, h.stream>>>(static_cast<const double *>(p.val), p.col_ind,
+                                                 dinv, nnz, m->val32);
+    MLSH_CUDA_TRY(cudaGetLastError());
+    return MLSH_SUCCESS;
+  }
+  ToF32Body cv;
+  cv.src = static_cast<const double *>(p.val);
+  cv.dst = m->val32;
+  cv.scale = 1.0;
+  RedArgs ra{h.partials, h.counters, nullptr};
+  vec_kernel<0, false, ToF32Body>
+      <<<vec_grid(p.nnz, h.num_sms), kVecThreads, 0, h.stream>>>(p.nnz, cv, ra);
+  MLSH_CUDA_TRY(cudaGetLastError());
+  return MLSH_SUCCESS;
+}
 
 template <typename Body>
 int run_plain(const Handle &h, int64_t n, const Body &b) {
@@ -152,7 +183,10 @@ void free_extras(MixedExtras *m, cudaStream_t s) {
   m->valid = false;
 }
 
-int ensure_extras(mlsh_handle hs, CsrPlan &p, MixedExtras **out) {
+// The FP32 copy of p: plain (dinv == nullptr) or right-scaled by the FP64
+// inverse diagonal `dinv`.  Switching between the two rewrites the values
+// only; the structure (tiles, 16-bit columns) is kept.
+int ensure_extras(mlsh_handle hs, CsrPlan &p, MixedExtras **out, const double *dinv) {
   Handle &h = hs->h;
   MixedExtras *m = static_cast<MixedExtras *>(p.extras);
   if (!m) {
@@ -160,7 +194,14 @@ int ensure_extras(mlsh_handle hs, CsrPlan &p, MixedExtras **out) {
     if (!m) return MLSH_ERR_OOM;
     p.extras = m;
   }
+  const int want = dinv != nullptr ? 1 : 0;
   if (m->valid) {
+    if (m->scaled != want) {
+      const int st = fill_val32(h, p, m, dinv);
+      if (st != MLSH_SUCCESS) return st;
+      mlsh_csr_plan_values_changed(m->plan32);
+      m->scaled = want;
+    }
     *out = m;
     return MLSH_SUCCESS;
   }
@@ -175,14 +216,11 @@ int ensure_extras(mlsh_handle hs, CsrPlan &p, MixedExtras **out) {
     free_extras(m, h.stream);
     return MLSH_ERR_OOM;
   }
-  if (p.nnz > 0) {
-    ToF32Body cv;
-    cv.src = static_cast<const double *>(p.val);
-    cv.dst = m->val32;
-    cv.scale = 1.0;
-    const int st = run_plain(h, p.nnz, cv);
+  {
+    const int st = fill_val32(h, p, m, dinv);
     if (st != MLSH_SUCCESS) return st;
   }
+  m->scaled = want;
   int st = mlsh_csr_plan_create(hs, p.n_rows, p.n_cols, p.nnz, p.row_ptr, p.col_ind, m->val32,
                                 MLSH_F32, nullptr, 0, &m->plan32);
   if (st != MLSH_SUCCESS) return st;
@@ -231,9 +269,6 @@ int mixed_solve(int kind, mlsh_handle hs, mlsh_csr_plan ps, const void *d_b, voi
   if (n == 0) return kind == 0 ? mlsh_cg_solve(hs, ps, d_b, d_x, opts, res)
                                : mlsh_bicgstab_solve(hs, ps, d_b, d_x, opts, res);
   if (!d_b || !d_x) return MLSH_ERR_INVALID_ARG;
-  MixedExtras *m = nullptr;
-  int st = ensure_extras(hs, p, &m);
-  if (st != MLSH_SUCCESS) return st;
   // Large systems (the FP32 iteration on the kernel engine): BiCGSTAB with
   // reliable updates in one graph.  Systems that fit a thread-block cluster
   // keep the restarted refinement below, whose inner solves run on it.
@@ -241,11 +276,23 @@ int mixed_solve(int kind, mlsh_handle hs, mlsh_csr_plan ps, const void *d_b, voi
       opts->engine == MLSH_ENGINE_CLUSTER ||
       (opts->engine == MLSH_ENGINE_AUTO && opts->maxiter <= kClusterMaxIterAuto &&
        cluster_rows_for(kind, MLSH_F32, n, opts->cluster_rows) != 0);
+  MixedExtras *m = nullptr;
   if (kind == 1 && !inner_on_cluster) {
     if (opts->precond != MLSH_PRECOND_NONE && opts->precond != MLSH_PRECOND_JACOBI)
       return MLSH_ERR_INVALID_ARG;
-    return mixed_bicgstab_kernels(h, p, m->plan32->p, m->r64, d_b, d_x, opts, inner_tol, res);
+    const void *dinv = nullptr;
+    if (opts->precond == MLSH_PRECOND_JACOBI) {
+      const int s2 = plan_inv_diag(p, h.stream, &dinv);
+      if (s2 != MLSH_SUCCESS) return s2;
+    }
+    int s1 = ensure_extras(hs, p, &m, static_cast<const double *>(dinv));
+    if (s1 != MLSH_SUCCESS) return s1;
+    return mixed_bicgstab_kernels(h, p, m->plan32->p, m->r64,
+                                  static_cast<const double *>(dinv), d_b, d_x, opts, inner_tol,
+                                  res);
   }
+  int st = ensure_extras(hs, p, &m, nullptr);
+  if (st != MLSH_SUCCESS) return st;
 
   mlsh_solver_opts in = *opts;
   in.tol = inner_tol;

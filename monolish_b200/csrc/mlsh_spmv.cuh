@@ -90,8 +90,9 @@ struct SpmvArgs {
 
 template <typename VT, int STAGES, int CSZ = 4>
 struct SpmvSmem {
-  static constexpr int kValBytes = ((kTileNnz * (int)sizeof(VT) + 16) + 15) & ~15;
-  static constexpr int kColBytes = ((kTileNnz * CSZ + 16) + 15) & ~15;
+  // a tile's range rounded out to 16-byte boundaries: at most 32 extra bytes
+  static constexpr int kValBytes = ((kTileNnz * (int)sizeof(VT) + 32) + 15) & ~15;
+  static constexpr int kColBytes = ((kTileNnz * CSZ + 32) + 15) & ~15;
   static constexpr int kStageBytes = kValBytes + kColBytes;
   static constexpr int kYsOff = STAGES * kStageBytes;
   static constexpr int kSegSumOff = kYsOff + kTileRows * (int)sizeof(VT) + 16;
@@ -139,34 +140,21 @@ __device__ __forceinline__ bool consumers_sync_or(bool pred) {
   return r != 0;
 }
 
-// Producer side: stage tile elements [nb, ne) of `arr` into smem `dst`,
-// element nb landing at dst[head].  The <16-byte ragged ends are loaded by
-// lanes 0..15 (head) and 16..31 (tail).  Returns the bytes the bulk copy
-// of the aligned interior will deliver (0 if none).  Called by all lanes.
+// Producer side: the bulk copy of a tile's [nb, ne) range of `arr` covers
+// the range rounded out to 16-byte boundaries (what a bulk copy needs), so
+// element nb lands at element offset head_elems(arr, nb) of the stage.  The
+// rounded range never leaves the 16-byte chunks holding elements nb and
+// ne-1, so it stays inside memory that holds the array.
 template <typename E>
-__device__ __forceinline__ uint32_t stage_range(const E *arr, int nb, int ne, E *dst,
-                                                int lane) {
-  const uintptr_t b0 = (uintptr_t)(arr + nb);
-  const uintptr_t b1 = (uintptr_t)(arr + ne);
-  const uintptr_t lo = b0 & ~(uintptr_t)15;
-  uintptr_t i0 = (b0 + 15) & ~(uintptr_t)15;
-  uintptr_t i1 = b1 & ~(uintptr_t)15;
-  const int head = (int)((b0 - lo) / sizeof(E));
-  int e0, e1;
-  if (i1 > i0) {
-    e0 = nb + (int)((i0 - b0) / sizeof(E));
-    e1 = nb + (int)((i1 - b0) / sizeof(E));
-  } else {
-    e0 = ne;  // everything by plain loads
-    e1 = ne;
-    i0 = i1 = 0;
+__device__ __forceinline__ uint32_t rounded_range(const E *arr, int nb, int ne, uintptr_t *src) {
+  if (ne <= nb) {
+    *src = 0;
+    return 0;
   }
-  const int nhead = e0 - nb;
-  const int ntail = ne - e1;
-  if (lane < nhead) dst[head + lane] = arr[nb + lane];
-  if (lane >= 16 && lane - 16 < ntail)
-    dst[head + (e1 - nb) + (lane - 16)] = arr[e1 + (lane - 16)];
-  return (uint32_t)(i1 - i0);
+  const uintptr_t lo = (uintptr_t)(arr + nb) & ~(uintptr_t)15;
+  const uintptr_t hi = ((uintptr_t)(arr + ne) + 15) & ~(uintptr_t)15;
+  *src = lo;
+  return (uint32_t)(hi - lo);
 }
 
 // C16: columns stored as 16-bit offsets from a per-tile base (2 bytes per
@@ -207,9 +195,13 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
     const uint64_t stream_policy = l2_evict_first_policy();
     int k = 0;
     bool aborted = false;
+    Tile tl_next = {0, 0, 0, 0, 0, {0, 0, 0}};
+    if ((int)blockIdx.x < a.n_tiles) tl_next = a.tiles[blockIdx.x];
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++k) {
       const int s = k % STAGES;
-      const Tile tl = a.tiles[t];  // issued before the wait for a free stage
+      const Tile tl = tl_next;
+      // the next tile's record is in flight while this one is issued
+      if (t + (int)gridDim.x < a.n_tiles) tl_next = a.tiles[t + gridDim.x];
       if (k >= STAGES) {
         int ok = 1;
         if (lane == 0) {
@@ -228,38 +220,21 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (!ok) { aborted = true; break; }
       }
-      unsigned char *st = smem + s * L::kStageBytes;
-      VT *sv = reinterpret_cast<VT *>(st);
-      const uint32_t bar = full0 + 8 * s;
-      const uint32_t vb = stage_range<VT>(a.val, tl.nnz_begin, tl.nnz_end, sv, lane);
-      uint32_t cb;
-      const void *col_src;
-      if constexpr (C16) {
-        cb = stage_range<uint16_t>(a.col16, tl.nnz_begin, tl.nnz_end,
-                                   reinterpret_cast<uint16_t *>(st + L::kValBytes), lane);
-        col_src = a.col16 + tl.nnz_begin;
-      } else {
-        cb = stage_range<int>(a.col, tl.nnz_begin, tl.nnz_end,
-                              reinterpret_cast<int *>(st + L::kValBytes), lane);
-        col_src = a.col + tl.nnz_begin;
-      }
-      __threadfence_block();
-      __syncwarp();
       if (lane == 0) {
+        unsigned char *st = smem + s * L::kStageBytes;
+        const uint32_t bar = full0 + 8 * s;
+        uintptr_t vsrc, csrc;
+        const uint32_t vb = rounded_range<VT>(a.val, tl.nnz_begin, tl.nnz_end, &vsrc);
+        uint32_t cb;
+        if constexpr (C16)
+          cb = rounded_range<uint16_t>(a.col16, tl.nnz_begin, tl.nnz_end, &csrc);
+        else
+          cb = rounded_range<int>(a.col, tl.nnz_begin, tl.nnz_end, &csrc);
         fence_proxy_async_smem();
         mbar_arrive_expect_tx(bar, vb + cb);
-        if (vb) {
-          const uintptr_t i0 = ((uintptr_t)(a.val + tl.nnz_begin) + 15) & ~(uintptr_t)15;
-          const uintptr_t lo = (uintptr_t)(a.val + tl.nnz_begin) & ~(uintptr_t)15;
-          bulk_g2s_hint(smem_addr(st) + (uint32_t)(i0 - lo), (const void *)i0, vb, bar,
-                        stream_policy);
-        }
-        if (cb) {
-          const uintptr_t i0 = ((uintptr_t)col_src + 15) & ~(uintptr_t)15;
-          const uintptr_t lo = (uintptr_t)col_src & ~(uintptr_t)15;
-          bulk_g2s_hint(smem_addr(st + L::kValBytes) + (uint32_t)(i0 - lo), (const void *)i0,
-                        cb, bar, stream_policy);
-        }
+        if (vb) bulk_g2s_hint(smem_addr(st), (const void *)vsrc, vb, bar, stream_policy);
+        if (cb)
+          bulk_g2s_hint(smem_addr(st + L::kValBytes), (const void *)csrc, cb, bar, stream_policy);
       }
       __syncwarp();
     }

@@ -7,6 +7,8 @@
 // update their device-side scalars and convergence state without a host
 // round trip.  Grid geometry depends only on n, so sums are reproducible.
 #pragma once
+#include <type_traits>
+
 #include "mlsh_internal.cuh"
 #include "mlsh_reduce.cuh"
 
@@ -44,6 +46,58 @@ __global__ void __launch_bounds__(kVecThreads)
     }
   }
 }
+
+// --------------------------------------------------------- packed form --
+// Bodies that provide `template <int W> step(i, acc)` over W consecutive
+// elements (and a host-side aligned() check of their pointers) run with
+// 16-byte vector loads and stores: 4 floats or 2 doubles per access, four
+// or two times the bytes in flight per load instruction.
+template <typename T, int W>
+struct alignas(sizeof(T) * W) Pack {
+  T v[W];
+};
+template <int W, typename T>
+__device__ __forceinline__ Pack<T, W> ldp(const T *p, int64_t i) {
+  return *reinterpret_cast<const Pack<T, W> *>(p + i);
+}
+template <int W, typename T>
+__device__ __forceinline__ void stp(T *p, int64_t i, const Pack<T, W> &x) {
+  *reinterpret_cast<Pack<T, W> *>(p + i) = x;
+}
+inline bool al16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+template <int NR, bool FIN, int W, typename Body>
+__global__ void __launch_bounds__(kVecThreads)
+    vec_pack_kernel(int64_t n, Body body, RedArgs ra) {
+  if (ra.done != nullptr && *ra.done != 0) return;
+  constexpr int NA = NR > 0 ? NR : 1;
+  __shared__ double red[kVecThreads / 32 * NA];
+  __shared__ int last_flag;
+  body.prepare();
+  double acc[NA];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) acc[k] = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t np = n / W;
+  for (int64_t q = gt; q < np; q += stride) body.template step<W>(q * W, acc);
+  for (int64_t i = np * W + gt; i < n; i += stride) body.template step<1>(i, acc);
+  if constexpr (NR > 0 || FIN) {
+    group_sum<NA>(acc, red, threadIdx.x, kVecThreads, 0);
+    if (publish_partials<NA>(acc, ra.partials, ra.counter, &last_flag, threadIdx.x,
+                             kVecThreads, 0)) {
+      double tot[NA];
+      reduce_partials<NA>(tot, ra.partials, (int)gridDim.x, nullptr, 0, NA, ra.counter,
+                          red, threadIdx.x, kVecThreads, 0);
+      if (threadIdx.x == 0) body.finish(tot);
+    }
+  }
+}
+
+template <typename B, typename = void>
+struct has_step : std::false_type {};
+template <typename B>
+struct has_step<B, std::void_t<decltype(&B::aligned)>> : std::true_type {};
 
 // ---------------------------------------------------------------- bodies --
 struct NoPrep {
