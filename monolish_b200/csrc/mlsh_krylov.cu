@@ -580,6 +580,26 @@ struct MixXRBody : NoPrep {  // x32 += a phat + w shat; r = s - w t; decide on a
 // --------------------------------------------------------------- driver --
 namespace {
 
+// CTAs of a packed launch: at most one wave of the kernel's resident CTAs
+// (a second partial wave would leave most SMs idle at its end).
+template <auto kernel>
+int pack_grid(int64_t n, int w, int num_sms) {
+  static int per_sm = 0;  // one value per kernel
+  if (per_sm == 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kVecThreads, 0) !=
+            cudaSuccess ||
+        b < 1) {
+      cudaGetLastError();
+      b = 1;
+    }
+    per_sm = std::min(b, kMaxVecBlocksPerSm);
+  }
+  int64_t g = (n + (int64_t)kVecThreads * w * 4 - 1) / ((int64_t)kVecThreads * w * 4);
+  g = std::min<int64_t>(g, (int64_t)per_sm * num_sms);
+  return (int)std::max<int64_t>(g, 1);
+}
+
 template <int NR, bool FIN, typename Body>
 cudaError_t run_body(const Handle &h, int64_t n, const Body &b, const int *done,
                      cudaStream_t s) {
@@ -587,10 +607,13 @@ cudaError_t run_body(const Handle &h, int64_t n, const Body &b, const int *done,
   const int g = vec_grid(n, h.num_sms);
   if constexpr (has_step<Body>::value) {
     constexpr int W = 16 / (int)sizeof(typename Body::elem);
-    if (b.aligned())
-      vec_pack_kernel<NR, FIN, W, Body><<<g, kVecThreads, 0, s>>>(n, b, ra);
-    else
-      vec_pack_kernel<NR, FIN, 1, Body><<<g, kVecThreads, 0, s>>>(n, b, ra);
+    if (b.aligned()) {
+      constexpr auto k = vec_pack_kernel<NR, FIN, W, Body>;
+      k<<<pack_grid<k>(n, W, h.num_sms), kVecThreads, 0, s>>>(n, b, ra);
+    } else {
+      constexpr auto k = vec_pack_kernel<NR, FIN, 1, Body>;
+      k<<<pack_grid<k>(n, 1, h.num_sms), kVecThreads, 0, s>>>(n, b, ra);
+    }
   } else {
     vec_kernel<NR, FIN, Body><<<g, kVecThreads, 0, s>>>(n, b, ra);
   }
