@@ -34,14 +34,14 @@ void build_tiles(const int *rp, int n_rows, std::vector<Tile> &tiles,
   int r = 0;
   while (r < n_rows) {
     const int len = rp[r + 1] - rp[r];
-    if (len > kTileNnz) {
+    if (len > kLongRow) {
       const int li = (int)longs.size();
       const int nch = (len + kTileNnz - 1) / kTileNnz;
       longs.push_back(LongRow{r, n_chunks, nch, 0});
       for (int c = 0; c < nch; ++c) {
         const int b = rp[r] + c * kTileNnz;
         const int e = std::min(b + kTileNnz, rp[r + 1]);
-        tiles.push_back(Tile{r, -(li + 1), b, e, 0, {0, 0, 0}});
+        tiles.push_back(Tile{r, -(li + 1), b, e, 0, {nch, 0, 0}});
       }
       n_chunks += nch;
       ++r;
@@ -51,7 +51,7 @@ void build_tiles(const int *rp, int n_rows, std::vector<Tile> &tiles,
     int nnz = 0, longest = 0;
     while (r < n_rows && r - rb < kTileRows) {
       const int l = rp[r + 1] - rp[r];
-      if (l > kTileNnz || nnz + l > kTileNnz) break;
+      if (l > kLongRow || nnz + l > kTileNnz) break;
       nnz += l;
       longest = std::max(longest, l);
       ++r;

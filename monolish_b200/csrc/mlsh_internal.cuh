@@ -19,6 +19,11 @@ namespace mlsh {
 // chunks of kTileNnz nonzeros that are summed by a second step.
 constexpr int kTileRows = 256;
 constexpr int kTileNnz = 1792;  // = 256 rows x 7 nonzeros (7-point stencil)
+// Rows longer than this get tiles of their own (chunks of kTileNnz), summed
+// by the whole CTA; shorter rows are summed by the warp that owns them.
+// (A lower threshold was measured slower on Zipf-law rows: one-row tiles
+// cost a CTA barrier each.)
+constexpr int kLongRow = kTileNnz;
 constexpr int kConsumers = 256;  // consumer threads per CTA (8 warps)
 constexpr int kSpmvThreads = kConsumers + 32;  // + one producer warp
 constexpr int kShortRow = 8;     // rows up to this length: thread-per-row sum
@@ -38,7 +43,8 @@ constexpr int kRunning = 1;
 
 // --------------------------------------------------------- tile record ---
 // Normal tile: rows [row_begin, row_end), nonzeros [nnz_begin, nnz_end).
-// Chunk of a long row: row_begin = row, row_end = -(long_index + 1).
+// Chunk of a long row: row_begin = row, row_end = -(long_index + 1),
+// pad[0] = the row's chunk count.
 // short_only: every row of a normal tile has at most kShortRow entries.
 struct __align__(16) Tile {
   int row_begin;

@@ -11,27 +11,21 @@
 //  * A persistent grid (a few CTAs per SM) walks the tiles round-robin, so
 //    every CTA's work and summation order are fixed by the sizes.
 //  * Warp specialisation: warp 0 is the producer.  Lane 0 streams each
-//    tile's contiguous val[] and col_ind[] ranges into a STAGES-deep ring
-//    of shared-memory stages with 1-D bulk (TMA) copies that complete on an
-//    mbarrier; the other lanes fill the <16-byte ragged ends with plain
-//    loads.  HBM sees only long, aligned, fully used bursts, and the copies
-//    carry an L2 evict-first policy so the once-read matrix does not push
-//    the gathered x out of L2.
-//  * 8 consumer warps.  Each thread first issues the row_ptr loads of its
-//    row of the tile (independent of the stage, so they overlap the wait),
-//    then:
-//      pass A  val[j]*x[col[j]] in place over the tile's nonzeros
-//              (nonzero-parallel: the x gathers are balanced and
-//              independent; x goes through the read-only path);
-//      pass B  one thread sums each row of up to kShortRow entries in row
-//              order (the reference's loop order, so those rows are
-//              bit-identical to it);
-//      pass C  longer rows are cut into kSegW-entry segments spread over
-//              all warps (an 8-lane tree per segment, four segments per
-//              warp instruction), then each row adds its segment sums in
-//              order -- balanced and deterministic;
-//      pass D  y written coalesced, fused dots accumulated in a fixed
-//              per-thread order.
+//    tile's contiguous val[] and col_ind[] ranges (rounded out to 16-byte
+//    boundaries) into a STAGES-deep ring of shared-memory stages with 1-D
+//    bulk (TMA) copies that complete on an mbarrier.  HBM sees only long,
+//    aligned, fully used bursts, and the copies carry an L2 evict-first
+//    policy so the once-read matrix does not push the gathered x out of L2.
+//  * 8 consumer warps, each owning 32 rows of the tile and working on its
+//    own between the "stage full" barrier and its own stage release:
+//      rows of up to kShortRow entries: one thread each, gathering x and
+//              summing in row order with separately rounded products (the
+//              reference's loop, so those rows are bit-identical to it);
+//      longer rows: the whole warp, one such row after another (lane-
+//              strided partial sums, then an xor tree) -- deterministic;
+//      then y is written coalesced and the fused dots accumulate in a
+//      fixed per-thread order.  Each thread's row bounds, dot weight and
+//      the tile's column base for the next tile are fetched one tile ahead.
 //  * Chunk tiles reduce their products CTA-wide into a per-chunk partial;
 //    the last chunk to arrive (atomic counter per long row) sums the
 //    partials in chunk order and writes the row.
@@ -51,13 +45,6 @@ namespace mlsh {
 constexpr int kDotNone = 0;
 constexpr int kDotW = 1;     // sum w[i] * y[i]
 constexpr int kDotSelf = 2;  // sum y[i] * y[i]
-
-// Rows longer than kShortRow are summed in segments of kSegW entries.
-constexpr int kSegW = 8;
-// Upper bound of segments in one tile: each such row has > kSegW entries,
-// so ceil(len/kSegW) < 2*len/kSegW.
-constexpr int kMaxSegs = 2 * kTileNnz / kSegW;
-static_assert(kShortRow >= kSegW, "segments must not be longer than short rows");
 
 template <typename VT, typename XT>
 struct SpmvArgs {
@@ -94,10 +81,7 @@ struct SpmvSmem {
   static constexpr int kValBytes = ((kTileNnz * (int)sizeof(VT) + 32) + 15) & ~15;
   static constexpr int kColBytes = ((kTileNnz * CSZ + 32) + 15) & ~15;
   static constexpr int kStageBytes = kValBytes + kColBytes;
-  static constexpr int kYsOff = STAGES * kStageBytes;
-  static constexpr int kSegSumOff = kYsOff + kTileRows * (int)sizeof(VT) + 16;
-  static constexpr int kSegIdxOff = kSegSumOff + kMaxSegs * (int)sizeof(VT) + 16;
-  static constexpr int kBarOff = (kSegIdxOff + 2 * kMaxSegs * 2 + 64 + 15) & ~15;
+  static constexpr int kBarOff = STAGES * kStageBytes;
   static constexpr int kRedOff = kBarOff + 2 * STAGES * 8;
   static constexpr int kFlagOff = kRedOff + 32 * 8;
   static constexpr int kBytes = kFlagOff + 16 * 4;
@@ -108,7 +92,6 @@ constexpr int kFlagProdAbort = 0;
 constexpr int kFlagConsAbort = 1;
 constexpr int kFlagConsumed = 2;
 constexpr int kFlagLast = 3;
-constexpr int kFlagWarpSeg = 4;  // 8 per-warp segment counts (4..11)
 
 template <typename T>
 __device__ __forceinline__ T spmv_mul_rn(T a, T b) {
@@ -124,20 +107,6 @@ __device__ __forceinline__ T spmv_add_rn(T a, T b) {
 template <typename T>
 __device__ __forceinline__ int head_elems(const T *base, int idx) {
   return (int)(((uintptr_t)(base + idx) & 15u) / sizeof(T));
-}
-
-// Named barrier over the consumer threads that also ORs a predicate.
-__device__ __forceinline__ bool consumers_sync_or(bool pred) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.u32 p, %1, 0;\n\t"
-      "bar.red.or.pred q, 1, %2, p;\n\t"
-      "selp.u32 %0, 1, 0, q;\n\t}"
-      : "=r"(r)
-      : "r"((uint32_t)pred), "n"(kConsumers)
-      : "memory");
-  return r != 0;
 }
 
 // Producer side: the bulk copy of a tile's [nb, ne) range of `arr` covers
@@ -171,10 +140,6 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::kBarOff);
   double *red = reinterpret_cast<double *>(smem + L::kRedOff);
   volatile int *flags = reinterpret_cast<volatile int *>(smem + L::kFlagOff);
-  VT *ys = reinterpret_cast<VT *>(smem + L::kYsOff);
-  VT *segsum = reinterpret_cast<VT *>(smem + L::kSegSumOff);
-  short *seg_lo = reinterpret_cast<short *>(smem + L::kSegIdxOff);
-  short *seg_hi = seg_lo + kMaxSegs;
   const int tid = threadIdx.x;
   const uint32_t full0 = smem_addr(bars);
   const uint32_t empty0 = smem_addr(bars + STAGES);
@@ -274,7 +239,6 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
 #pragma unroll
   for (int q = 0; q < (NR > 0 ? NR : 1); ++q) acc[q] = 0.0;
   const double alpha = a.alpha, beta = a.beta;
-  constexpr int kPer = kTileNnz / kConsumers;  // 7 products per thread
 
   // Per-tile values each thread needs besides the staged val/col: the tile
   // record, its row bounds, the 16-bit column base and the fused dot's
@@ -321,50 +285,18 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
 
     const int nb = tl.nnz_begin, ne = tl.nnz_end, nt = ne - nb;
     unsigned char *st = smem + s * L::kStageBytes;
-    VT *v = reinterpret_cast<VT *>(st) + head_elems(a.val, nb);
-
-    if (normal && tl.short_only) {
-      // ---------------------------------------------- direct: short rows
-      // Every row has <= kShortRow entries: each thread gathers and sums
-      // its own row in row order with separately rounded products (the
-      // reference's loop, as passes A+B compute it), with no exchange
-      // through shared memory and no barrier before the stage is released.
-      VT sum = VT(0);
-      if (ct < nrows) {
-        const int s0 = g0 - nb, len = g1 - g0;
-        XT xx[kShortRow];
-        if constexpr (C16) {
-          const uint16_t *c = reinterpret_cast<const uint16_t *>(st + L::kValBytes) +
-                              head_elems(a.col16, nb);
-#pragma unroll
-          for (int u = 0; u < kShortRow; ++u)
-            if (u < len) xx[u] = __ldg(a.x + col_base + (int)c[s0 + u]);
-        } else {
-          const int *c = reinterpret_cast<const int *>(st + L::kValBytes) + head_elems(a.col, nb);
-#pragma unroll
-          for (int u = 0; u < kShortRow; ++u)
-            if (u < len) xx[u] = __ldg(a.x + c[s0 + u]);
-        }
-#pragma unroll
-        for (int u = 0; u < kShortRow; ++u)
-          if (u < len) sum = spmv_add_rn(sum, spmv_mul_rn(v[s0 + u], (VT)xx[u]));
-      }
-      // this warp is done with the stage
-      __syncwarp();
-      if (lane == 0) mbar_arrive(empty0 + 8 * s);
-      if (ct == 0) flags[kFlagConsumed] = k + 1;
-      if (ct < nrows) {
-        const int r = rb + ct;
-        const double dsum = (double)sum;
-        const XT out = (beta == 0.0) ? (XT)(alpha * dsum)
-                                     : (XT)(alpha * dsum + beta * (double)a.y_in[r]);
-        a.y_out[r] = out;
-        if constexpr (M0 == kDotW) acc[0] += (double)w0v * (double)out;
-        if constexpr (M0 == kDotSelf) acc[0] += (double)out * (double)out;
-        if constexpr (M1 == kDotW) acc[1] += (double)a.w1[r] * (double)out;
-        if constexpr (M1 == kDotSelf) acc[1] += (double)out * (double)out;
-      }
-      // prefetch the next tile's per-thread values
+    const VT *v = reinterpret_cast<const VT *>(st) + head_elems(a.val, nb);
+    const uint16_t *c16 = reinterpret_cast<const uint16_t *>(st + L::kValBytes) +
+                          (C16 ? head_elems(a.col16, nb) : 0);
+    const int *c32 = reinterpret_cast<const int *>(st + L::kValBytes) +
+                     (C16 ? 0 : head_elems(a.col, nb));
+    // column of the tile's j-th staged entry
+    auto col_at = [&](int j) -> int {
+      if constexpr (C16) return col_base + (int)c16[j];
+      else return c32[j];
+    };
+    // the next tile's per-thread values, fetched while this tile computes
+    auto prefetch_next = [&]() {
       g0c = g1c = cbc = 0;
       w0c = XT(0);
       if (tn < a.n_tiles) {
@@ -377,120 +309,57 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
         if constexpr (C16) cbc = __ldg(a.tile_base + tn);
       }
       tl_c = tl_n;
-      continue;
-    }
-
-    // pass A: products in place
-    {
-      int cc[kPer];
-      XT xx[kPer];
-      if constexpr (C16) {
-        const uint16_t *c = reinterpret_cast<const uint16_t *>(st + L::kValBytes) +
-                            head_elems(a.col16, nb);
-#pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-          const int j = ct + u * kConsumers;
-          cc[u] = (j < nt) ? col_base + (int)c[j] : 0;
-        }
-      } else {
-        const int *c = reinterpret_cast<const int *>(st + L::kValBytes) + head_elems(a.col, nb);
-#pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-          const int j = ct + u * kConsumers;
-          cc[u] = (j < nt) ? c[j] : 0;
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kPer; ++u) {
-        const int j = ct + u * kConsumers;
-        xx[u] = (j < nt) ? __ldg(a.x + cc[u]) : XT(0);
-      }
-#pragma unroll
-      for (int u = 0; u < kPer; ++u) {
-        const int j = ct + u * kConsumers;
-        if (j < nt) v[j] = v[j] * (VT)xx[u];
-      }
-    }
-    named_sync(1, kConsumers);
-    // prefetch the next tile's per-thread values
-    g0c = g1c = cbc = 0;
-    w0c = XT(0);
-    if (tn < a.n_tiles) {
-      const int nr = tl_n.row_end >= 0 ? tl_n.row_end - tl_n.row_begin : 0;
-      if (ct < nr) {
-        g0c = __ldg(a.row_ptr + tl_n.row_begin + ct);
-        g1c = __ldg(a.row_ptr + tl_n.row_begin + ct + 1);
-        if constexpr (M0 == kDotW) w0c = a.w0[tl_n.row_begin + ct];
-      }
-      if constexpr (C16) cbc = __ldg(a.tile_base + tn);
-    }
-    tl_c = tl_n;
+    };
 
     if (normal) {
-      // ------------------------------------------------ pass B: short rows
-      const int s0 = g0 - nb, s1 = g1 - nb, len = s1 - s0;
-      const bool med = ct < nrows && len > kShortRow;
-      if (ct < nrows && !med) {
-        VT sum = VT(0);
-        for (int j = s0; j < s1; ++j) sum += v[j];
-        ys[ct] = sum;
+      // Each warp handles its 32 rows on its own (no CTA barrier):
+      //  * rows of <= kShortRow entries: one thread each, gathering and
+      //    summing in row order with separately rounded products -- the
+      //    reference's loop, so these rows are bit-identical to it;
+      //  * longer rows: the whole warp, one row after another (lane-strided
+      //    partial sums, then an xor tree), the owning thread keeps the sum.
+      VT sum = VT(0);
+      const int s0 = g0 - nb, len = g1 - g0;
+      if (ct < nrows && len <= kShortRow) {
+        XT xx[kShortRow];
+#pragma unroll
+        for (int u = 0; u < kShortRow; ++u)
+          if (u < len) xx[u] = __ldg(a.x + col_at(s0 + u));
+#pragma unroll
+        for (int u = 0; u < kShortRow; ++u)
+          if (u < len) sum = spmv_add_rn(sum, spmv_mul_rn(v[s0 + u], (VT)xx[u]));
       }
-      // ------------------------------------ pass C: kSegW-entry segments
-      if (consumers_sync_or(med)) {
-        // exclusive scan of segment counts over the tile's rows
-        const int nseg = med ? (len + kSegW - 1) / kSegW : 0;
-        int inc = nseg;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int y = __shfl_up_sync(0xffffffffu, inc, o);
-          if (lane >= o) inc += y;
+      prefetch_next();
+      unsigned lm = __ballot_sync(0xffffffffu, ct < nrows && len > kShortRow);
+      while (lm) {
+        const int src = __ffs(lm) - 1;
+        lm &= lm - 1;
+        const int ls = __shfl_sync(0xffffffffu, s0, src);
+        const int le = ls + __shfl_sync(0xffffffffu, len, src);
+        VT part = VT(0);
+        int j = ls + lane;
+        for (; j + 96 < le; j += 128) {
+          const XT x0 = __ldg(a.x + col_at(j)), x1 = __ldg(a.x + col_at(j + 32)),
+                   x2 = __ldg(a.x + col_at(j + 64)), x3 = __ldg(a.x + col_at(j + 96));
+          part = spmv_add_rn(part, spmv_mul_rn(v[j], (VT)x0));
+          part = spmv_add_rn(part, spmv_mul_rn(v[j + 32], (VT)x1));
+          part = spmv_add_rn(part, spmv_mul_rn(v[j + 64], (VT)x2));
+          part = spmv_add_rn(part, spmv_mul_rn(v[j + 96], (VT)x3));
         }
-        if (lane == 31) flags[kFlagWarpSeg + warp] = inc;
-        named_sync(1, kConsumers);
-        int base = 0, total = 0;
-#pragma unroll
-        for (int w = 0; w < kConsumers / 32; ++w) {
-          const int cw = flags[kFlagWarpSeg + w];
-          if (w < warp) base += cw;
-          total += cw;
-        }
-        const int first = base + inc - nseg;
-        for (int q = 0; q < nseg; ++q) {
-          seg_lo[first + q] = (short)(s0 + kSegW * q);
-          seg_hi[first + q] = (short)min(s0 + kSegW * (q + 1), s1);
-        }
-        named_sync(1, kConsumers);
-        // four segments per warp step: lanes 8g..8g+7 take segment g
-        constexpr int kSegPerWarp = 32 / kSegW;
-        const int sub = lane / kSegW, sl = lane % kSegW;
-        for (int sg0 = warp * kSegPerWarp; sg0 < total; sg0 += kConsumers / kSegW) {
-          const int sg = sg0 + sub;
-          VT part = VT(0);
-          if (sg < total) {
-            const int j = seg_lo[sg] + sl;
-            if (j < seg_hi[sg]) part = v[j];
-          }
-#pragma unroll
-          for (int o = kSegW / 2; o > 0; o >>= 1)
-            part += __shfl_xor_sync(0xffffffffu, part, o, kSegW);
-          if (sl == 0 && sg < total) segsum[sg] = part;
-        }
-        named_sync(1, kConsumers);
-        if (med) {
-          VT sum = VT(0);
-          for (int q = 0; q < nseg; ++q) sum += segsum[first + q];
-          ys[ct] = sum;
-        }
+        for (; j < le; j += 32) part = spmv_add_rn(part, spmv_mul_rn(v[j], (VT)__ldg(a.x + col_at(j))));
+        part = warp_sum(part);
+        if (lane == src) sum = part;
       }
-      // all reads of the stage are done (the last barrier above)
+      // this warp is done with the stage
+      __syncwarp();
       if (lane == 0) mbar_arrive(empty0 + 8 * s);
       if (ct == 0) flags[kFlagConsumed] = k + 1;
-      // ----------------------------------------------------- pass D: y
+      // ----------------------------------------------------- y and dots
       if (ct < nrows) {
         const int r = rb + ct;
-        const double sum = (double)ys[ct];
-        const XT out = (beta == 0.0) ? (XT)(alpha * sum)
-                                     : (XT)(alpha * sum + beta * (double)a.y_in[r]);
+        const double dsum = (double)sum;
+        const XT out = (beta == 0.0) ? (XT)(alpha * dsum)
+                                     : (XT)(alpha * dsum + beta * (double)a.y_in[r]);
         a.y_out[r] = out;
         if constexpr (M0 == kDotW) acc[0] += (double)w0v * (double)out;
         if constexpr (M0 == kDotSelf) acc[0] += (double)out * (double)out;
@@ -500,7 +369,9 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
     } else {
       // --------------------------------------------- chunk of a long row ---
       VT part = VT(0);
-      for (int j = ct; j < nt; j += kConsumers) part += v[j];
+      for (int j = ct; j < nt; j += kConsumers)
+        part = spmv_add_rn(part, spmv_mul_rn(v[j], (VT)__ldg(a.x + col_at(j))));
+      prefetch_next();
       part = warp_sum(part);
       if (lane == 0) red[warp] = (double)part;
       named_sync(1, kConsumers);
@@ -510,16 +381,26 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
         double tot = 0.0;
         for (int w = 0; w < kConsumers / 32; ++w) tot += red[w];
         const int li = -tl.row_end - 1;
-        const LongRow lr = a.longs[li];
-        const int row = lr.row;
-        const int slot = lr.first_slot + (nb - __ldg(a.row_ptr + row)) / kTileNnz;
-        a.chunk_part[slot] = tot;
-        __threadfence();
-        const unsigned prev = atomicAdd(a.long_cnt + li, 1u);
-        if (prev == (unsigned)(lr.n_chunks - 1)) {
+        const int row = tl.row_begin;
+        bool last = true;
+        double sum = tot;
+        if (tl.pad[0] > 1) {
+          // several chunks: the last one to arrive sums them in chunk order
+          const LongRow lr = a.longs[li];
+          const int slot = lr.first_slot + (nb - __ldg(a.row_ptr + row)) / kTileNnz;
+          a.chunk_part[slot] = tot;
           __threadfence();
-          double sum = 0.0;
-          for (int q = 0; q < lr.n_chunks; ++q) sum += __ldcg(a.chunk_part + lr.first_slot + q);
+          const unsigned prev = atomicAdd(a.long_cnt + li, 1u);
+          last = prev == (unsigned)(lr.n_chunks - 1);
+          if (last) {
+            __threadfence();
+            sum = 0.0;
+            for (int q = 0; q < lr.n_chunks; ++q)
+              sum += __ldcg(a.chunk_part + lr.first_slot + q);
+            a.long_cnt[li] = 0u;
+          }
+        }
+        if (last) {
           const double ysum = (double)(VT)sum;
           const XT out = (beta == 0.0) ? (XT)(alpha * ysum)
                                        : (XT)(alpha * ysum + beta * (double)a.y_in[row]);
@@ -533,7 +414,6 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
             a.long_dot[2 * li] = d0;
             a.long_dot[2 * li + 1] = d1;
           }
-          a.long_cnt[li] = 0u;
         }
       }
     }
