@@ -413,6 +413,7 @@ def run_solve(args, wl, rank, world, local):
     db = torch.from_numpy(b).cuda()
     dx = torch.zeros(n, dtype=torch.float64, device="cuda")
     base_fn = D.cg_solve if wl["kind"] == "cg" else D.bicgstab_solve
+    inner_tol = 1e-4 if args.inner_tol is None else args.inner_tol
     mixed_fn = D.cg_solve_mixed if wl["kind"] == "cg" else D.bicgstab_solve_mixed
     engine = {"auto": 0, "kernels": 1, "cluster": 2}[args.engine]
 
@@ -422,7 +423,7 @@ def run_solve(args, wl, rank, world, local):
 
     def fn(A_, b_, x_, tol_, maxiter_):
         if args.precision == "mixed":
-            return mixed_fn(A_, b_, x_, tol_, maxiter_, inner_tol=args.inner_tol, engine=engine,
+            return mixed_fn(A_, b_, x_, tol_, maxiter_, inner_tol=inner_tol, engine=engine,
                             use_graph=not args.eager)
         return plain_fn(A_, b_, x_, tol_, maxiter_)
 
@@ -519,7 +520,7 @@ def run_solve(args, wl, rank, world, local):
             out["config"]["outer_steps"] = r.outer
             out["roofline"]["note"] = ("algorithmic bytes: FP32 inner iterations (V = X = 4) "
                                        "plus an FP64 residual per outer step, / solve time")
-            out["config"]["inner_tol"] = args.inner_tol
+            out["config"]["inner_tol"] = inner_tol
             if plain_ms is not None:
                 out["plain_fp64"] = {"value": round(1e3 / plain_ms, 3), "unit": "solves/s",
                                      "iters": rp_res.iters, "true_rel_residual": plain_rel,
@@ -530,7 +531,7 @@ def run_solve(args, wl, rank, world, local):
                 # so inner tolerances near it cost extra FP32 iterations
                 sweep = []
                 for itol in (1e-1, 1e-2, 1e-3):
-                    if itol == args.inner_tol:
+                    if itol == inner_tol:
                         continue
                     for _ in range(2):
                         dx.zero_()
@@ -611,9 +612,17 @@ def run_batch(args, wl, rank, world, local):
     db = torch.from_numpy(b_all).cuda()
     dx = torch.zeros_like(db)
     stream = torch.cuda.current_stream()
+    mixed = args.precision == "mixed"
+    inner_tol = 1e-2 if args.inner_tol is None else args.inner_tol
+
+    def batch_solve():
+        if mixed:
+            return B.solve_mixed(db, dx, tol, 20000, inner_tol=inner_tol)
+        return B.solve("cg", db, dx, tol, 20000)
+
     for _ in range(args.warmup):
         dx.zero_()
-        status, iters, resid = B.solve("cg", db, dx, tol, 20000)
+        status, iters, resid = batch_solve()
     clocks = ClockSampler(local)
     clocks.start()
     if world > 1:
@@ -624,7 +633,7 @@ def run_batch(args, wl, rank, world, local):
     e0.record(stream)
     for _ in range(args.steps):
         dx.zero_()
-        status, iters, resid = B.solve("cg", db, dx, tol, 20000)
+        status, iters, resid = batch_solve()
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -637,11 +646,29 @@ def run_batch(args, wl, rank, world, local):
     for _ in range(max(1, min(args.steps, 3))):
         db.copy_(hb, non_blocking=True)
         dx.zero_()
-        B.solve("cg", db, dx, tol, 20000)
+        batch_solve()
         hx.copy_(dx, non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / max(1, min(args.steps, 3))
+    # mixed: the same batch in plain FP64, timed the same way
+    fp64_ms, fp64_iters = None, None
+    if mixed:
+        for _ in range(2):
+            dx.zero_()
+            B.solve("cg", db, dx, tol, 20000)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            dx.zero_()
+            _, it64, _ = B.solve("cg", db, dx, tol, 20000)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fp64_ms = e0.elapsed_time(e1) / args.steps
+        fp64_iters = int(np.asarray(it64).sum())
+        dx.zero_()
+        batch_solve()
+        x_all = dx.cpu().numpy()
     # the comparison: a loop of single plain FP64 solves (mlsh_cg_solve per
     # system, its default engine), device time over the whole loop
     loop_ms = None
@@ -678,18 +705,22 @@ def run_batch(args, wl, rank, world, local):
         nnz = int(sum(int(rp[-1]) for rp, _, _ in systems))
         iters = np.asarray(iters)
         # algorithmic bytes of the fused CG iteration, summed over systems
-        bytes_all = float(sum(it * ((int(systems[k][0][-1]) * 12 + (len(bs[k]) + 1) * 4)
-                                    + 13 * len(bs[k]) * 8) for k, it in enumerate(iters)))
+        vb, xb = (4, 4) if mixed else (8, 8)  # value / vector bytes of the iteration
+        bytes_all = float(sum(it * ((int(systems[k][0][-1]) * (vb + 4) + (len(bs[k]) + 1) * 4)
+                                    + 13 * len(bs[k]) * xb) for k, it in enumerate(iters)))
         peak, peak_kind = measured_peak()
         out = {
             "metric": METRIC_BATCH, "value": round(value, 2), "unit": "solves/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 iteration / f64 refresh" if mixed else "f64",
             "data": "synthetic (seeded generators)",
             "config": {"workload": f"{count} variable-coefficient 2D diffusion systems, n "
                                    "log-uniform in [1e3, 1e5] (seed 3), Jacobi-CG to 1e-8 "
-                                   "relative residual, FP64, one launch per cluster-size group",
+                                   "relative residual, " +
+                                   (f"mixed FP32/FP64 (refresh every {inner_tol:g})" if mixed
+                                    else "FP64") + ", one launch per cluster-size group",
                        "systems": count, "rows": rows, "nnz": nnz,
                        "iters_total": int(iters.sum()), "iters_max": int(iters.max()),
                        "all_converged": bool((np.asarray(status) == 0).all()),
@@ -708,8 +739,14 @@ def run_batch(args, wl, rank, world, local):
         if loop_ms is not None:
             out["loop_of_single_solves"] = {
                 "value": round(count / (loop_ms / 1e3), 2), "unit": "solves/s",
-                "speedup_of_batch": round((count / per_step_s) / (count / (loop_ms / 1e3)), 2),
-                "iters_match": bool(np.array_equal(np.asarray(loop_iters), iters))}
+                "speedup_of_batch": round((count / per_step_s) / (count / (loop_ms / 1e3)), 2)}
+            if not mixed:
+                out["loop_of_single_solves"]["iters_match"] = bool(
+                    np.array_equal(np.asarray(loop_iters), iters))
+        if mixed and fp64_ms is not None:
+            out["fp64_batch"] = {"value": round(count / (fp64_ms / 1e3), 2), "unit": "solves/s",
+                                 "iters_total": fp64_iters,
+                                 "speedup_of_mixed": round(fp64_ms / (per_step_s * 1e3), 3)}
         if world == 1 and not args.no_cpu:
             threads = os.cpu_count() or 1
             sec, ns, kind = cpu_reference_batch(systems, bs, tol, max(1, count // 16), threads)
@@ -1069,8 +1106,9 @@ def main():
     ap.add_argument("--rates", default="100,500,2000,5000",
                     help="serve_stream: arrival rates (req/s); the last one is the headline")
     ap.add_argument("--lanes", type=int, default=4, help="serve_stream: worker lanes")
-    ap.add_argument("--inner-tol", type=float, default=1e-4,
-                    help="mixed precision: inner tolerance / FP64 update threshold")
+    ap.add_argument("--inner-tol", type=float, default=None,
+                    help="mixed precision: inner tolerance / FP64 update threshold "
+                         "(default 1e-4 for the single solves, 1e-2 for the batch)")
     ap.add_argument("--eager", action="store_true",
                     help="solver workloads: launch iterations one by one instead of a graph "
                          "(kernel-level profiling)")

@@ -342,6 +342,19 @@ int mlsh_batch_solve(mlsh_handle handle, mlsh_batch batch, int kind, const void 
                      void *d_x, const double *host_tol, const mlsh_solver_opts *opts,
                      int *host_status, int64_t *host_iters, double *host_resid);
 
+/* The batch's Jacobi-CG solves in mixed precision (no reference
+ * counterpart): FP32 matrix values and FP32 iteration vectors inside each
+ * cluster, the solution and the true residual in FP64.  The FP64 solution
+ * and residual are refreshed whenever the iterated residual has fallen by
+ * inner_tol since the last refresh (reliable updates); the stopping test
+ * (host_tol / opts->tol, absolute) is on the true residual.  The batch must
+ * hold FP64 values; its FP32 copy is made on the first call.  host_iters
+ * receives FP32 iterations, host_resid the final true ||b - A x||. */
+int mlsh_batch_cg_solve_mixed(mlsh_handle handle, mlsh_batch batch, const void *d_b,
+                              void *d_x, const double *host_tol,
+                              const mlsh_solver_opts *opts, double inner_tol,
+                              int *host_status, int64_t *host_iters, double *host_resid);
+
 /* ------------------------------------------------------------- serving -- */
 /* A solve server (no reference counterpart): requests of different sizes
  * are submitted from any host thread while others run; a scheduler thread

@@ -115,6 +115,8 @@ SIGNATURES = {
     "mlsh_batch_create": (i32, [vp, i32, vp, vp, vp, vp, i32, C.POINTER(vp)]),
     "mlsh_batch_destroy": (i32, [vp]),
     "mlsh_batch_solve": (i32, [vp, vp, i32, vp, vp, vp, C.POINTER(SolverOpts), vp, vp, vp]),
+    "mlsh_batch_cg_solve_mixed": (i32, [vp, vp, vp, vp, vp, C.POINTER(SolverOpts), f64, vp, vp,
+                                        vp]),
     "mlsh_server_create": (i32, [C.c_size_t, i32, C.POINTER(vp)]),
     "mlsh_server_submit": (i32, [vp, C.POINTER(Request), C.POINTER(i64)]),
     "mlsh_server_poll": (i32, [vp, i64, C.POINTER(RequestResult)]),

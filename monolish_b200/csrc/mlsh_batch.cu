@@ -37,11 +37,12 @@ struct Batch {
   int dtype = MLSH_F64;
   int64_t total_rows = 0;
   std::vector<int64_t> row_off;
-  std::vector<int> order[2];  // per kind: record i solves system order[i]
+  std::vector<int> order[3];  // per kind: record i solves system order[i]
   const int *row_ptr = nullptr;
   const int *col_ind = nullptr;
   const void *val = nullptr;
-  std::vector<BatchGroup> groups[2];  // per kind (CG, BiCGSTAB)
+  std::vector<BatchGroup> groups[3];  // per kind (CG, BiCGSTAB, mixed CG)
+  float *val32 = nullptr;             // FP32 copy of the values (mixed CG)
   ClusterSystem *d_sys = nullptr;     // n_systems records
   ClusterSystem *h_sys = nullptr;     // pinned mirror
   unsigned *d_queue = nullptr;        // one counter per group
@@ -55,20 +56,21 @@ namespace {
 int build_groups(Batch &B, int kind, std::vector<BatchGroup> &groups,
                  std::vector<int> &order) {
   const int n = B.n_systems;
+  const int dt = kind == 2 ? MLSH_F32 : B.dtype;  // mixed CG iterates in FP32
   std::vector<int> rpc(n), cs(n);
   for (int k = 0; k < n; ++k) {
     const int64_t nk = B.row_off[k + 1] - B.row_off[k];
     // one CTA while the system fits one; otherwise the widest slices
-    int r = cluster_rows_for(kind, B.dtype, nk, 0);
+    int r = cluster_rows_for(kind, dt, nk, 0);
     if (r == 0) return MLSH_ERR_INVALID_ARG;
-    int single = cluster_rows_for(kind, B.dtype, nk, (int)std::max<int64_t>(nk, 1));
+    int single = cluster_rows_for(kind, dt, nk, (int)std::max<int64_t>(nk, 1));
     if (single > 0 && nk <= single) {
       r = single;
     } else {
       // largest slice that fits: fewer CTAs per system
       int best = r;
       for (int t = r; t <= 16384; t <<= 1) {
-        const int ok = cluster_rows_for(kind, B.dtype, nk, t);
+        const int ok = cluster_rows_for(kind, dt, nk, t);
         if (ok == t) best = t;
       }
       r = best;
@@ -111,7 +113,14 @@ void free_batch(Batch &B) {
   cudaFreeHost(B.h_sys);
   cudaFree(B.d_queue);
   cudaFree(B.ws);
+  cudaFree(B.val32);
   if (B.done_event) cudaEventDestroy(B.done_event);
+}
+
+__global__ void values_to_f32(const double *v, int64_t n, float *out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (float)v[i];
 }
 
 }  // namespace
@@ -181,12 +190,16 @@ int mlsh_batch_destroy(mlsh_batch bs) {
   return MLSH_SUCCESS;
 }
 
-int mlsh_batch_solve(mlsh_handle hs, mlsh_batch bs, int kind, const void *d_b, void *d_x,
-                     const double *host_tol, const mlsh_solver_opts *opts, int *host_status,
-                     int64_t *host_iters, double *host_resid) {
-  if (!hs || !bs || !opts || (kind != 0 && kind != 1)) return MLSH_ERR_INVALID_ARG;
-  Batch &B = bs->b;
-  Handle &h = hs->h;
+}  // extern "C"
+
+namespace mlsh {
+namespace {
+
+// One batched solve of `kind` (0 CG, 1 BiCGSTAB, 2 mixed CG with refresh
+// factor `delta`).
+int batch_run(Handle &h, Batch &B, int kind, const void *d_b, void *d_x, const double *host_tol,
+              const mlsh_solver_opts *opts, double delta, int *host_status,
+              int64_t *host_iters, double *host_resid) {
   if (B.n_systems == 0) return MLSH_SUCCESS;
   if (!d_b || !d_x) return MLSH_ERR_INVALID_ARG;
   std::vector<BatchGroup> &groups = B.groups[kind];
@@ -196,7 +209,9 @@ int mlsh_batch_solve(mlsh_handle hs, mlsh_batch bs, int kind, const void *d_b, v
     if (st != MLSH_SUCCESS) return st;
   }
   if ((int)order.size() != B.n_systems) return MLSH_ERR_INVALID_ARG;
-  const size_t esz = (size_t)dtype_size(B.dtype);
+  const int dt = kind == 2 ? MLSH_F32 : B.dtype;   // the iteration's type
+  const size_t esz = (size_t)dtype_size(B.dtype);  // b, x, values
+  const size_t isz = (size_t)dtype_size(dt);       // work vectors
   char *ws = static_cast<char *>(B.ws);
   const bool jac = opts->precond == MLSH_PRECOND_JACOBI;
   for (int i = 0; i < B.n_systems; ++i) {
@@ -206,11 +221,16 @@ int mlsh_batch_solve(mlsh_handle hs, mlsh_batch bs, int kind, const void *d_b, v
     const int64_t r0 = B.row_off[k];
     S.rp = B.row_ptr + r0;
     S.ci = B.col_ind;
-    S.val = B.val;
     S.b = static_cast<const char *>(d_b) + r0 * esz;
     S.x = static_cast<char *>(d_x) + r0 * esz;
-    S.dinv = ws + r0 * esz;
-    S.aux = ws + (B.total_rows + r0) * esz;
+    S.dinv = ws + r0 * isz;
+    if (kind == 2) {
+      S.val = B.val32;
+      S.aux = const_cast<void *>(B.val);  // the FP64 values of the true residual
+    } else {
+      S.val = B.val;
+      S.aux = ws + (B.total_rows + r0) * isz;
+    }
     S.n = (int)(B.row_off[k + 1] - r0);
     S.tol = host_tol ? host_tol[k] : opts->tol;
     S.maxiter = opts->maxiter;
@@ -227,12 +247,12 @@ int mlsh_batch_solve(mlsh_handle hs, mlsh_batch bs, int kind, const void *d_b, v
     BatchGroup &g = groups[gi];
     if (!g.stream) MLSH_CUDA_TRY(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     MLSH_CUDA_TRY(cudaStreamWaitEvent(g.stream, B.done_event, 0));
-    int n_clusters = cluster_max_active(kind, B.dtype, jac, g.rpc, g.csize);
+    int n_clusters = cluster_max_active(kind, dt, jac, g.rpc, g.csize);
     if (n_clusters < 1) return MLSH_NOT_IMPL;
     n_clusters = std::min(n_clusters, g.count);
-    const int st = cluster_launch(h, kind, B.dtype, jac, B.d_sys + g.first, g.count,
-                                  B.d_queue + gi, g.rpc, g.csize, n_clusters,
-                                  kClusterBudgetSeconds, g.stream);
+    const int st = cluster_launch(h, kind, dt, jac, B.d_sys + g.first, g.count, B.d_queue + gi,
+                                  g.rpc, g.csize, n_clusters, kClusterBudgetSeconds, g.stream,
+                                  delta);
     if (st != MLSH_SUCCESS) return st;
   }
   for (int gi = 0; gi < n_groups; ++gi) {
@@ -255,6 +275,48 @@ int mlsh_batch_solve(mlsh_handle hs, mlsh_batch bs, int kind, const void *d_b, v
     if (S.status != MLSH_SUCCESS && first_bad == MLSH_SUCCESS) first_bad = S.status;
   }
   return first_bad;
+}
+
+}  // namespace
+}  // namespace mlsh
+
+extern "C" {
+
+int mlsh_batch_solve(mlsh_handle hs, mlsh_batch bs, int kind, const void *d_b, void *d_x,
+                     const double *host_tol, const mlsh_solver_opts *opts, int *host_status,
+                     int64_t *host_iters, double *host_resid) {
+  if (!hs || !bs || !opts || (kind != 0 && kind != 1)) return MLSH_ERR_INVALID_ARG;
+  return batch_run(hs->h, bs->b, kind, d_b, d_x, host_tol, opts, 0.0, host_status, host_iters,
+                   host_resid);
+}
+
+int mlsh_batch_cg_solve_mixed(mlsh_handle hs, mlsh_batch bs, const void *d_b, void *d_x,
+                              const double *host_tol, const mlsh_solver_opts *opts,
+                              double inner_tol, int *host_status, int64_t *host_iters,
+                              double *host_resid) {
+  if (!hs || !bs || !opts || !(inner_tol > 0.0) || !(inner_tol < 1.0))
+    return MLSH_ERR_INVALID_ARG;
+  Batch &B = bs->b;
+  Handle &h = hs->h;
+  if (B.dtype != MLSH_F64) return MLSH_ERR_INVALID_ARG;
+  if (B.n_systems > 0 && !B.val32) {
+    int nnz = 0;
+    MLSH_CUDA_TRY(cudaMemcpy(&nnz, B.row_ptr + B.total_rows, sizeof(int),
+                             cudaMemcpyDeviceToHost));
+    if (cudaMalloc(&B.val32, sizeof(float) * (size_t)std::max(nnz, 1)) != cudaSuccess) {
+      cudaGetLastError();
+      B.val32 = nullptr;
+      return MLSH_ERR_OOM;
+    }
+    if (nnz > 0) {
+      const unsigned g = (unsigned)std::min<int64_t>(((int64_t)nnz + 255) / 256, 148 * 16);
+      values_to_f32<<<g, 256, 0, h.stream>>>(static_cast<const double *>(B.val), nnz,
+                                             B.val32);
+      MLSH_CUDA_TRY(cudaGetLastError());
+    }
+  }
+  return batch_run(h, B, 2, d_b, d_x, host_tol, opts, inner_tol, host_status, host_iters,
+                   host_resid);
 }
 
 }  // extern "C"

@@ -308,6 +308,123 @@ __device__ __forceinline__ SolveOut bicgstab_system(ClusterEnv &E, const Cluster
   return SolveOut{status, it, resid};
 }
 
+// ----------------------------------------------------------- mixed CG --
+// Jacobi-CG with FP32 iteration vectors and FP32 matrix values, the
+// solution and the true residual in FP64: reliable updates (Sleijpen & van
+// der Vorst 1996) as in the kernel engine's mixed BiCGSTAB.  Shared memory
+// (FP32): r, g (= p, gathered), q, y (the correction since the last
+// update).  Whenever the iterated ||r|| has fallen by `delta` since the last
+// true residual (or the iteration has to stop), x += y in FP64 and the true
+// residual b - A x is formed with the FP64 values (S.aux); the iteration
+// then goes on from it with its search direction kept.
+template <bool JAC>
+__device__ __forceinline__ SolveOut cg_mixed_system(ClusterEnv &E, const ClusterSystem &S,
+                                                    unsigned long long budget_ns,
+                                                    double delta) {
+  const int RPC = E.rpc;
+  float *r = reinterpret_cast<float *>(E.dyn);
+  float *g = r + RPC;
+  float *q = g + RPC;
+  float *y = q + RPC;
+  float *const *remote = reinterpret_cast<float *const *>(E.sh.remote_vec);
+  const int rank = (int)E.rank, shift = E.shift, mask = E.mask;
+  const int n = S.n;
+  const int row0 = rank * RPC;
+  const int nloc = max(0, min(RPC, n - row0));
+  const int *rp = S.rp, *ci = S.ci;
+  const float *val = static_cast<const float *>(S.val);
+  const double *val64 = static_cast<const double *>(S.aux);
+  const double *b = static_cast<const double *>(S.b);
+  double *x = static_cast<double *>(S.x);
+  float *dinv = static_cast<float *>(S.dinv);
+  const double tol = S.tol;
+  const long long maxiter = S.maxiter, miniter = S.miniter;
+  const uint64_t t0 = global_timer_ns();
+
+  cluster_jacobi_setup<float>(rp, ci, val, dinv, row0, nloc, JAC);
+  // r = b - A x in FP64 (x through L2: other CTAs of the cluster write it),
+  // kept in FP32; sums (z, r) and ||r64||^2; y = 0
+  auto refresh = [&](double (&s2)[2]) {
+    s2[0] = 0.0;
+    s2[1] = 0.0;
+    MLSH_FOR_OWN_ROWS(i, nloc) {
+      const int row = row0 + i;
+      double acc = 0.0;
+      for (int j = __ldg(rp + row); j < __ldg(rp + row + 1); ++j)
+        acc = __dadd_rn(acc, __dmul_rn(__ldg(val64 + j), __ldcg(x + __ldg(ci + j))));
+      const double r64 = b[row] - acc;
+      const float ri = (float)r64;
+      r[i] = ri;
+      const float zi = JAC ? dinv[row] * ri : ri;
+      s2[0] += (double)zi * (double)ri;
+      s2[1] += r64 * r64;
+      y[i] = 0.0f;
+    }
+    env_sum<2>(E, s2);
+  };
+  double s2[2];
+  E.cl.sync();  // dinv of every CTA
+  refresh(s2);
+  double rz = s2[0];
+  double resid = sqrt(s2[1]);
+  double rel_true = resid;
+  MLSH_FOR_OWN_ROWS(i, nloc) g[i] = JAC ? dinv[row0 + i] * r[i] : r[i];
+  long long it = 0;
+  int status = maxiter <= 0 ? MLSH_SOLVER_MAXITER : kRunning;
+  E.cl.sync();
+
+  while (status == kRunning) {
+    // q = A p, (p, q)
+    double pq[1] = {0.0};
+    MLSH_FOR_OWN_ROWS(i, nloc) {
+      const float qv = cluster_row_dot<float>(rp, ci, val, row0 + i, g, remote, shift, mask, rank);
+      q[i] = qv;
+      pq[0] += (double)g[i] * (double)qv;
+    }
+    env_sum<1>(E, pq);
+    const float alpha = (float)(rz / pq[0]);
+    // y += alpha p; r -= alpha q; (z, r), (r, r); time budget
+    double s3[3] = {0.0, 0.0, 0.0};
+    MLSH_FOR_OWN_ROWS(i, nloc) {
+      const int row = row0 + i;
+      y[i] = alpha * g[i] + y[i];
+      const float ri = -alpha * q[i] + r[i];
+      r[i] = ri;
+      const float zi = JAC ? dinv[row] * ri : ri;
+      s3[0] += (double)zi * (double)ri;
+      s3[1] += (double)ri * (double)ri;
+    }
+    if (rank == 0 && threadIdx.x == 0 && global_timer_ns() - t0 > budget_ns) s3[2] = 1.0;
+    env_sum<3>(E, s3);
+    ++it;
+    double rz_new = s3[0];
+    const double rec = sqrt(s3[1]);
+    const bool timeout = s3[2] > 0.0;
+    if (rec < delta * rel_true || rec < tol || it >= maxiter || isnan(rec) || timeout) {
+      MLSH_FOR_OWN_ROWS(i, nloc) x[row0 + i] += (double)y[i];
+      E.cl.sync();  // every CTA's part of x before anyone gathers it
+      refresh(s2);
+      rz_new = s2[0];
+      resid = sqrt(s2[1]);
+      rel_true = resid;
+      if (resid < tol && miniter <= it) status = MLSH_SUCCESS;
+      else if (isnan(resid)) status = MLSH_SOLVER_RESIDUAL_NAN;
+      else if (it >= maxiter) status = MLSH_SOLVER_MAXITER;
+      else if (timeout) status = MLSH_ERR_TIMEOUT;
+    }
+    if (status != kRunning) break;
+    const float beta = (float)(rz_new / rz);
+    rz = rz_new;
+    MLSH_FOR_OWN_ROWS(i, nloc) {
+      const float zi = JAC ? dinv[row0 + i] * r[i] : r[i];
+      g[i] = zi + beta * g[i];
+    }
+    E.cl.sync();
+  }
+  // every x write precedes the last cluster barrier (inside env_sum)
+  return SolveOut{status, it, resid};
+}
+
 // ------------------------------------------------------------- kernels --
 __device__ __forceinline__ void env_init(ClusterEnv &E, void *gathered) {
   if (threadIdx.x < E.csize) {
@@ -327,7 +444,7 @@ __device__ __forceinline__ unsigned long long queue_next(ClusterEnv &E, unsigned
   return E.sh.sys_idx;
 }
 
-// KIND 0: CG, 1: BiCGSTAB.
+// KIND 0: CG, 1: BiCGSTAB, 2: mixed CG (T = float).
 template <typename T, int KIND, bool JAC>
 __global__ void __launch_bounds__(kClusterThreads, 1) cluster_queue_kernel(const ClusterArgs a) {
   cgs::cluster_group cl = cgs::this_cluster();
@@ -335,14 +452,16 @@ __global__ void __launch_bounds__(kClusterThreads, 1) cluster_queue_kernel(const
   __shared__ ClusterShared sh;
   ClusterEnv E{cl, sh, dyn, cl.num_blocks(), cl.block_rank(), a.rpc_shift, 1 << a.rpc_shift,
                (1 << a.rpc_shift) - 1, 0};
-  T *gathered = reinterpret_cast<T *>(dyn) + (KIND == 0 ? 1 : 5) * E.rpc;
+  T *gathered = reinterpret_cast<T *>(dyn) + (KIND == 1 ? 5 : 1) * E.rpc;
   env_init(E, gathered);
   while (true) {
     const unsigned long long idx = queue_next(E, a.queue);
     if (idx >= (unsigned long long)a.n_systems) break;
     ClusterSystem &S = a.systems[idx];
-    const SolveOut o = KIND == 0 ? cg_system<T>(E, S, JAC, a.budget_ns)
-                                 : bicgstab_system<T>(E, S, JAC, a.budget_ns);
+    SolveOut o;
+    if constexpr (KIND == 0) o = cg_system<T>(E, S, JAC, a.budget_ns);
+    else if constexpr (KIND == 1) o = bicgstab_system<T>(E, S, JAC, a.budget_ns);
+    else o = cg_mixed_system<JAC>(E, S, a.budget_ns, a.delta);
     if (E.rank == 0 && threadIdx.x == 0) {
       S.status = o.status;
       S.iters = o.iters;
@@ -438,6 +557,7 @@ namespace {
 using KernelFn = void (*)(const ClusterArgs);
 
 KernelFn cluster_kernel(int kind, int dtype, bool jac) {
+  if (kind == 2) return jac ? cluster_queue_kernel<float, 2, true> : cluster_queue_kernel<float, 2, false>;
   if (kind == 0) {
     if (dtype == MLSH_F64)
       return jac ? cluster_queue_kernel<double, 0, true> : cluster_queue_kernel<double, 0, false>;
@@ -448,7 +568,7 @@ KernelFn cluster_kernel(int kind, int dtype, bool jac) {
   return jac ? cluster_queue_kernel<float, 1, true> : cluster_queue_kernel<float, 1, false>;
 }
 
-int cluster_nvec(int kind) { return kind == 0 ? 3 : 6; }
+int cluster_nvec(int kind) { return kind == 0 ? 3 : (kind == 1 ? 6 : 4); }
 
 int set_cluster_attributes() {
   static std::once_flag once;
@@ -466,6 +586,7 @@ int set_cluster_attributes() {
     for (int kind = 0; kind < 2; ++kind)
       for (int dt = 0; dt < 2; ++dt)
         for (int j = 0; j < 2; ++j) set(cluster_kernel(kind, dt, j != 0));
+    for (int j = 0; j < 2; ++j) set(cluster_kernel(2, MLSH_F32, j != 0));
     set(cluster_serve_kernel);
   });
   return status;
@@ -504,7 +625,7 @@ int cluster_rows_for(int kind, int dtype, int64_t n, int requested) {
 
 int cluster_launch(const Handle &h, int kind, int dtype, bool jac, ClusterSystem *d_systems,
                    int n_systems, unsigned *d_queue, int rpc, int csize, int n_clusters,
-                   double budget_s, cudaStream_t stream) {
+                   double budget_s, cudaStream_t stream, double delta) {
   (void)h;
   if (set_cluster_attributes() != MLSH_SUCCESS) return MLSH_NOT_IMPL;
   int shift = 0;
@@ -516,6 +637,7 @@ int cluster_launch(const Handle &h, int kind, int dtype, bool jac, ClusterSystem
   a.queue = d_queue;
   a.budget_ns = (unsigned long long)(budget_s * 1e9);
   a.precond = jac ? MLSH_PRECOND_JACOBI : MLSH_PRECOND_NONE;
+  a.delta = delta;
   cudaLaunchAttribute attr[1];
   cudaLaunchConfig_t cfg = cluster_config(
       csize, n_clusters, (size_t)cluster_nvec(kind) * rpc * dtype_size(dtype), stream, attr);

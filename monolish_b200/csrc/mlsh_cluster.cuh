@@ -86,6 +86,7 @@ struct ClusterArgs {
   unsigned long long budget_ns;
   int precond;              // MLSH_PRECOND_*
   ServeRing ring;           // used by the serving kernel only
+  double delta;             // mixed CG: refresh once ||r|| fell by this factor
 };
 
 template <typename T>

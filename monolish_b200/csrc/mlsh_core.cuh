@@ -25,7 +25,9 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
 int plan_diag(const CsrPlan &p, void *out, bool invert, cudaStream_t stream);
 int plan_inv_diag(CsrPlan &p, cudaStream_t stream, const void **out);
 
-// Cluster engine (mlsh_cluster.cu).  kind: 0 = CG, 1 = BiCGSTAB.
+// Cluster engine (mlsh_cluster.cu).  kind: 0 = CG, 1 = BiCGSTAB, 2 = mixed
+// CG (FP32 iteration, FP64 x and true residual; launched with dtype F32,
+// records carrying the FP64 values in `aux`).
 struct ClusterSystem;
 // Rows per CTA for an n-row system (0 if it does not fit 16 CTAs).
 int cluster_rows_for(int kind, int dtype, int64_t n, int requested);
@@ -33,7 +35,7 @@ int cluster_rows_for(int kind, int dtype, int64_t n, int requested);
 // d_queue (zero it first) until n_systems are done.
 int cluster_launch(const Handle &h, int kind, int dtype, bool jac, ClusterSystem *d_systems,
                    int n_systems, unsigned *d_queue, int rpc, int csize, int n_clusters,
-                   double budget_s, cudaStream_t stream);
+                   double budget_s, cudaStream_t stream, double delta = 0.0);
 int cluster_max_active(int kind, int dtype, bool jac, int rpc, int csize);
 struct ServeRing;
 // The serving kernel (FP64, kServeRows rows per CTA) on n_clusters

@@ -334,6 +334,23 @@ class Batch:
             raise _abi.MlshError(st, "batch_solve")
         return status, iters, resid
 
+    def solve_mixed(self, d_b, d_x, tol, maxiter, inner_tol=1e-2, miniter=0,
+                    precond=_abi.PRECOND_JACOBI):
+        """Jacobi-CG on every system, FP32 iterations with FP64 refreshes."""
+        o = _opts(1e-8, maxiter, miniter, precond, True, 0, _abi.ENGINE_CLUSTER, 0)
+        tol_arr = np.ascontiguousarray(np.broadcast_to(np.asarray(tol, np.float64),
+                                                       (self.n_systems,)))
+        status = np.zeros(self.n_systems, np.int32)
+        iters = np.zeros(self.n_systems, np.int64)
+        resid = np.zeros(self.n_systems, np.float64)
+        st = self.lib.mlsh_batch_cg_solve_mixed(
+            self.handle.h, self.b, ptr(d_b), ptr(d_x), tol_arr.ctypes.data_as(C.c_void_p),
+            C.byref(o), float(inner_tol), status.ctypes.data_as(C.c_void_p),
+            iters.ctypes.data_as(C.c_void_p), resid.ctypes.data_as(C.c_void_p))
+        if st < _abi.NOT_IMPL:
+            raise _abi.MlshError(st, "batch_cg_solve_mixed")
+        return status, iters, resid
+
 
 def cg_solve(A: Crs, b, x, tol, maxiter, **kw) -> SolveResult:
     return _solve(A.lib.mlsh_cg_solve, A, b, x, tol, maxiter, **kw)

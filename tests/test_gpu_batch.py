@@ -120,3 +120,43 @@ def test_batch_statuses_per_system(handle, restatement):
     status, iters, resid = B.solve("cg", db, dx, 1e-8, 3)
     assert (status[[0, 2]] == _abi.SOLVER_MAXITER).all() and (iters[[0, 2]] == 3).all()
     B.close()
+
+
+def test_batch_mixed_cg(handle, restatement):
+    """Mixed-precision batch (FP32 iterations, FP64 refreshes every 1e-2):
+    every system reaches the requested true residual, in about as many
+    iterations as the FP64 oracle, and its result does not depend on the
+    batch it is in."""
+    import torch
+    from monolish_b200 import device as D
+    rng = np.random.default_rng(17)
+    sizes = np.exp(rng.uniform(np.log(40), np.log(30000), 40)).round().astype(int)
+    sizes[:3] = [1, 2, 20000]
+    systems = make_systems(sizes, seed=19)
+    bs, tol = [], []
+    for k, (rp, ci, v) in enumerate(systems):
+        b = restatement.spmv(rp, ci, v, W.uniform_mt(len(rp) - 1, -1, 1, 31 + k))
+        bs.append(b)
+        tol.append(1e-8 * np.linalg.norm(b))
+    B = D.Batch(handle, systems)
+    db = torch.from_numpy(np.concatenate(bs)).cuda()
+    dx = torch.zeros_like(db)
+    status, iters, resid = B.solve_mixed(db, dx, np.array(tol), 20000, inner_tol=1e-2)
+    xs = np.split(dx.cpu().numpy(), np.cumsum([len(b) for b in bs])[:-1])
+    for k, (rp, ci, v) in enumerate(systems):
+        assert status[k] == 0, (k, status[k])
+        rel = restatement.true_relres(rp, ci, v, bs[k], xs[k])
+        assert rel < 1e-8 * 1.0000001 and abs(resid[k] - rel * np.linalg.norm(bs[k])) <= \
+            1e-6 * resid[k] + 1e-300
+        st, it, _, _ = restatement.cg(rp, ci, v, bs[k], np.zeros(len(bs[k])), tol[k], 20000)
+        assert iters[k] <= 1.3 * it + 5, (k, iters[k], it)
+    # one system alone: same iterations and bits
+    k = 2
+    B1 = D.Batch(handle, [systems[k]])
+    db1 = torch.from_numpy(bs[k]).cuda()
+    dx1 = torch.zeros_like(db1)
+    s1, i1, r1 = B1.solve_mixed(db1, dx1, tol[k], 20000, inner_tol=1e-2)
+    assert (s1[0], i1[0]) == (status[k], iters[k])
+    assert np.array_equal(dx1.cpu().numpy(), xs[k])
+    B.close()
+    B1.close()
