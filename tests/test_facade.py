@@ -37,7 +37,7 @@ def progs(tmp_path_factory):
         from monolish_b200 import build
         build.build_facade()
     d = tmp_path_factory.mktemp("cpp")
-    return {n: compile_prog(n, str(d)) for n in ("equation_test", "blas_test")}, d
+    return {n: compile_prog(n, str(d)) for n in ("equation_test", "blas_test", "view_test")}, d
 
 
 def test_dropin_programs_compile(progs):
@@ -66,3 +66,10 @@ def test_dropin_equation(progs, cuda):
         r = subprocess.run([exes["equation_test"], f], capture_output=True, text=True,
                            timeout=300)
         assert r.returncode == 0 and "PASS" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_dropin_view1d(progs, cuda):
+    exes, _ = progs
+    r = subprocess.run([exes["view_test"]], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "PASS" in r.stdout, r.stdout + r.stderr
