@@ -55,6 +55,9 @@ extern "C" {
 
 #define MLSH_PRECOND_NONE 0   /* equation::none (src/equation/none.cpp:40-46) */
 #define MLSH_PRECOND_JACOBI 1 /* equation::Jacobi (src/equation/jacobi.cpp:12-61) */
+#define MLSH_PRECOND_SOR 2    /* equation::SOR as preconditioner (src/equation/sor.cpp:12-77) */
+#define MLSH_PRECOND_IC 3     /* equation::IC, IC(0) (src/equation/ic.cpp:12-140) */
+#define MLSH_PRECOND_ILU 4    /* equation::ILU, ILU(0) (src/equation/ilu.cpp:12-140) */
 
 typedef struct mlsh_handle_s *mlsh_handle;
 typedef struct mlsh_csr_plan_s *mlsh_csr_plan;
@@ -309,6 +312,69 @@ int mlsh_bicgstab_solve_mixed(mlsh_handle handle, mlsh_csr_plan plan,
                               const void *d_b, void *d_x,
                               const mlsh_solver_opts *opts, double inner_tol,
                               mlsh_solver_result *result);
+
+/* ------------------------------------------ SOR / IC / ILU (factored) -- */
+/* Preconditioners that need triangular sweeps (the reference's SOR, IC and
+ * ILU; its IC and ILU run only on the GPU, through cuSPARSE csric02 /
+ * csrilu02 and csrsv2).  All work -- the factorization and every sweep --
+ * runs in this library's kernels.  Rows must be sorted by column
+ * (MLSH_ERR_INVALID_CSR otherwise); the matrix must be square.
+ *
+ *   MLSH_PRECOND_SOR  M = 1 / (omega * diag(A)); apply z = M^{-1} r is a
+ *                     forward sweep y_i = (r_i - sum_{j<i} a_ij y_j) M_i then
+ *                     a backward sweep z_i = y_i - (sum_{j>i} a_ij z_j) M_i
+ *                     (src/equation/kernel/sor_kernel.hpp:42-72).  The
+ *                     sweeps read the plan's values at apply time.
+ *   MLSH_PRECOND_IC   IC(0): L with A ~ L L^T on A's lower pattern; apply
+ *                     solves L y = r, L^T z = y.
+ *   MLSH_PRECOND_ILU  ILU(0): A ~ L U on A's pattern, L unit lower; apply
+ *                     solves L y = r, U z = y.
+ * The object refers to the plan, which must outlive it; after the plan's
+ * values change, create it again (the reference builds it in every solve).
+ * Apply and the solves below run on the handle's stream; one object is used
+ * by one stream at a time. */
+typedef struct mlsh_precond_s *mlsh_precond;
+
+/* omega: SOR relaxation (solver::set_omega, default 1.9); ignored for IC /
+ * ILU.  Synchronous. */
+int mlsh_precond_create(mlsh_handle handle, mlsh_csr_plan plan, int kind,
+                        double omega, mlsh_precond *out);
+/* First zero pivot of an IC / ILU factorization, like
+ * cusparseXcsric02_zeroPivot / cusparseXcsrilu02_zeroPivot in
+ * src/equation/kernel/{ic,ilu}_kernel.hpp: *row = the first row without a
+ * stored diagonal (*structural = 1) or whose pivot is zero (ILU: u_ii == 0;
+ * IC: a_ii - sum l_ik^2 <= 0), -1 if there is none.  SOR: always -1. */
+int mlsh_precond_zero_pivot(mlsh_precond pc, int64_t *row, int *structural);
+/* z = M^{-1} r (equation::SOR/IC/ILU::apply_precond); r and z distinct. */
+int mlsh_precond_apply(mlsh_handle handle, mlsh_precond pc, const void *d_r,
+                       void *d_z);
+/* Copies the factor: IC / ILU its values in the plan's pattern (nnz
+ * elements; IC fills the lower triangle with L and keeps A's upper
+ * triangle), SOR the vector M (n elements). */
+int mlsh_precond_factor(mlsh_handle handle, mlsh_precond pc, void *d_out);
+int mlsh_precond_destroy(mlsh_precond pc);
+
+/* CG / BiCGSTAB preconditioned by `pc` (the reference's solvers with
+ * set_create_precond / set_apply_precond bound to equation::SOR, IC or
+ * ILU): the same recurrences, stopping rule and codes as mlsh_cg_solve /
+ * mlsh_bicgstab_solve, with z = M^{-1} r from the sweeps.  opts->precond
+ * and opts->engine are ignored (kernel engine). */
+int mlsh_cg_solve_precond(mlsh_handle handle, mlsh_csr_plan plan, mlsh_precond pc,
+                          const void *d_b, void *d_x, const mlsh_solver_opts *opts,
+                          mlsh_solver_result *result);
+int mlsh_bicgstab_solve_precond(mlsh_handle handle, mlsh_csr_plan plan,
+                                mlsh_precond pc, const void *d_b, void *d_x,
+                                const mlsh_solver_opts *opts,
+                                mlsh_solver_result *result);
+/* The SOR iteration of equation::SOR::solve (src/equation/sor.cpp:92-162):
+ * x += (D/omega + L)^{-1} (b - A x) until ||b - A x|| / ||b|| < opts->tol
+ * (relative, as the reference's SOR checks it) and miniter <= iter.
+ * result->final_resid is the absolute ||b - A x|| of the last check, the
+ * history (if requested) the relative one.  opts->precond must be
+ * MLSH_PRECOND_NONE (the solver's own preconditioner). */
+int mlsh_sor_solve(mlsh_handle handle, mlsh_csr_plan plan, const void *d_b,
+                   void *d_x, double omega, const mlsh_solver_opts *opts,
+                   mlsh_solver_result *result);
 
 /* ------------------------------------------------------ batched solves -- */
 /* Thousands of independent, uneven systems solved together (no reference

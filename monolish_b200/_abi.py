@@ -29,6 +29,9 @@ F64 = 0
 F32 = 1
 PRECOND_NONE = 0
 PRECOND_JACOBI = 1
+PRECOND_SOR = 2
+PRECOND_IC = 3
+PRECOND_ILU = 4
 
 vp = C.c_void_p
 i32 = C.c_int
@@ -112,6 +115,17 @@ SIGNATURES = {
                                   C.POINTER(SolverResult)]),
     "mlsh_bicgstab_solve_mixed": (i32, [vp, vp, vp, vp, C.POINTER(SolverOpts), f64,
                                         C.POINTER(SolverResult)]),
+    "mlsh_precond_create": (i32, [vp, vp, i32, f64, C.POINTER(vp)]),
+    "mlsh_precond_zero_pivot": (i32, [vp, C.POINTER(i64), C.POINTER(i32)]),
+    "mlsh_precond_apply": (i32, [vp, vp, vp, vp]),
+    "mlsh_precond_factor": (i32, [vp, vp, vp]),
+    "mlsh_precond_destroy": (i32, [vp]),
+    "mlsh_cg_solve_precond": (i32, [vp, vp, vp, vp, vp, C.POINTER(SolverOpts),
+                                    C.POINTER(SolverResult)]),
+    "mlsh_bicgstab_solve_precond": (i32, [vp, vp, vp, vp, vp, C.POINTER(SolverOpts),
+                                          C.POINTER(SolverResult)]),
+    "mlsh_sor_solve": (i32, [vp, vp, vp, vp, f64, C.POINTER(SolverOpts),
+                             C.POINTER(SolverResult)]),
     "mlsh_batch_create": (i32, [vp, i32, vp, vp, vp, vp, i32, C.POINTER(vp)]),
     "mlsh_batch_destroy": (i32, [vp]),
     "mlsh_batch_solve": (i32, [vp, vp, i32, vp, vp, vp, C.POINTER(SolverOpts), vp, vp, vp]),

@@ -47,6 +47,12 @@ int cluster_serve_launch(const ServeRing &ring, int csize, int n_clusters, doubl
 void mixed_release(CsrPlan &p);
 void mixed_invalidate(CsrPlan &p);
 
+// A^T of an n_rows x n_cols CRS (rows of A^T sorted by column), the entry
+// permutation into perm_out if given (mlsh_sort.cu).  Synchronous.
+int transpose_build(Handle &h, int n_rows, int n_cols, int nnz, const int *rp, const int *ci,
+                    const void *val, int dtype, int *rp_t, int *ci_t, void *val_t,
+                    unsigned *perm_out);
+
 // The cached transpose of a plan (mlsh_sort.cu).
 void transpose_release(CsrPlan &p);
 void transpose_invalidate(CsrPlan &p);

@@ -148,6 +148,7 @@ struct CsrPlan {
   bool inv_diag_valid = false;
   void *extras = nullptr;         // precision/format variants (mixed solver)
   void *transpose = nullptr;      // cached A^T for the transposed SpMV
+  void *sor = nullptr;            // the SOR solver's sweep (mlsh_krylov.cu)
   // 16-bit column format (FP32 plans made for the mixed solver)
   uint16_t *col16 = nullptr;      // device, nnz: col - tile_base[tile]
   int *tile_base = nullptr;       // device, n_tiles

@@ -23,10 +23,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <new>
 #include <vector>
 
 #include "mlsh_cluster.cuh"
 #include "mlsh_core.cuh"
+#include "mlsh_precond.cuh"
 
 namespace mlsh {
 
@@ -155,6 +157,112 @@ struct CgPBody : NoPrep {  // p = z + b p; stopping test
   __device__ void finish(const double *) {
     st->rz = st->rz_new;
     finish_iteration<T>(st, cond);
+    cond.set(st->done ? 0 : 1);
+  }
+};
+
+// --------------------------------- CG with a sweep preconditioner -------
+// (SOR, IC, ILU: z = M^{-1} r comes from the triangular sweeps, so z is a
+// vector of its own and (z, r) a reduction of its own.)
+template <typename T>
+struct CgInitZBody : NoPrep {  // p = z; sums (z,r), (r,r)
+  const T *r;
+  const T *z;
+  T *p;
+  SolverState *st;
+  CondRef cond;
+  __device__ void operator()(int64_t i, double *acc) const {
+    const T ri = r[i], zi = z[i];
+    p[i] = zi;
+    acc[0] += (double)zi * (double)ri;
+    acc[1] += (double)ri * (double)ri;
+  }
+  __device__ void finish(const double *s) {
+    st->rz = s[0];
+    st->rr = s[1];
+    st->resid = resid_of<T>(s[1]);
+    if (st->maxiter <= 0) {
+      st->status = MLSH_SOLVER_MAXITER;
+      st->done = 1;
+    }
+    cond.set(st->done ? 0 : 1);
+  }
+};
+
+template <typename T>
+struct ZRBody : NoPrep {  // (z, r) of the preconditioned residual
+  const T *z;
+  const T *r;
+  SolverState *st;
+  using elem = T;
+  bool aligned() const { return al16(z) && al16(r); }
+  template <int W>
+  __device__ void step(int64_t i, double *acc) const {
+    const Pack<T, W> zz = ldp<W>(z, i), rr = ldp<W>(r, i);
+#pragma unroll
+    for (int k = 0; k < W; ++k) acc[0] += (double)zz.v[k] * (double)rr.v[k];
+  }
+  __device__ void finish(const double *s) { st->rz_new = s[0]; }
+};
+
+// ------------------------------------------------------------------ SOR --
+// equation::SOR::solve (src/equation/sor.cpp:92-162): per iteration
+// r = b - A x, t = (D/omega + L)^{-1} r, x += t, then the test on
+// ||r|| / ||b||.
+template <typename T>
+struct SorInitBody : NoPrep {  // 1 / ||b||  (sor.cpp:118-119)
+  const T *b;
+  SolverState *st;
+  CondRef cond;
+  __device__ void operator()(int64_t i, double *acc) const {
+    const double v = (double)b[i];
+    acc[0] += v * v;
+  }
+  __device__ void finish(const double *s) {
+    const T nb = (T)resid_of<T>(s[0]);
+    st->scale = (double)(T)(1.0 / (double)nb);
+    st->resid = 0.0;
+    if (st->maxiter <= 0) {
+      st->status = MLSH_SOLVER_MAXITER;
+      st->done = 1;
+    }
+    cond.set(st->done ? 0 : 1);
+  }
+};
+
+template <typename T>
+struct SorXBody : NoPrep {  // x += t; stopping test (sor.cpp:137-157)
+  T *x;
+  const T *t;
+  SolverState *st;
+  CondRef cond;
+  using elem = T;
+  bool aligned() const { return al16(x) && al16(t); }
+  template <int W>
+  __device__ void step(int64_t i, double *) const {
+    const Pack<T, W> tt = ldp<W>(t, i);
+    Pack<T, W> xx = ldp<W>(x, i);
+#pragma unroll
+    for (int k = 0; k < W; ++k) xx.v[k] = tt.v[k] + xx.v[k];
+    stp<W>(x, i, xx);
+  }
+  __device__ void finish(const double *) {
+    const long long it = st->iter + 1;
+    st->iter = it;
+    const T nrm = (T)resid_of<T>(st->rr);
+    const T rel = nrm * (T)st->scale;
+    st->resid = (double)nrm;  // final_resid = get_residual(r), absolute
+    if (st->hist != nullptr && it <= st->hist_cap) st->hist[it - 1] = (double)rel;
+    if ((double)rel < st->tol && st->miniter <= it) {
+      st->status = MLSH_SUCCESS;
+      st->done = 1;
+    } else if (isnan(rel)) {
+      st->status = MLSH_SOLVER_RESIDUAL_NAN;
+      st->done = 1;
+    } else if (it >= st->maxiter) {
+      st->status = MLSH_SOLVER_MAXITER;
+      st->done = 1;
+    }
     cond.set(st->done ? 0 : 1);
   }
 };
@@ -620,7 +728,7 @@ cudaError_t run_body(const Handle &h, int64_t n, const Body &b, const int *done,
   return cudaGetLastError();
 }
 
-enum Kind { kCG = 0, kBiCGSTAB = 1, kMixedBiCGSTAB = 3 };
+enum Kind { kCG = 0, kBiCGSTAB = 1, kMixedBiCGSTAB = 3, kSOR = 4 };
 
 struct SolveCtx {
   Kind kind;
@@ -638,6 +746,8 @@ struct SolveCtx {
   const CsrPlan *plan64 = nullptr;  // the FP64 matrix
   double *r64 = nullptr;            // FP64 residual vector
   CondRef upd_cond = {0, 0};        // graph: the IF node that runs the update
+  // sweep preconditioner (SOR / IC / ILU), or for kSOR the solver's sweep
+  const Precond *pc = nullptr;
 };
 
 template <typename T>
@@ -716,6 +826,99 @@ cudaError_t bi_iter(const SolveCtx &c, cudaStream_t s, CondRef cond) {
   xb.x = static_cast<T *>(c.x); xb.r = r; xb.r0 = r0; xb.phat = phat; xb.shat = shat;
   xb.s = sv; xb.t = t; xb.st = st; xb.cond = cond;
   return run_body<2, true>(*c.h, c.n, xb, done, s);
+}
+
+// ---- CG with a sweep preconditioner: ws = r, p, q, z
+template <typename T>
+cudaError_t cgf_init(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  T *r = wsv<T>(c, 0), *p = wsv<T>(c, 1), *z = wsv<T>(c, 3);
+  cudaError_t e = launch_spmv_t<T, kDotNone, kDotNone>(
+      *c.plan, *c.h, -1.0, static_cast<const T *>(c.x), 1.0,
+      static_cast<const T *>(c.b), r, nullptr, nullptr, nullptr, nullptr, s);
+  if (e != cudaSuccess) return e;
+  e = precond_apply_launch(*c.pc, r, z, nullptr, c.h->err_flag, s);
+  if (e != cudaSuccess) return e;
+  CgInitZBody<T> ib;
+  ib.r = r; ib.z = z; ib.p = p; ib.st = c.h->state; ib.cond = cond;
+  return run_body<2, true>(*c.h, c.n, ib, nullptr, s);
+}
+
+template <typename T>
+cudaError_t cgf_iter(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  T *r = wsv<T>(c, 0), *p = wsv<T>(c, 1), *q = wsv<T>(c, 2), *z = wsv<T>(c, 3);
+  SolverState *st = c.h->state;
+  const int *done = &st->done;
+  cudaError_t e = launch_spmv_t<T, kDotW, kDotNone>(*c.plan, *c.h, 1.0, p, 0.0, nullptr, q,
+                                                    p, nullptr, &st->pq, done, s);
+  if (e != cudaSuccess) return e;
+  CgXRBody<T, false> xb;
+  xb.x = static_cast<T *>(c.x); xb.r = r; xb.p = p; xb.q = q; xb.d = nullptr; xb.st = st;
+  e = run_body<2, true>(*c.h, c.n, xb, done, s);
+  if (e != cudaSuccess) return e;
+  e = precond_apply_launch(*c.pc, r, z, done, c.h->err_flag, s);
+  if (e != cudaSuccess) return e;
+  ZRBody<T> zb;
+  zb.z = z; zb.r = r; zb.st = st;
+  e = run_body<1, true>(*c.h, c.n, zb, done, s);
+  if (e != cudaSuccess) return e;
+  CgPBody<T, false> pb;
+  pb.p = p; pb.r = z; pb.d = nullptr; pb.st = st; pb.cond = cond;
+  return run_body<0, true>(*c.h, c.n, pb, done, s);
+}
+
+// ---- BiCGSTAB with a sweep preconditioner: ws = r, r0, p, v, s, t, phat, shat
+template <typename T>
+cudaError_t bif_iter(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  T *r = wsv<T>(c, 0), *r0 = wsv<T>(c, 1), *p = wsv<T>(c, 2), *v = wsv<T>(c, 3);
+  T *sv = wsv<T>(c, 4), *t = wsv<T>(c, 5), *phat = wsv<T>(c, 6), *shat = wsv<T>(c, 7);
+  SolverState *st = c.h->state;
+  const int *done = &st->done;
+  BiPBody<T, false> pb;
+  pb.r = r; pb.p = p; pb.v = v; pb.phat = p; pb.d = nullptr; pb.st = st;
+  cudaError_t e = run_body<0, false>(*c.h, c.n, pb, done, s);
+  if (e != cudaSuccess) return e;
+  e = precond_apply_launch(*c.pc, p, phat, done, c.h->err_flag, s);
+  if (e != cudaSuccess) return e;
+  e = launch_spmv_t<T, kDotW, kDotNone>(*c.plan, *c.h, 1.0, phat, 0.0, nullptr, v, r0,
+                                        nullptr, &st->vr0, done, s);
+  if (e != cudaSuccess) return e;
+  BiSBody<T, false> sb;
+  sb.r = r; sb.v = v; sb.s = sv; sb.shat = sv; sb.d = nullptr; sb.st = st;
+  e = run_body<0, true>(*c.h, c.n, sb, done, s);
+  if (e != cudaSuccess) return e;
+  e = precond_apply_launch(*c.pc, sv, shat, done, c.h->err_flag, s);
+  if (e != cudaSuccess) return e;
+  e = launch_spmv_t<T, kDotW, kDotSelf>(*c.plan, *c.h, 1.0, shat, 0.0, nullptr, t, sv,
+                                        nullptr, &st->ts, done, s);
+  if (e != cudaSuccess) return e;
+  BiXRBody<T> xb;
+  xb.x = static_cast<T *>(c.x); xb.r = r; xb.r0 = r0; xb.phat = phat; xb.shat = shat;
+  xb.s = sv; xb.t = t; xb.st = st; xb.cond = cond;
+  return run_body<2, true>(*c.h, c.n, xb, done, s);
+}
+
+// ---- SOR: ws = r, t
+template <typename T>
+cudaError_t sor_init(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  SorInitBody<T> ib;
+  ib.b = static_cast<const T *>(c.b); ib.st = c.h->state; ib.cond = cond;
+  return run_body<1, true>(*c.h, c.n, ib, nullptr, s);
+}
+
+template <typename T>
+cudaError_t sor_iter(const SolveCtx &c, cudaStream_t s, CondRef cond) {
+  T *r = wsv<T>(c, 0), *t = wsv<T>(c, 1);
+  SolverState *st = c.h->state;
+  const int *done = &st->done;
+  cudaError_t e = launch_spmv_t<T, kDotSelf, kDotNone>(
+      *c.plan, *c.h, -1.0, static_cast<const T *>(c.x), 1.0, static_cast<const T *>(c.b), r,
+      nullptr, nullptr, &st->rr, done, s);
+  if (e != cudaSuccess) return e;
+  e = sweep_launch(*c.pc, c.pc->fwd, false, r, t, done, c.h->err_flag, s);
+  if (e != cudaSuccess) return e;
+  SorXBody<T> xb;
+  xb.x = static_cast<T *>(c.x); xb.t = t; xb.st = st; xb.cond = cond;
+  return run_body<0, true>(*c.h, c.n, xb, done, s);
 }
 
 // ---- mixed BiCGSTAB: ws (FP32) = r, r0, p, v, s, t, x32.  With Jacobi the
@@ -799,6 +1002,19 @@ void pick_steps(const SolveCtx &c, StepFn *init, StepFn *iter) {
     *iter = mixbi_iter;
     return;
   }
+  if (c.pc != nullptr) {
+    if (c.kind == kSOR) {
+      *init = f64 ? sor_init<double> : sor_init<float>;
+      *iter = f64 ? sor_iter<double> : sor_iter<float>;
+    } else if (c.kind == kCG) {
+      *init = f64 ? cgf_init<double> : cgf_init<float>;
+      *iter = f64 ? cgf_iter<double> : cgf_iter<float>;
+    } else {
+      *init = f64 ? bi_init<double, false> : bi_init<float, false>;
+      *iter = f64 ? bif_iter<double> : bif_iter<float>;
+    }
+    return;
+  }
   if (c.kind == kCG) {
     if (f64) {
       *init = c.jac ? cg_init<double, true> : cg_init<double, false>;
@@ -831,6 +1047,7 @@ struct GraphEntry {
   cudaGraph_t graph;
   cudaGraphExec_t exec;
   unsigned long long last_use;
+  const Precond *pc;
 };
 
 struct GraphCache {
@@ -963,14 +1180,15 @@ int get_graph(const SolveCtx &c, Handle &h, cudaGraphExec_t *ex) {
   ++gc.clock;
   for (auto &e : gc.entries) {
     if (e.kind == c.kind && e.dtype == c.dtype && e.jac == c.jac && e.plan == c.plan &&
-        e.b == c.b && e.x == c.x && e.d == c.d && e.ws == c.ws && e.n == c.n) {
+        e.b == c.b && e.x == c.x && e.d == c.d && e.ws == c.ws && e.n == c.n &&
+        e.pc == c.pc) {
       e.last_use = gc.clock;
       *ex = e.exec;
       return MLSH_SUCCESS;
     }
   }
   GraphEntry ne{c.kind, c.dtype, c.jac, c.plan, c.b, c.x, c.d, c.ws, c.n, nullptr, nullptr,
-                gc.clock};
+                gc.clock, c.pc};
   int st = build_graph(c, h, ne);
   if (st != MLSH_SUCCESS) return st;
   constexpr size_t kMaxEntries = 16;
@@ -1083,7 +1301,8 @@ int cluster_solve_one(Kind kind, Handle &h, CsrPlan &p, const void *b, void *x,
 }
 
 int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, void *x,
-                 const mlsh_solver_opts *opts, mlsh_solver_result *res) {
+                 const mlsh_solver_opts *opts, mlsh_solver_result *res,
+                 const Precond *pc = nullptr) {
   if (!hs || !ps || !opts) return MLSH_ERR_INVALID_ARG;
   Handle &h = hs->h;
   CsrPlan &p = ps->p;
@@ -1091,12 +1310,20 @@ int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, voi
     if (res) res->status = MLSH_SOLVER_SIZE_ERROR;
     return MLSH_SOLVER_SIZE_ERROR;
   }
-  if (opts->precond != MLSH_PRECOND_NONE && opts->precond != MLSH_PRECOND_JACOBI)
+  if (!pc && opts->precond != MLSH_PRECOND_NONE && opts->precond != MLSH_PRECOND_JACOBI)
     return MLSH_ERR_INVALID_ARG;
   const int64_t n = p.n_rows;
+  if (pc && pc->n != n) return MLSH_ERR_INVALID_ARG;
   if (n > 0 && (!b || !x)) return MLSH_ERR_INVALID_ARG;
   mlsh_solver_result local{};
   if (!res) res = &local;
+  if (n == 0 && kind == kSOR) {
+    // ||b|| = 0: the relative residual is 0 * inf = NaN at the first check
+    res->final_resid = 0.0;
+    res->iters = opts->maxiter > 0 ? 1 : 0;
+    res->status = opts->maxiter > 0 ? MLSH_SOLVER_RESIDUAL_NAN : MLSH_SOLVER_MAXITER;
+    return res->status;
+  }
   if (n == 0) {
     // nothing to solve: ||r|| = 0 < tol from the first iteration on, so the
     // loop ends at max(1, miniter) unless maxiter comes first or tol <= 0
@@ -1111,8 +1338,8 @@ int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, voi
     }
     return res->status;
   }
-  if (opts->engine == MLSH_ENGINE_CLUSTER ||
-      (opts->engine == MLSH_ENGINE_AUTO && opts->maxiter <= kClusterMaxIterAuto)) {
+  if (!pc && (opts->engine == MLSH_ENGINE_CLUSTER ||
+              (opts->engine == MLSH_ENGINE_AUTO && opts->maxiter <= kClusterMaxIterAuto))) {
     const int st = cluster_solve_one(kind, h, p, b, x, opts, res);
     if (st != MLSH_NOT_IMPL) return st;
     if (opts->engine == MLSH_ENGINE_CLUSTER) return MLSH_ERR_INVALID_ARG;
@@ -1120,7 +1347,8 @@ int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, voi
   SolveCtx c;
   c.kind = kind;
   c.dtype = p.dtype;
-  c.jac = opts->precond == MLSH_PRECOND_JACOBI;
+  c.jac = !pc && opts->precond == MLSH_PRECOND_JACOBI;
+  c.pc = pc;
   c.plan = &p;
   c.h = &h;
   c.b = b;
@@ -1132,7 +1360,7 @@ int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, voi
     int st = plan_inv_diag(p, h.stream, &c.d);
     if (st != MLSH_SUCCESS) return st;
   }
-  const int nvec = kind == kCG ? 3 : 8;
+  const int nvec = kind == kSOR ? 2 : (kind == kCG ? (pc ? 4 : 3) : 8);
   const size_t esz = (size_t)dtype_size(p.dtype);
   // round each vector up to 256 bytes so every work vector stays aligned
   const int64_t n_al = (int64_t)(((size_t)n * esz + 255) / 256 * 256 / esz);
@@ -1330,13 +1558,63 @@ void release_solver_graphs(Handle &h) {
   h.hist_cap = 0;
 }
 
+void purge_precond_graphs(Handle &h, const Precond *pc) {
+  if (!h.graph_cache || !pc) return;
+  GraphCache &gc = cache_of(h);
+  for (size_t i = 0; i < gc.entries.size();) {
+    if (gc.entries[i].pc == pc) {
+      destroy_entry(gc.entries[i]);
+      gc.entries.erase(gc.entries.begin() + i);
+    } else {
+      ++i;
+    }
+  }
+}
+
+// The SOR solver's sweep (scaling omega / diag(A)) kept with the plan.
+struct SorCache {
+  Precond pc;
+  double omega = 0.0;
+};
+
+void sor_cache_release(CsrPlan &p) {
+  auto *c = static_cast<SorCache *>(p.sor);
+  if (!c) return;
+  if (p.handle) purge_precond_graphs(*p.handle, &c->pc);
+  precond_release(c->pc);
+  delete c;
+  p.sor = nullptr;
+}
+
+int sor_cache_get(Handle &h, CsrPlan &p, double omega, const Precond **out) {
+  auto *c = static_cast<SorCache *>(p.sor);
+  if (c && c->omega == omega) {
+    *out = &c->pc;
+    return MLSH_SUCCESS;
+  }
+  sor_cache_release(p);
+  c = new (std::nothrow) SorCache;
+  if (!c) return MLSH_ERR_OOM;
+  const int st = precond_build(h, p, MLSH_PRECOND_SOR, omega, true, c->pc);
+  if (st != MLSH_SUCCESS) {
+    delete c;
+    return st;
+  }
+  c->omega = omega;
+  p.sor = c;
+  *out = &c->pc;
+  return MLSH_SUCCESS;
+}
+
 void release_plan_extras(CsrPlan &p) {
+  sor_cache_release(p);
   if (p.handle) purge_graphs(*p.handle, &p, nullptr);
   mixed_release(p);
   transpose_release(p);
 }
 
 void invalidate_plan_extras(CsrPlan &p) {
+  sor_cache_release(p);
   if (p.handle) purge_graphs(*p.handle, &p, nullptr);
   mixed_invalidate(p);
   transpose_invalidate(p);
@@ -1372,6 +1650,34 @@ int mlsh_cg_solve(mlsh_handle hs, mlsh_csr_plan ps, const void *b, void *x,
 int mlsh_bicgstab_solve(mlsh_handle hs, mlsh_csr_plan ps, const void *b, void *x,
                         const mlsh_solver_opts *opts, mlsh_solver_result *res) {
   return solve_common(kBiCGSTAB, hs, ps, b, x, opts, res);
+}
+
+int mlsh_cg_solve_precond(mlsh_handle hs, mlsh_csr_plan ps, mlsh_precond pc, const void *b,
+                          void *x, const mlsh_solver_opts *opts, mlsh_solver_result *res) {
+  if (!pc) return MLSH_ERR_INVALID_ARG;
+  return solve_common(kCG, hs, ps, b, x, opts, res, &pc->p);
+}
+
+int mlsh_bicgstab_solve_precond(mlsh_handle hs, mlsh_csr_plan ps, mlsh_precond pc,
+                                const void *b, void *x, const mlsh_solver_opts *opts,
+                                mlsh_solver_result *res) {
+  if (!pc) return MLSH_ERR_INVALID_ARG;
+  return solve_common(kBiCGSTAB, hs, ps, b, x, opts, res, &pc->p);
+}
+
+int mlsh_sor_solve(mlsh_handle hs, mlsh_csr_plan ps, const void *b, void *x, double omega,
+                   const mlsh_solver_opts *opts, mlsh_solver_result *res) {
+  if (!hs || !ps || !opts || !(omega == omega)) return MLSH_ERR_INVALID_ARG;
+  if (opts->precond != MLSH_PRECOND_NONE) return MLSH_ERR_INVALID_ARG;
+  CsrPlan &p = ps->p;
+  if (p.n_rows != p.n_cols) {
+    if (res) res->status = MLSH_SOLVER_SIZE_ERROR;
+    return MLSH_SOLVER_SIZE_ERROR;
+  }
+  const Precond *pc = nullptr;
+  const int st = sor_cache_get(hs->h, p, omega, &pc);
+  if (st != MLSH_SUCCESS) return st;
+  return solve_common(kSOR, hs, ps, b, x, opts, res, pc);
 }
 
 }  // extern "C"

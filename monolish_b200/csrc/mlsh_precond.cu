@@ -1,0 +1,996 @@
+// SOR / IC(0) / ILU(0) on the device: pattern analysis, the two
+// factorizations, the synchronization-free triangular sweeps and the C ABI
+// of the preconditioner object.  The algorithms and the reference each one
+// follows are described in mlsh_precond.cuh.
+//
+// Arithmetic is written with explicitly rounded operations (no fused
+// multiply-add), so that every value is the one a sequential evaluation in
+// the same order produces:
+//   * the forward sweeps accumulate each row in ascending column order, as
+//     src/equation/kernel/sor_kernel.hpp:50-58 does;
+//   * the factorizations apply every update to an entry in the order of the
+//     row-by-row (IKJ) algorithms, and sum the IC inner products in
+//     ascending column order;
+//   * the backward sweeps accumulate a row's entries outside its 32-row
+//     block in ascending order, then those inside it in descending order
+//     (the order in which the block's chain produces them).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "mlsh_core.cuh"
+#include "mlsh_precond.cuh"
+#include "mlsh_ptx.cuh"
+
+namespace mlsh {
+namespace {
+
+constexpr int kSweepThreads = 256;
+constexpr int kSweepWarps = kSweepThreads / 32;
+constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s per wait
+constexpr unsigned kFull = 0xffffffffu;
+
+// ---- explicitly rounded arithmetic
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double sqrt_rn(double a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ float sqrt_rn(float a) { return __fsqrt_rn(a); }
+
+// Waits until *flag == want.  Gives up (recording MLSH_ERR_TIMEOUT) after
+// kWaitNs, or at once once another warp has recorded an error.
+__device__ __noinline__ bool wait_flag(const unsigned *flag, unsigned want, int *err) {
+  if (ld_acquire_gpu(flag) == want) return true;
+  const uint64_t t0 = global_timer_ns();
+  unsigned spins = 0;
+  while (true) {
+    if (ld_acquire_gpu(flag) == want) return true;
+    if ((++spins & 63u) == 0) {
+      if (*(volatile int *)err != 0) return false;
+      if (global_timer_ns() - t0 > kWaitNs) {
+        atomicCAS(err, 0, MLSH_ERR_TIMEOUT);
+        return false;
+      }
+      __nanosleep(64);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pattern analysis: lo_end / up_beg per row, sorted in-range columns, first
+// missing diagonal.
+__global__ void split_rows_kernel(const int *rp, const int *ci, int n, int *lo_end,
+                                  int *up_beg, int *bad, unsigned long long *missing) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int b = rp[i], e = rp[i + 1];
+  int lo = e, up = e, prev = -1;
+  for (int j = b; j < e; ++j) {
+    const int c = ci[j];
+    if (c <= prev || c >= n) atomicExch(bad, 1);
+    prev = c;
+    if (lo == e && c >= i) lo = j;
+    if (up == e && c > i) up = j;
+  }
+  lo_end[i] = lo;
+  up_beg[i] = up;
+  if (up == lo) atomicMin(missing, (unsigned long long)i);
+}
+
+// SOR multipliers: scale_i = 1 / (w * a_ii), w = omega (preconditioner,
+// sor.cpp:29-32) or 1/omega rounded to T (the solver, sor.cpp:112-115).
+template <typename T>
+__global__ void sor_scale_kernel(const T *val, const int *lo_end, const int *up_beg, int n,
+                                 T w, T *scale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int d = lo_end[i];
+  const T aii = up_beg[i] > d ? val[d] : T(0);
+  scale[i] = div_rn(T(1), mul_rn(w, aii));
+}
+
+// ---------------------------------------------------------------------------
+// The sweeps.
+template <typename T>
+struct SweepArgs {
+  const int *rp;
+  const int *ci;
+  const T *val;
+  const int *lo_end;
+  const int *up_beg;
+  const T *scale;
+  const T *rhs;
+  T *out;
+  int n;
+  unsigned nb;
+  unsigned long long *ticket;
+  unsigned *flags;
+  const int *done;
+  int *err;
+  const int *order;
+  const int *dep_off;
+  const int *dep_ids;
+};
+
+template <int MODE, typename T>
+__device__ __forceinline__ T fwd_finish(T acc, T fin) {
+  if constexpr (MODE == kSorFwd) return mul_rn(acc, fin);
+  else if constexpr (MODE == kDiagFwd) return div_rn(acc, fin);
+  else return acc;
+}
+
+// Takes this warp's ticket; false if the warp has no block or the launch
+// is to be skipped.  Every warp with a block takes exactly one ticket, so a
+// launch consumes nb tickets and the epoch is ticket / nb + 1.
+template <typename T>
+__device__ __forceinline__ bool sweep_ticket(const SweepArgs<T> &a, int lane,
+                                             unsigned long long *t) {
+  const unsigned gw = blockIdx.x * kSweepWarps + (threadIdx.x >> 5);
+  if (gw >= a.nb) return false;
+  unsigned long long v = 0;
+  if (lane == 0) v = atomicAdd(a.ticket, 1ull);
+  *t = __shfl_sync(kFull, v, 0);
+  return !(a.done != nullptr && *(volatile const int *)a.done != 0);
+}
+
+__device__ __forceinline__ void publish_block(unsigned *flag, unsigned epoch, int lane) {
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) st_release_gpu(flag, epoch);
+}
+
+// Schedule entries: block id, and a bit marking blocks whose rows depend
+// inside the block only on the adjacent row (row - 1 lower, row + 1 upper).
+constexpr unsigned kScanBit = 0x80000000u;
+constexpr unsigned kBlockMask = 0x7fffffffu;
+
+// x_k = al_k + be_k x_{k-1} (REV: x_{k+1}) over the 32 lanes, as a
+// Kogge-Stone scan of affine maps (log2 32 = 5 shuffle steps instead of a
+// 32-step chain).  A lane with be_k == 0 takes nothing from its neighbour,
+// so a non-finite value there does not leak into it.
+template <bool REV, typename T>
+__device__ __forceinline__ T affine_scan(T al, T be, int lane) {
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const T al2 = REV ? __shfl_down_sync(kFull, al, d) : __shfl_up_sync(kFull, al, d);
+    const T be2 = REV ? __shfl_down_sync(kFull, be, d) : __shfl_up_sync(kFull, be, d);
+    const bool in = REV ? lane + d < 32 : lane >= d;
+    if (in && be != T(0)) {
+      al = al + be * al2;
+      be = be * be2;
+    }
+  }
+  return al;
+}
+
+// Lanes wait, in parallel, for the flags of the block's dependency blocks.
+__device__ __forceinline__ void wait_deps(const int *dep_off, const int *dep_ids,
+                                          const unsigned *flags, unsigned blk, unsigned epoch,
+                                          int *err, int lane) {
+  const int d1 = dep_off[blk + 1];
+  for (int d = dep_off[blk] + lane; d < d1; d += 32) wait_flag(flags + dep_ids[d], epoch, err);
+  __syncwarp();
+}
+
+constexpr int kPre = 4;  // out-of-block entries fetched ahead of the wait
+
+// Lower sweep.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kSweepThreads) sweep_fwd_kernel(SweepArgs<T> a) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long t;
+  if (!sweep_ticket(a, lane, &t)) return;
+  const unsigned epoch = (unsigned)(t / a.nb) + 1u;
+  const unsigned ov = (unsigned)a.order[t % a.nb];
+  const unsigned blk = ov & kBlockMask;
+  const int base = (int)blk * 32;
+  const int row = base + lane;
+  const bool valid = row < a.n;
+  T acc = T(0), fin = T(1);
+  int j = 0, e = 0;
+  if (valid) {
+    j = a.rp[row];
+    e = a.lo_end[row];
+    acc = a.rhs[row];
+    if constexpr (MODE == kSorFwd) fin = a.scale[row];
+    if constexpr (MODE == kDiagFwd) fin = a.up_beg[row] > e ? a.val[e] : T(0);
+  }
+  // the row's first entries, fetched while the dependencies are awaited
+  int pc[kPre];
+  T pv[kPre];
+#pragma unroll
+  for (int u = 0; u < kPre; ++u) {
+    pc[u] = j + u < e ? a.ci[j + u] : 0x7fffffff;
+    pv[u] = j + u < e ? a.val[j + u] : T(0);
+  }
+  wait_deps(a.dep_off, a.dep_ids, a.flags, blk, epoch, a.err, lane);
+  // entries left of the block (a prefix of the row), ascending
+  T xs[kPre];
+#pragma unroll
+  for (int u = 0; u < kPre; ++u) xs[u] = pc[u] < base ? __ldcg(a.out + pc[u]) : T(0);
+#pragma unroll
+  for (int u = 0; u < kPre; ++u)
+    if (pc[u] < base) {
+      acc = sub_rn(acc, mul_rn(pv[u], xs[u]));
+      ++j;
+    }
+  if (pc[kPre - 1] < base) {
+    for (; j < e; ++j) {
+      const int c = a.ci[j];
+      if (c >= base) break;
+      acc = sub_rn(acc, mul_rn(a.val[j], __ldcg(a.out + c)));
+    }
+  }
+  T xv = T(0);
+  if (ov & kScanBit) {
+    // the block's only in-block dependencies are row - 1 -> row: the
+    // recurrence x_k = al_k + be_k x_{k-1} as a 5-step affine scan
+    const T a1 = (j < e) ? a.val[j] : T(0);
+    T al, be;
+    if constexpr (MODE == kSorFwd) {
+      al = acc * fin;
+      be = -(a1 * fin);
+    } else if constexpr (MODE == kDiagFwd) {
+      al = acc / fin;
+      be = -(a1 / fin);
+    } else {
+      al = acc;
+      be = -a1;
+    }
+    xv = affine_scan<false>(al, be, lane);
+    if (valid) a.out[row] = xv;
+    publish_block(a.flags + blk, epoch, lane);
+    return;
+  }
+  // entries inside the block, ascending: a 32-step chain; the next two are
+  // kept in registers so the chain carries no memory latency
+  int c0 = 64, c1 = 64;
+  T v0 = T(0), v1 = T(0);
+  if (j < e) {
+    c0 = a.ci[j] - base;
+    v0 = a.val[j];
+  }
+  if (j + 1 < e) {
+    c1 = a.ci[j + 1] - base;
+    v1 = a.val[j + 1];
+  }
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    if (lane == k) xv = fwd_finish<MODE>(acc, fin);
+    const T xk = __shfl_sync(kFull, xv, k);
+    if (c0 == k) {
+      acc = sub_rn(acc, mul_rn(v0, xk));
+      c0 = c1;
+      v0 = v1;
+      ++j;
+      if (j + 1 < e) {
+        c1 = a.ci[j + 1] - base;
+        v1 = a.val[j + 1];
+      } else {
+        c1 = 64;
+      }
+    }
+  }
+  if (valid) a.out[row] = xv;
+  publish_block(a.flags + blk, epoch, lane);
+}
+
+// Upper sweep.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kSweepThreads) sweep_bwd_kernel(SweepArgs<T> a) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long t;
+  if (!sweep_ticket(a, lane, &t)) return;
+  const unsigned epoch = (unsigned)(t / a.nb) + 1u;
+  const unsigned ov = (unsigned)a.order[t % a.nb];
+  const unsigned blk = ov & kBlockMask;
+  const int base = (int)blk * 32;
+  const int row = base + lane;
+  const bool valid = row < a.n;
+  // SOR accumulates in double ("auto tmp = 0.0", sor_kernel.hpp:61-66)
+  T acc = T(0), fin = T(1), rh = T(0);
+  double sacc = 0.0;
+  int jb = 0, e = 0, split = 0;
+  if (valid) {
+    jb = a.up_beg[row];
+    e = a.rp[row + 1];
+    rh = a.rhs[row];
+    if constexpr (MODE == kSorBwd) {
+      fin = a.scale[row];
+    } else {
+      acc = rh;
+      const int d = a.lo_end[row];
+      fin = jb > d ? a.val[d] : T(0);
+    }
+    split = jb;
+    while (split < e && a.ci[split] < base + 32) ++split;
+  }
+  int pc[kPre];
+  T pv[kPre];
+#pragma unroll
+  for (int u = 0; u < kPre; ++u) {
+    pc[u] = split + u < e ? a.ci[split + u] : -1;
+    pv[u] = split + u < e ? a.val[split + u] : T(0);
+  }
+  wait_deps(a.dep_off, a.dep_ids, a.flags, blk, epoch, a.err, lane);
+  // entries right of the block (the row's suffix from split), ascending
+  T xs[kPre];
+#pragma unroll
+  for (int u = 0; u < kPre; ++u) xs[u] = pc[u] >= 0 ? __ldcg(a.out + pc[u]) : T(0);
+#pragma unroll
+  for (int u = 0; u < kPre; ++u)
+    if (pc[u] >= 0) {
+      const T prod = mul_rn(pv[u], xs[u]);
+      if constexpr (MODE == kSorBwd) sacc = __dadd_rn(sacc, (double)prod);
+      else acc = sub_rn(acc, prod);
+    }
+  for (int j = split + kPre; j < e; ++j) {
+    const T prod = mul_rn(a.val[j], __ldcg(a.out + a.ci[j]));
+    if constexpr (MODE == kSorBwd) sacc = __dadd_rn(sacc, (double)prod);
+    else acc = sub_rn(acc, prod);
+  }
+  if (ov & kScanBit) {
+    // only row + 1 -> row inside the block: z_k = al_k + be_k z_{k+1}
+    const T a1 = (split > jb) ? a.val[jb] : T(0);
+    T xv;
+    if constexpr (MODE == kSorBwd) {
+      const double al = (double)rh - sacc * (double)fin;
+      const double be = -((double)a1 * (double)fin);
+      xv = (T)affine_scan<true>(al, be, lane);
+    } else {
+      xv = affine_scan<true>(acc / fin, -(a1 / fin), lane);
+    }
+    if (valid) a.out[row] = xv;
+    publish_block(a.flags + blk, epoch, lane);
+    return;
+  }
+  // entries inside the block, consumed from the highest column down
+  int q = split - 1;
+  int c0 = 64, c1 = 64;
+  T v0 = T(0), v1 = T(0);
+  if (q >= jb) {
+    c0 = a.ci[q] - base;
+    v0 = a.val[q];
+  }
+  if (q - 1 >= jb) {
+    c1 = a.ci[q - 1] - base;
+    v1 = a.val[q - 1];
+  }
+  T xv = T(0);
+#pragma unroll
+  for (int k = 31; k >= 0; --k) {
+    if (lane == k) {
+      if constexpr (MODE == kSorBwd)
+        xv = (T)__dsub_rn((double)rh, __dmul_rn(sacc, (double)fin));
+      else
+        xv = div_rn(acc, fin);
+    }
+    const T xk = __shfl_sync(kFull, xv, k);
+    if (c0 == k) {
+      const T prod = mul_rn(v0, xk);
+      if constexpr (MODE == kSorBwd) sacc = __dadd_rn(sacc, (double)prod);
+      else acc = sub_rn(acc, prod);
+      c0 = c1;
+      v0 = v1;
+      --q;
+      if (q - 1 >= jb) {
+        c1 = a.ci[q - 1] - base;
+        v1 = a.val[q - 1];
+      } else {
+        c1 = 64;
+      }
+    }
+  }
+  if (valid) a.out[row] = xv;
+  publish_block(a.flags + blk, epoch, lane);
+}
+
+// ---------------------------------------------------------------------------
+// Schedules: each block's dependency blocks, counted (FILL = false) or
+// written (FILL = true) in ascending order without repeats.  Lower: the
+// blocks of the columns < base its rows reference; upper: those >= base+32.
+template <bool UPPER, bool FILL>
+__global__ void __launch_bounds__(kSweepThreads)
+    block_deps_kernel(const int *rp, const int *ci, const int *lo_end, const int *up_beg, int n,
+                      unsigned nb, int *cnt, const int *off, int *ids) {
+  const int lane = threadIdx.x & 31;
+  const unsigned blk = blockIdx.x * kSweepWarps + (threadIdx.x >> 5);
+  if (blk >= nb) return;
+  const int base = (int)blk * 32;
+  const int row = base + lane;
+  int j = 0, je = 0;
+  if (row < n) {
+    if (UPPER) {
+      je = rp[row + 1];
+      j = up_beg[row];
+      while (j < je && ci[j] < base + 32) ++j;
+    } else {
+      j = rp[row];
+      je = lo_end[row];
+      int k = j;
+      while (k < je && ci[k] < base) ++k;
+      je = k;
+    }
+  }
+  // scan-eligible: each row's in-block dependencies are at most the
+  // adjacent row
+  bool adj = true;
+  if (!FILL && row < n) {
+    if (UPPER) {
+      const int b0 = up_beg[row];
+      const int nin = j - b0;  // entries in (row, base + 32)
+      adj = nin == 0 || (nin == 1 && ci[b0] == row + 1);
+    } else {
+      const int le = lo_end[row];
+      const int nin = le - je;  // entries in [base, row)
+      adj = nin == 0 || (nin == 1 && ci[je] == row - 1);
+    }
+  }
+  const bool scan = __all_sync(kFull, adj);
+  constexpr int kNone = 0x7fffffff;
+  int cur = j < je ? (ci[j] >> 5) : kNone;
+  int count = 0;
+  const int o = FILL ? off[blk] : 0;
+  while (true) {
+    const int m = __reduce_min_sync(kFull, cur);
+    if (m == kNone) break;
+    if (FILL && lane == 0) ids[o + count] = m;
+    ++count;
+    if (cur == m) {
+      while (j < je && (ci[j] >> 5) == m) ++j;
+      cur = j < je ? (ci[j] >> 5) : kNone;
+    }
+  }
+  if (!FILL && lane == 0) cnt[blk] = count | (scan ? (1 << 30) : 0);
+}
+
+// ---------------------------------------------------------------------------
+// Factorizations: one warp per row, rows handed out by a ticket in
+// ascending order, a ready flag per row (1 once the row is final).
+template <typename T>
+struct FactorArgs {
+  const int *rp;
+  const int *ci;
+  const int *lo_end;
+  const int *up_beg;
+  T *f;  // A's values on entry, the factor on exit
+  int n;
+  unsigned long long *ticket;
+  unsigned *rowflag;
+  int *err;
+  unsigned long long *pivot;  // first zero pivot (min row), ~0 if none
+  const int *order;           // blocks of 32 rows in level order
+  unsigned nb;
+};
+
+// Waits until row k is final; afterwards every lane may read it.
+__device__ __forceinline__ void wait_row(const unsigned *rowflag, int k, int *err, int lane) {
+  if (lane == 0) wait_flag(rowflag + k, 1u, err);
+  __syncwarp();
+  (void)ld_acquire_gpu(rowflag + k);
+}
+
+// First position in ci[lo, hi) whose column is >= c.
+__device__ __forceinline__ int lower_bound_col(const int *ci, int lo, int hi, int c) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ci[mid] < c) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Row of this warp: tickets walk the blocks in level order and the rows of
+// a block in ascending order, so every row a row depends on has a smaller
+// ticket.  -1: no row (past the grid or past the last row).
+template <typename T>
+__device__ __forceinline__ int factor_ticket(const FactorArgs<T> &a, int lane) {
+  const unsigned gw = blockIdx.x * kSweepWarps + (threadIdx.x >> 5);
+  if (gw >= a.nb * 32u) return -1;
+  unsigned long long v = 0;
+  if (lane == 0) v = atomicAdd(a.ticket, 1ull);
+  const unsigned long long t = __shfl_sync(kFull, v, 0);
+  const int row = (int)((unsigned)a.order[(unsigned)(t >> 5)] & kBlockMask) * 32 + (int)(t & 31ull);
+  return row < a.n ? row : -1;
+}
+
+// ILU(0), row by row (the IKJ form; Saad, Iterative Methods for Sparse
+// Linear Systems, 2nd ed., Algorithm 10.4):
+//   for each k < i with a_ik stored, ascending:
+//     a_ik = a_ik / a_kk
+//     a_ij = a_ij - a_ik * a_kj   for every stored a_ij, j > k, with a_kj stored
+template <typename T>
+__global__ void __launch_bounds__(kSweepThreads) ilu0_kernel(FactorArgs<T> a) {
+  const int lane = threadIdx.x & 31;
+  const int row = factor_ticket(a, lane);
+  if (row < 0) return;
+  const int rb = a.rp[row], re = a.rp[row + 1], le = a.lo_end[row];
+  T *f = a.f;
+  for (int q = rb; q < le; ++q) {
+    const int k = a.ci[q];
+    wait_row(a.rowflag, k, a.err, lane);
+    const int kd = a.lo_end[k], kb = a.up_beg[k], ke = a.rp[k + 1];
+    const T ukk = kb > kd ? __ldcg(f + kd) : T(0);
+    const T l = div_rn(__ldcg(f + q), ukk);
+    __syncwarp();
+    if (lane == 0) f[q] = l;
+    for (int p = q + 1 + lane; p < re; p += 32) {
+      const int c = a.ci[p];
+      const int pos = lower_bound_col(a.ci, kb, ke, c);
+      if (pos < ke && a.ci[pos] == c) f[p] = sub_rn(__ldcg(f + p), mul_rn(l, __ldcg(f + pos)));
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    const bool has = a.up_beg[row] > le;
+    if (!has || __ldcg(f + le) == T(0)) atomicMin(a.pivot, (unsigned long long)row);
+  }
+  publish_block(a.rowflag + row, 1u, lane);
+}
+
+// IC(0), row by row on the lower triangle (the row-oriented Cholesky
+// recurrence restricted to A's pattern):
+//   l_ik = (a_ik - sum_{m<k} l_im l_km) / l_kk   for stored a_ik, k < i
+//   l_ii = sqrt(a_ii - sum_{m<i} l_im^2)
+// each sum over the stored positions of both rows, ascending in m.
+template <typename T>
+__global__ void __launch_bounds__(kSweepThreads) ic0_kernel(FactorArgs<T> a) {
+  const int lane = threadIdx.x & 31;
+  const int row = factor_ticket(a, lane);
+  if (row < 0) return;
+  const int rb = a.rp[row], le = a.lo_end[row];
+  const bool has = a.up_beg[row] > le;
+  T *f = a.f;
+  for (int q = rb; q < le; ++q) {
+    const int k = a.ci[q];
+    wait_row(a.rowflag, k, a.err, lane);
+    const int kb = a.rp[k], kd = a.lo_end[k];
+    const bool kh = a.up_beg[k] > kd;
+    T s = __ldcg(f + q);
+    for (int c0 = rb; c0 < q; c0 += 32) {
+      const int p = c0 + lane;
+      T prod = T(0);
+      bool found = false;
+      if (p < q) {
+        const int m = a.ci[p];
+        const int pos = lower_bound_col(a.ci, kb, kd, m);
+        if (pos < kd && a.ci[pos] == m) {
+          prod = mul_rn(__ldcg(f + p), __ldcg(f + pos));
+          found = true;
+        }
+      }
+      const unsigned fm = __ballot_sync(kFull, found);
+#pragma unroll 4
+      for (int u = 0; u < 32; ++u) {
+        const T pu = __shfl_sync(kFull, prod, u);
+        if ((fm >> u) & 1u) s = sub_rn(s, pu);
+      }
+    }
+    const T lkk = kh ? __ldcg(f + kd) : T(0);
+    const T l = div_rn(s, lkk);
+    __syncwarp();
+    if (lane == 0) f[q] = l;
+    __syncwarp();
+  }
+  T d = has ? __ldcg(f + le) : T(0);
+  for (int c0 = rb; c0 < le; c0 += 32) {
+    const int p = c0 + lane;
+    T fp = T(0);
+    if (p < le) fp = __ldcg(f + p);
+    const T prod = mul_rn(fp, fp);
+    const int cnt = min(32, le - c0);
+    for (int u = 0; u < cnt; ++u) d = sub_rn(d, __shfl_sync(kFull, prod, u));
+  }
+  const T lii = sqrt_rn(d);
+  __syncwarp();
+  if (lane == 0) {
+    if (!(d > T(0))) atomicMin(a.pivot, (unsigned long long)row);
+    if (has) f[le] = lii;
+  }
+  publish_block(a.rowflag + row, 1u, lane);
+}
+
+int grid_of(long long n, int threads) { return (int)std::max<long long>(1, (n + threads - 1) / threads); }
+
+template <typename T>
+cudaError_t sweep_launch_t(const Precond &pc, const Sweep &sw, bool backward, const void *rhs,
+                           void *out, const int *done, int *err, cudaStream_t s) {
+  SweepArgs<T> a;
+  a.rp = sw.rp;
+  a.ci = sw.ci;
+  a.val = static_cast<const T *>(sw.val);
+  a.lo_end = sw.lo_end;
+  a.up_beg = sw.up_beg;
+  a.scale = static_cast<const T *>(sw.scale);
+  a.rhs = static_cast<const T *>(rhs);
+  a.out = static_cast<T *>(out);
+  a.n = pc.n;
+  a.nb = pc.nb;
+  a.ticket = pc.ticket;
+  a.flags = pc.flags;
+  a.done = done;
+  a.err = err;
+  a.order = sw.order;
+  a.dep_off = sw.dep_off;
+  a.dep_ids = sw.dep_ids;
+  const int g = grid_of(pc.nb, kSweepWarps);
+  switch (sw.mode) {
+    case kSorFwd: sweep_fwd_kernel<T, kSorFwd><<<g, kSweepThreads, 0, s>>>(a); break;
+    case kUnitFwd: sweep_fwd_kernel<T, kUnitFwd><<<g, kSweepThreads, 0, s>>>(a); break;
+    case kDiagFwd: sweep_fwd_kernel<T, kDiagFwd><<<g, kSweepThreads, 0, s>>>(a); break;
+    case kSorBwd: sweep_bwd_kernel<T, kSorBwd><<<g, kSweepThreads, 0, s>>>(a); break;
+    default: sweep_bwd_kernel<T, kDiagBwd><<<g, kSweepThreads, 0, s>>>(a); break;
+  }
+  (void)backward;
+  return cudaGetLastError();
+}
+
+template <typename T>
+int factor_run(Handle &h, Precond &pc, const int *rp, const int *ci) {
+  cudaStream_t s = h.stream;
+  unsigned *rowflag = nullptr;
+  unsigned long long *scratch = nullptr;  // [ticket, pivot]
+  MLSH_CUDA_TRY(pool_alloc(&rowflag, sizeof(unsigned) * (size_t)std::max(pc.n, 1), s));
+  MLSH_CUDA_TRY(pool_alloc(&scratch, 2 * sizeof(unsigned long long), s));
+  MLSH_CUDA_TRY(cudaMemsetAsync(rowflag, 0, sizeof(unsigned) * (size_t)pc.n, s));
+  MLSH_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), s));
+  MLSH_CUDA_TRY(cudaMemsetAsync(scratch + 1, 0xff, sizeof(unsigned long long), s));
+  MLSH_CUDA_TRY(cudaMemsetAsync(h.err_flag, 0, sizeof(int), s));
+  FactorArgs<T> a;
+  a.rp = rp;
+  a.ci = ci;
+  a.lo_end = pc.lo_end;
+  a.up_beg = pc.up_beg;
+  a.f = static_cast<T *>(pc.fval);
+  a.n = pc.n;
+  a.ticket = scratch;
+  a.rowflag = rowflag;
+  a.err = h.err_flag;
+  a.pivot = scratch + 1;
+  a.order = pc.sfwd.order;
+  a.nb = pc.nb;
+  const int g = grid_of((long long)pc.nb * 32, kSweepWarps);
+  if (pc.kind == MLSH_PRECOND_IC) ic0_kernel<T><<<g, kSweepThreads, 0, s>>>(a);
+  else ilu0_kernel<T><<<g, kSweepThreads, 0, s>>>(a);
+  MLSH_CUDA_TRY(cudaGetLastError());
+  unsigned long long piv = 0;
+  int err = 0;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(&piv, scratch + 1, sizeof(piv), cudaMemcpyDeviceToHost, s));
+  MLSH_CUDA_TRY(cudaMemcpyAsync(&err, h.err_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(s));
+  pool_free(rowflag, s);
+  pool_free(scratch, s);
+  if (err != 0) return err;
+  if (pc.pivot < 0 && piv != ~0ull) pc.pivot = (long long)piv;
+  return MLSH_SUCCESS;
+}
+
+}  // namespace
+
+cudaError_t sweep_launch(const Precond &pc, const Sweep &sw, bool backward, const void *rhs,
+                         void *out, const int *done, int *err, cudaStream_t s) {
+  if (pc.n == 0) return cudaSuccess;
+  if (pc.dtype == MLSH_F64) return sweep_launch_t<double>(pc, sw, backward, rhs, out, done, err, s);
+  return sweep_launch_t<float>(pc, sw, backward, rhs, out, done, err, s);
+}
+
+cudaError_t precond_apply_launch(const Precond &pc, const void *r, void *z, const int *done,
+                                 int *err, cudaStream_t s) {
+  cudaError_t e = sweep_launch(pc, pc.fwd, false, r, pc.tmp, done, err, s);
+  if (e != cudaSuccess) return e;
+  return sweep_launch(pc, pc.bwd, true, pc.tmp, z, done, err, s);
+}
+
+void precond_release(Precond &pc) {
+  cudaStream_t s = pc.handle ? pc.handle->stream : nullptr;
+  void *bufs[] = {pc.lo_end,        pc.up_beg,        pc.fval,          pc.rp_t,
+                  pc.ci_t,          pc.val_t,         pc.lo_t,          pc.up_t,
+                  pc.scale,         pc.tmp,           pc.ticket,        pc.flags,
+                  pc.sfwd.order,    pc.sfwd.dep_off,  pc.sfwd.dep_ids,  pc.sbwd.order,
+                  pc.sbwd.dep_off,  pc.sbwd.dep_ids};
+  for (void *b : bufs) pool_free(b, s);
+  pc.sfwd = Schedule{};
+  pc.sbwd = Schedule{};
+  pc.lo_end = pc.up_beg = pc.rp_t = pc.ci_t = pc.lo_t = pc.up_t = nullptr;
+  pc.fval = pc.val_t = pc.scale = pc.tmp = nullptr;
+  pc.ticket = nullptr;
+  pc.flags = nullptr;
+}
+
+namespace {
+
+// lo_end / up_beg of a pattern; MLSH_ERR_INVALID_CSR if a row is not
+// sorted; *missing = first row without a stored diagonal (or ~0).
+int split_rows(Handle &h, const int *rp, const int *ci, int n, int *lo_end, int *up_beg,
+               unsigned long long *missing) {
+  cudaStream_t s = h.stream;
+  struct Flags {
+    unsigned long long missing;
+    int bad;
+    int pad;
+  };
+  Flags *d = nullptr;
+  MLSH_CUDA_TRY(pool_alloc(&d, sizeof(Flags), s));
+  MLSH_CUDA_TRY(cudaMemsetAsync(d, 0xff, sizeof(unsigned long long), s));
+  MLSH_CUDA_TRY(cudaMemsetAsync(&d->bad, 0, 2 * sizeof(int), s));
+  split_rows_kernel<<<grid_of(n, 256), 256, 0, s>>>(rp, ci, n, lo_end, up_beg, &d->bad,
+                                                    &d->missing);
+  MLSH_CUDA_TRY(cudaGetLastError());
+  Flags hf;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(&hf, d, sizeof(Flags), cudaMemcpyDeviceToHost, s));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(s));
+  pool_free(d, s);
+  if (hf.bad) return MLSH_ERR_INVALID_CSR;
+  *missing = hf.missing;
+  return MLSH_SUCCESS;
+}
+
+// The level schedule of one sweep direction: dependency blocks per block
+// on the device, levels and the level order computed on the host (one pass
+// over the block DAG in dependency order).
+int build_schedule(Handle &h, const int *rp, const int *ci, const int *lo, const int *up, int n,
+                   unsigned nb, bool upper, Schedule &sc) {
+  cudaStream_t s = h.stream;
+  if (nb == 0) return MLSH_SUCCESS;
+  const int g = grid_of(nb, kSweepWarps);
+  MLSH_CUDA_TRY(pool_alloc(&sc.dep_off, sizeof(int) * ((size_t)nb + 1), s));
+  MLSH_CUDA_TRY(pool_alloc(&sc.order, sizeof(int) * (size_t)nb, s));
+  int *cnt = sc.order;  // the counts pass borrows the order array
+  if (upper)
+    block_deps_kernel<true, false><<<g, kSweepThreads, 0, s>>>(rp, ci, lo, up, n, nb, cnt,
+                                                                nullptr, nullptr);
+  else
+    block_deps_kernel<false, false><<<g, kSweepThreads, 0, s>>>(rp, ci, lo, up, n, nb, cnt,
+                                                                 nullptr, nullptr);
+  MLSH_CUDA_TRY(cudaGetLastError());
+  std::vector<int> hc(nb), off((size_t)nb + 1, 0);
+  MLSH_CUDA_TRY(cudaMemcpyAsync(hc.data(), cnt, sizeof(int) * (size_t)nb,
+                                cudaMemcpyDeviceToHost, s));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(s));
+  long long total = 0;
+  std::vector<char> scan(nb);
+  for (unsigned b = 0; b < nb; ++b) {
+    scan[b] = (hc[b] >> 30) & 1;
+    hc[b] &= (1 << 30) - 1;
+    off[b] = (int)total;
+    total += hc[b];
+  }
+  off[nb] = (int)total;
+  sc.deps = total;
+  MLSH_CUDA_TRY(pool_alloc(&sc.dep_ids, sizeof(int) * (size_t)std::max(total, 1ll), s));
+  MLSH_CUDA_TRY(cudaMemcpyAsync(sc.dep_off, off.data(), sizeof(int) * ((size_t)nb + 1),
+                                cudaMemcpyHostToDevice, s));
+  if (upper)
+    block_deps_kernel<true, true><<<g, kSweepThreads, 0, s>>>(rp, ci, lo, up, n, nb, nullptr,
+                                                               sc.dep_off, sc.dep_ids);
+  else
+    block_deps_kernel<false, true><<<g, kSweepThreads, 0, s>>>(rp, ci, lo, up, n, nb, nullptr,
+                                                                sc.dep_off, sc.dep_ids);
+  MLSH_CUDA_TRY(cudaGetLastError());
+  std::vector<int> ids((size_t)std::max(total, 1ll));
+  MLSH_CUDA_TRY(cudaMemcpyAsync(ids.data(), sc.dep_ids, sizeof(int) * (size_t)total,
+                                cudaMemcpyDeviceToHost, s));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(s));
+  // level = 1 + the highest level among the dependencies (0 without any)
+  std::vector<int> lvl(nb, 0);
+  int levels = 0;
+  for (unsigned k = 0; k < nb; ++k) {
+    const unsigned b = upper ? nb - 1 - k : k;
+    int m = -1;
+    for (int d = off[b]; d < off[b + 1]; ++d) m = std::max(m, lvl[(size_t)ids[d]]);
+    lvl[b] = m + 1;
+    levels = std::max(levels, m + 2);
+  }
+  sc.levels = levels;
+  // blocks by level (within a level in sweep direction)
+  std::vector<int> start((size_t)levels + 1, 0), order(nb);
+  for (unsigned b = 0; b < nb; ++b) ++start[(size_t)lvl[b] + 1];
+  for (int l = 0; l < levels; ++l) start[(size_t)l + 1] += start[(size_t)l];
+  for (unsigned k = 0; k < nb; ++k) {
+    const unsigned b = upper ? nb - 1 - k : k;
+    order[(size_t)start[(size_t)lvl[b]]++] = (int)(b | (scan[b] ? kScanBit : 0u));
+  }
+  MLSH_CUDA_TRY(cudaMemcpyAsync(sc.order, order.data(), sizeof(int) * (size_t)nb,
+                                cudaMemcpyHostToDevice, s));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(s));
+  return MLSH_SUCCESS;
+}
+
+int build_impl(Handle &h, const CsrPlan &p, int kind, double omega, bool solver_scale,
+               Precond &pc) {
+  cudaStream_t s = h.stream;
+  const int n = p.n_rows;
+  const size_t esz = (size_t)dtype_size(p.dtype);
+  pc.handle = &h;
+  pc.plan = &p;
+  pc.kind = kind;
+  pc.dtype = p.dtype;
+  pc.n = n;
+  pc.nnz = p.nnz;
+  pc.nb = (unsigned)((n + 31) / 32);
+  const size_t nn = (size_t)std::max(n, 1);
+  MLSH_CUDA_TRY(pool_alloc(&pc.lo_end, sizeof(int) * nn, s));
+  MLSH_CUDA_TRY(pool_alloc(&pc.up_beg, sizeof(int) * nn, s));
+  MLSH_CUDA_TRY(pool_alloc(&pc.tmp, esz * nn, s));
+  MLSH_CUDA_TRY(pool_alloc(&pc.ticket, sizeof(unsigned long long), s));
+  MLSH_CUDA_TRY(pool_alloc(&pc.flags, sizeof(unsigned) * std::max<size_t>(pc.nb, 1), s));
+  MLSH_CUDA_TRY(cudaMemsetAsync(pc.ticket, 0, sizeof(unsigned long long), s));
+  MLSH_CUDA_TRY(cudaMemsetAsync(pc.flags, 0, sizeof(unsigned) * std::max<size_t>(pc.nb, 1), s));
+  if (n == 0) {
+    MLSH_CUDA_TRY(cudaStreamSynchronize(s));
+    return MLSH_SUCCESS;
+  }
+  unsigned long long missing = ~0ull;
+  int st = split_rows(h, p.row_ptr, p.col_ind, n, pc.lo_end, pc.up_beg, &missing);
+  if (st != MLSH_SUCCESS) return st;
+  st = build_schedule(h, p.row_ptr, p.col_ind, pc.lo_end, pc.up_beg, n, pc.nb, false, pc.sfwd);
+  if (st != MLSH_SUCCESS) return st;
+  if (kind != MLSH_PRECOND_IC && !solver_scale) {
+    st = build_schedule(h, p.row_ptr, p.col_ind, pc.lo_end, pc.up_beg, n, pc.nb, true, pc.sbwd);
+    if (st != MLSH_SUCCESS) return st;
+  }
+  if (kind == MLSH_PRECOND_SOR) {
+    // M = 1/(omega d) for the preconditioner; 1/((1/omega) d) for the solver
+    MLSH_CUDA_TRY(pool_alloc(&pc.scale, esz * nn, s));
+    if (p.dtype == MLSH_F64) {
+      const double w = solver_scale ? 1.0 / omega : omega;
+      sor_scale_kernel<double><<<grid_of(n, 256), 256, 0, s>>>(
+          static_cast<const double *>(p.val), pc.lo_end, pc.up_beg, n, w,
+          static_cast<double *>(pc.scale));
+    } else {
+      const float of = (float)omega;
+      const float w = solver_scale ? (float)(1.0 / (double)of) : of;
+      sor_scale_kernel<float><<<grid_of(n, 256), 256, 0, s>>>(
+          static_cast<const float *>(p.val), pc.lo_end, pc.up_beg, n, w,
+          static_cast<float *>(pc.scale));
+    }
+    MLSH_CUDA_TRY(cudaGetLastError());
+    pc.fwd = Sweep{p.row_ptr,     p.col_ind,       p.val,          pc.lo_end, pc.up_beg,
+                   pc.scale,      kSorFwd,         pc.sfwd.order,  pc.sfwd.dep_off,
+                   pc.sfwd.dep_ids};
+    pc.bwd = Sweep{p.row_ptr,     p.col_ind,       p.val,          pc.lo_end, pc.up_beg,
+                   pc.scale,      kSorBwd,         pc.sbwd.order,  pc.sbwd.dep_off,
+                   pc.sbwd.dep_ids};
+    MLSH_CUDA_TRY(cudaStreamSynchronize(s));
+    return MLSH_SUCCESS;
+  }
+  if (missing != ~0ull) {
+    pc.pivot = (long long)missing;
+    pc.structural = 1;
+  }
+  MLSH_CUDA_TRY(pool_alloc(&pc.fval, esz * (size_t)std::max(p.nnz, 1), s));
+  if (p.nnz > 0)
+    MLSH_CUDA_TRY(cudaMemcpyAsync(pc.fval, p.val, esz * (size_t)p.nnz,
+                                  cudaMemcpyDeviceToDevice, s));
+  st = p.dtype == MLSH_F64 ? factor_run<double>(h, pc, p.row_ptr, p.col_ind)
+                           : factor_run<float>(h, pc, p.row_ptr, p.col_ind);
+  if (st != MLSH_SUCCESS) return st;
+  if (kind == MLSH_PRECOND_ILU) {
+    pc.fwd = Sweep{p.row_ptr,     p.col_ind,       pc.fval,        pc.lo_end, pc.up_beg,
+                   nullptr,       kUnitFwd,        pc.sfwd.order,  pc.sfwd.dep_off,
+                   pc.sfwd.dep_ids};
+    pc.bwd = Sweep{p.row_ptr,     p.col_ind,       pc.fval,        pc.lo_end, pc.up_beg,
+                   nullptr,       kDiagBwd,        pc.sbwd.order,  pc.sbwd.dep_off,
+                   pc.sbwd.dep_ids};
+    return MLSH_SUCCESS;
+  }
+  // IC: L^T as the rows of the factor's transpose (its upper triangle)
+  MLSH_CUDA_TRY(pool_alloc(&pc.rp_t, sizeof(int) * (nn + 1), s));
+  MLSH_CUDA_TRY(pool_alloc(&pc.ci_t, sizeof(int) * (size_t)std::max(p.nnz, 1), s));
+  MLSH_CUDA_TRY(pool_alloc(&pc.val_t, esz * (size_t)std::max(p.nnz, 1), s));
+  MLSH_CUDA_TRY(pool_alloc(&pc.lo_t, sizeof(int) * nn, s));
+  MLSH_CUDA_TRY(pool_alloc(&pc.up_t, sizeof(int) * nn, s));
+  st = transpose_build(h, n, n, p.nnz, p.row_ptr, p.col_ind, pc.fval, p.dtype, pc.rp_t,
+                       pc.ci_t, pc.val_t, nullptr);
+  if (st != MLSH_SUCCESS) return st;
+  unsigned long long missing_t = ~0ull;
+  st = split_rows(h, pc.rp_t, pc.ci_t, n, pc.lo_t, pc.up_t, &missing_t);
+  if (st != MLSH_SUCCESS) return st;
+  st = build_schedule(h, pc.rp_t, pc.ci_t, pc.lo_t, pc.up_t, n, pc.nb, true, pc.sbwd);
+  if (st != MLSH_SUCCESS) return st;
+  pc.fwd = Sweep{p.row_ptr,     p.col_ind,       pc.fval,        pc.lo_end, pc.up_beg,
+                 nullptr,       kDiagFwd,        pc.sfwd.order,  pc.sfwd.dep_off,
+                 pc.sfwd.dep_ids};
+  pc.bwd = Sweep{pc.rp_t,       pc.ci_t,         pc.val_t,       pc.lo_t,   pc.up_t,
+                 nullptr,       kDiagBwd,        pc.sbwd.order,  pc.sbwd.dep_off,
+                 pc.sbwd.dep_ids};
+  return MLSH_SUCCESS;
+}
+
+}  // namespace
+
+int precond_build(Handle &h, const CsrPlan &p, int kind, double omega, bool solver_scale,
+                  Precond &out) {
+  const int st = build_impl(h, p, kind, omega, solver_scale, out);
+  if (st != MLSH_SUCCESS) {
+    cudaGetLastError();
+    precond_release(out);
+  }
+  return st;
+}
+
+}  // namespace mlsh
+
+using namespace mlsh;
+
+// ===================================================================== C ABI
+extern "C" {
+
+int mlsh_precond_create(mlsh_handle hs, mlsh_csr_plan ps, int kind, double omega,
+                        mlsh_precond *out) {
+  if (!hs || !ps || !out) return MLSH_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (kind != MLSH_PRECOND_SOR && kind != MLSH_PRECOND_IC && kind != MLSH_PRECOND_ILU)
+    return MLSH_ERR_INVALID_ARG;
+  const CsrPlan &p = ps->p;
+  if (p.n_rows != p.n_cols) return MLSH_ERR_INVALID_ARG;
+  if (kind == MLSH_PRECOND_SOR && !(omega == omega)) return MLSH_ERR_INVALID_ARG;
+  auto *pc = new (std::nothrow) mlsh_precond_s;
+  if (!pc) return MLSH_ERR_OOM;
+  const int st = precond_build(hs->h, p, kind, omega, false, pc->p);
+  if (st != MLSH_SUCCESS) {
+    delete pc;
+    return st;
+  }
+  *out = pc;
+  return MLSH_SUCCESS;
+}
+
+int mlsh_precond_zero_pivot(mlsh_precond pc, int64_t *row, int *structural) {
+  if (!pc || !row) return MLSH_ERR_INVALID_ARG;
+  *row = pc->p.pivot;
+  if (structural) *structural = pc->p.pivot >= 0 ? pc->p.structural : 0;
+  return MLSH_SUCCESS;
+}
+
+int mlsh_precond_apply(mlsh_handle hs, mlsh_precond pc, const void *r, void *z) {
+  if (!hs || !pc) return MLSH_ERR_INVALID_ARG;
+  const Precond &p = pc->p;
+  if (p.n == 0) return MLSH_SUCCESS;
+  if (!r || !z || r == z) return MLSH_ERR_INVALID_ARG;
+  Handle &h = hs->h;
+  MLSH_CUDA_TRY(cudaMemsetAsync(h.err_flag, 0, sizeof(int), h.stream));
+  MLSH_CUDA_TRY(precond_apply_launch(p, r, z, nullptr, h.err_flag, h.stream));
+  int err = 0;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(&h.host_scalars[7], h.err_flag, sizeof(int),
+                                cudaMemcpyDeviceToHost, h.stream));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  std::memcpy(&err, &h.host_scalars[7], sizeof(int));
+  return err;
+}
+
+int mlsh_precond_factor(mlsh_handle hs, mlsh_precond pc, void *out) {
+  if (!hs || !pc || !out) return MLSH_ERR_INVALID_ARG;
+  const Precond &p = pc->p;
+  const size_t esz = (size_t)dtype_size(p.dtype);
+  Handle &h = hs->h;
+  if (p.kind == MLSH_PRECOND_SOR) {
+    if (p.n > 0)
+      MLSH_CUDA_TRY(cudaMemcpyAsync(out, p.scale, esz * (size_t)p.n, cudaMemcpyDeviceToDevice,
+                                    h.stream));
+  } else if (p.nnz > 0) {
+    MLSH_CUDA_TRY(cudaMemcpyAsync(out, p.fval, esz * (size_t)p.nnz, cudaMemcpyDeviceToDevice,
+                                  h.stream));
+  }
+  MLSH_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  return MLSH_SUCCESS;
+}
+
+int mlsh_precond_destroy(mlsh_precond pc) {
+  if (!pc) return MLSH_SUCCESS;
+  if (pc->p.handle) {
+    purge_precond_graphs(*pc->p.handle, &pc->p);
+    cudaStreamSynchronize(pc->p.handle->stream);
+  }
+  precond_release(pc->p);
+  delete pc;
+  return MLSH_SUCCESS;
+}
+
+}  // extern "C"

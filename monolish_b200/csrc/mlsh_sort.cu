@@ -418,6 +418,8 @@ void run_compact_t(const unsigned *flag, const unsigned *pos, const int *row, co
                                              n, row_out, col_out, static_cast<T *>(val_out));
 }
 
+}  // namespace
+
 // A^T of an n_rows x n_cols CRS into (rp_t, ci_t, val_t); the entry
 // permutation (position in A of each entry of A^T) into perm_out if given.
 int transpose_build(Handle &h, int n_rows, int n_cols, int nnz, const int *rp, const int *ci,
@@ -459,6 +461,8 @@ int transpose_build(Handle &h, int n_rows, int n_cols, int nnz, const int *rp, c
   MLSH_CUDA_TRY(cudaStreamSynchronize(s));
   return MLSH_SUCCESS;
 }
+
+namespace {
 
 // The transpose kept with a plan for mlsh_spmv_transpose.
 struct TransposeCache {

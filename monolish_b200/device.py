@@ -133,9 +133,10 @@ class Crs:
         self.plan = plan
 
     def close(self):
-        if self.plan:
+        # after its handle is destroyed the plan's memory went with it
+        if self.plan and self.handle.h:
             self.lib.mlsh_csr_plan_destroy(self.plan)
-            self.plan = None
+        self.plan = None
 
     def __del__(self):
         try:
@@ -308,9 +309,9 @@ class Batch:
         self.b = bh
 
     def close(self):
-        if self.b:
+        if self.b and self.handle.h:
             self.lib.mlsh_batch_destroy(self.b)
-            self.b = None
+        self.b = None
 
     def __del__(self):
         try:
@@ -358,6 +359,90 @@ def cg_solve(A: Crs, b, x, tol, maxiter, **kw) -> SolveResult:
 
 def bicgstab_solve(A: Crs, b, x, tol, maxiter, **kw) -> SolveResult:
     return _solve(A.lib.mlsh_bicgstab_solve, A, b, x, tol, maxiter, **kw)
+
+
+class Precond:
+    """mlsh_precond: SOR / IC(0) / ILU(0) of a plan's matrix
+    (equation::SOR / IC / ILU create_precond; apply = apply_precond)."""
+
+    def __init__(self, A: Crs, kind, omega=1.9):
+        self.A = A
+        self.lib = A.lib
+        self.kind = int(kind)
+        h = C.c_void_p()
+        _abi.check(self.lib.mlsh_precond_create(A.handle.h, A.plan, self.kind, float(omega),
+                                                C.byref(h)), "mlsh_precond_create")
+        self.pc = h
+
+    def zero_pivot(self):
+        """(row, structural): the first zero pivot, row -1 if none."""
+        row, structural = C.c_int64(), C.c_int()
+        _abi.check(self.lib.mlsh_precond_zero_pivot(self.pc, C.byref(row), C.byref(structural)))
+        return int(row.value), int(structural.value)
+
+    def apply(self, r, z):
+        _abi.check(self.lib.mlsh_precond_apply(self.A.handle.h, self.pc, ptr(r), ptr(z)),
+                   "mlsh_precond_apply")
+
+    def factor(self):
+        """SOR: M (n); IC / ILU: the factor's values in A's pattern (nnz)."""
+        n = self.A.n_rows if self.kind == _abi.PRECOND_SOR else self.A.nnz
+        out = torch.empty(max(n, 1), dtype=_torch_dtype(self.A.dtype), device="cuda")
+        _abi.check(self.lib.mlsh_precond_factor(self.A.handle.h, self.pc, ptr(out)))
+        return out[:n]
+
+    def close(self):
+        if self.pc and self.A.handle.h:
+            self.lib.mlsh_precond_destroy(self.pc)
+        self.pc = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _solve_pc(fn, A: Crs, pc: Precond, b, x, tol, maxiter, miniter=0, use_graph=True,
+              check_every=0, history=None):
+    o = _opts(tol, maxiter, miniter, _abi.PRECOND_NONE, use_graph, check_every,
+              _abi.ENGINE_KERNELS, 0)
+    if history is not None:
+        o.history = history.ctypes.data_as(C.POINTER(C.c_double))
+        o.history_len = len(history)
+    r = _abi.SolverResult()
+    st = fn(A.handle.h, A.plan, pc.pc, ptr(b), ptr(x), C.byref(o), C.byref(r))
+    if st not in (_abi.SUCCESS, _abi.SOLVER_MAXITER, _abi.SOLVER_BREAKDOWN,
+                  _abi.SOLVER_RESIDUAL_NAN, _abi.SOLVER_SIZE_ERROR):
+        raise _abi.MlshError(st, "preconditioned solve")
+    return SolveResult(st, int(r.iters), float(r.final_resid), 0)
+
+
+def cg_solve_precond(A: Crs, pc: Precond, b, x, tol, maxiter, **kw) -> SolveResult:
+    """CG preconditioned by an SOR / IC / ILU object."""
+    return _solve_pc(A.lib.mlsh_cg_solve_precond, A, pc, b, x, tol, maxiter, **kw)
+
+
+def bicgstab_solve_precond(A: Crs, pc: Precond, b, x, tol, maxiter, **kw) -> SolveResult:
+    """BiCGSTAB preconditioned by an SOR / IC / ILU object."""
+    return _solve_pc(A.lib.mlsh_bicgstab_solve_precond, A, pc, b, x, tol, maxiter, **kw)
+
+
+def sor_solve(A: Crs, b, x, tol, maxiter, omega=1.9, miniter=0, use_graph=True,
+              check_every=0, history=None) -> SolveResult:
+    """equation::SOR::solve: relative stopping rule ||r|| / ||b|| < tol."""
+    o = _opts(tol, maxiter, miniter, _abi.PRECOND_NONE, use_graph, check_every,
+              _abi.ENGINE_KERNELS, 0)
+    if history is not None:
+        o.history = history.ctypes.data_as(C.POINTER(C.c_double))
+        o.history_len = len(history)
+    r = _abi.SolverResult()
+    st = A.lib.mlsh_sor_solve(A.handle.h, A.plan, ptr(b), ptr(x), float(omega), C.byref(o),
+                              C.byref(r))
+    if st not in (_abi.SUCCESS, _abi.SOLVER_MAXITER, _abi.SOLVER_BREAKDOWN,
+                  _abi.SOLVER_RESIDUAL_NAN, _abi.SOLVER_SIZE_ERROR):
+        raise _abi.MlshError(st, "SOR solve")
+    return SolveResult(st, int(r.iters), float(r.final_resid), 0)
 
 
 @dataclass

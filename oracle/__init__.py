@@ -57,7 +57,17 @@ class Restatement:
         lib.oracle_true_relres_d.restype = D
         for nm in ("oracle_cg_d", "oracle_cg_s", "oracle_bicgstab_d", "oracle_bicgstab_s"):
             f = getattr(lib, nm)
-            f.argtypes = [I, P, P, P, P, P, D, L, L, I, C.POINTER(L), C.POINTER(D)]
+            f.argtypes = [I, P, P, P, P, P, D, L, L, I, D, C.POINTER(L), C.POINTER(D)]
+            f.restype = I
+        for sfx in ("d", "s"):
+            f = getattr(lib, f"oracle_precond_factor_{sfx}")
+            f.argtypes = [I, P, P, P, I, D, P, C.POINTER(L)]
+            f.restype = I
+            f = getattr(lib, f"oracle_precond_apply_{sfx}")
+            f.argtypes = [I, P, P, P, I, D, P, P]
+            f.restype = I
+            f = getattr(lib, f"oracle_sor_{sfx}")
+            f.argtypes = [I, P, P, P, P, P, D, D, L, L, P, C.POINTER(L), C.POINTER(D)]
             f.restype = I
 
     def spmv(self, rp, ci, v, x):
@@ -110,13 +120,46 @@ class Restatement:
     def true_relres(self, rp, ci, v, b, x):
         return self.lib.oracle_true_relres_d(len(rp) - 1, _p(rp), _p(ci), _p(v), _p(b), _p(x))
 
-    def _solve(self, name, rp, ci, v, b, x0, tol, maxiter, miniter=0, precond=1):
+    def _solve(self, name, rp, ci, v, b, x0, tol, maxiter, miniter=0, precond=1, omega=1.9):
+        """precond: 0 none, 1 Jacobi, 2 SOR (omega), 3 IC(0), 4 ILU(0)."""
         sfx = "d" if v.dtype == np.float64 else "s"
         x = x0.copy()
         it, res = C.c_long(), C.c_double()
         st = getattr(self.lib, f"oracle_{name}_{sfx}")(
             len(rp) - 1, _p(rp), _p(ci), _p(v), _p(b), _p(x), tol, maxiter, miniter, precond,
-            C.byref(it), C.byref(res))
+            omega, C.byref(it), C.byref(res))
+        return st, it.value, res.value, x
+
+    def precond_factor(self, rp, ci, v, kind, omega=1.9):
+        """(values, pivot): SOR M (n), IC / ILU the factor in A's pattern."""
+        sfx = "d" if v.dtype == np.float64 else "s"
+        n = len(rp) - 1
+        out = np.zeros(n if kind == 2 else int(rp[-1]), v.dtype)
+        piv = C.c_long()
+        st = getattr(self.lib, f"oracle_precond_factor_{sfx}")(
+            n, _p(rp), _p(ci), _p(v), kind, omega, _p(out), C.byref(piv))
+        if st != 0:
+            raise ValueError("rows not sorted")
+        return out, piv.value
+
+    def precond_apply(self, rp, ci, v, kind, r, omega=1.9):
+        sfx = "d" if v.dtype == np.float64 else "s"
+        z = np.zeros_like(r)
+        getattr(self.lib, f"oracle_precond_apply_{sfx}")(
+            len(rp) - 1, _p(rp), _p(ci), _p(v), kind, omega, _p(r), _p(z))
+        return z
+
+    def sor(self, rp, ci, v, b, x0, tol, maxiter, omega=1.9, miniter=0, history=False):
+        """(status, iters, final resid, x[, relative residual history])."""
+        sfx = "d" if v.dtype == np.float64 else "s"
+        x = x0.copy()
+        it, res = C.c_long(), C.c_double()
+        hist = np.zeros(max(int(maxiter), 1), np.float64) if history else None
+        st = getattr(self.lib, f"oracle_sor_{sfx}")(
+            len(rp) - 1, _p(rp), _p(ci), _p(v), _p(b), _p(x), omega, tol, maxiter, miniter,
+            _p(hist) if history else None, C.byref(it), C.byref(res))
+        if history:
+            return st, it.value, res.value, x, hist[:it.value].copy()
         return st, it.value, res.value, x
 
     def cg(self, *a, **k):
@@ -161,6 +204,13 @@ class Reference:
         lib.ref_coo_sort_d.restype = L
         lib.ref_coo_to_crs_d.argtypes = [I, I, L, P, P, P, P]
         lib.ref_coo_to_crs_d.restype = I
+        for sfx in ("d", "s"):
+            f = getattr(lib, f"ref_sor_{sfx}")
+            f.argtypes = [I, I, P, P, P, P, P, D, D, L, C.POINTER(L), C.POINTER(D), C.POINTER(D)]
+            f.restype = I
+            f = getattr(lib, f"ref_sor_apply_{sfx}")
+            f.argtypes = [I, I, P, P, P, D, P, P]
+            f.restype = I
 
     def threads(self):
         return self.lib.ref_max_threads()
@@ -207,10 +257,29 @@ class Reference:
         return st, it.value, res.value, x, sec.value
 
     def cg(self, *a, **k):
+        """precond: 0 none, 1 Jacobi, 2 SOR (omega 1.9)."""
         return self._solve("cg", *a, **k)
 
     def bicgstab(self, *a, **k):
         return self._solve("bicgstab", *a, **k)
+
+    def sor(self, rp, ci, v, b, x0, tol, maxiter, omega=1.9):
+        """equation::SOR::solve: (status, iters, final resid, x, seconds)."""
+        sfx = "d" if v.dtype == np.float64 else "s"
+        x = x0.copy()
+        it, res, sec = C.c_long(), C.c_double(), C.c_double()
+        st = getattr(self.lib, f"ref_sor_{sfx}")(
+            len(rp) - 1, int(rp[-1]), _p(rp), _p(ci), _p(v), _p(b), _p(x), omega, tol,
+            maxiter, C.byref(it), C.byref(res), C.byref(sec))
+        return st, it.value, res.value, x, sec.value
+
+    def sor_apply(self, rp, ci, v, r, omega=1.9):
+        """equation::SOR create_precond + apply_precond: z = M^{-1} r."""
+        sfx = "d" if v.dtype == np.float64 else "s"
+        z = np.zeros_like(r)
+        getattr(self.lib, f"ref_sor_apply_{sfx}")(len(rp) - 1, int(rp[-1]), _p(rp), _p(ci),
+                                                  _p(v), omega, _p(r), _p(z))
+        return z
 
     def dot(self, x, y):
         return self.lib.ref_dot_d(len(x), _p(x), _p(y))

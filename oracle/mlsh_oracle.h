@@ -53,18 +53,46 @@ double oracle_dot_d(long n, const double *x, const double *y);
 double oracle_nrm2_d(long n, const double *x);
 double oracle_dot_s(long n, const float *x, const float *y);
 
+/* precond: 0 none, 1 Jacobi, 2 SOR (relaxation omega), 3 IC(0), 4 ILU(0). */
 int oracle_cg_d(int n, const int *rp, const int *ci, const double *v,
                 const double *b, double *x, double tol_abs, long maxiter,
-                long miniter, int precond, long *iters, double *resid);
+                long miniter, int precond, double omega, long *iters,
+                double *resid);
 int oracle_cg_s(int n, const int *rp, const int *ci, const float *v,
                 const float *b, float *x, double tol_abs, long maxiter,
-                long miniter, int precond, long *iters, double *resid);
+                long miniter, int precond, double omega, long *iters,
+                double *resid);
 int oracle_bicgstab_d(int n, const int *rp, const int *ci, const double *v,
                       const double *b, double *x, double tol_abs, long maxiter,
-                      long miniter, int precond, long *iters, double *resid);
+                      long miniter, int precond, double omega, long *iters,
+                      double *resid);
 int oracle_bicgstab_s(int n, const int *rp, const int *ci, const float *v,
                       const float *b, float *x, double tol_abs, long maxiter,
-                      long miniter, int precond, long *iters, double *resid);
+                      long miniter, int precond, double omega, long *iters,
+                      double *resid);
+
+/* SOR / IC(0) / ILU(0) (kinds 2 / 3 / 4), rows sorted by column.
+ * factor: SOR M = 1/(omega diag) (n values); IC / ILU the factor in A's
+ * pattern (nnz values); *pivot = first zero pivot row or -1.  Returns -1
+ * for unsorted rows.  apply: z = M^{-1} r. */
+int oracle_precond_factor_d(int n, const int *rp, const int *ci, const double *v,
+                            int kind, double omega, double *out, long *pivot);
+int oracle_precond_factor_s(int n, const int *rp, const int *ci, const float *v,
+                            int kind, double omega, float *out, long *pivot);
+int oracle_precond_apply_d(int n, const int *rp, const int *ci, const double *v,
+                           int kind, double omega, const double *r, double *z);
+int oracle_precond_apply_s(int n, const int *rp, const int *ci, const float *v,
+                           int kind, double omega, const float *r, float *z);
+/* equation::SOR::solve: relative stopping test, history of the relative
+ * residual (maxiter entries) if hist is given. */
+int oracle_sor_d(int n, const int *rp, const int *ci, const double *v,
+                 const double *b, double *x, double omega, double tol,
+                 long maxiter, long miniter, double *hist, long *iters,
+                 double *resid);
+int oracle_sor_s(int n, const int *rp, const int *ci, const float *v,
+                 const float *b, float *x, double omega, double tol,
+                 long maxiter, long miniter, double *hist, long *iters,
+                 double *resid);
 
 /* ||b - A x||_2 / ||b||_2 in double. */
 double oracle_true_relres_d(int n, const int *rp, const int *ci,

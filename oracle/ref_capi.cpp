@@ -12,6 +12,7 @@
 //   - equation::CG::solve: src/equation/cg.cpp:13-116
 //   - equation::BiCGSTAB::solve: src/equation/bicgstab.cpp:13-166
 //   - equation::Jacobi as preconditioner: src/equation/jacobi.cpp:12-61
+//   - equation::SOR as preconditioner and as solver: src/equation/sor.cpp
 //   - blas::matvec_T, COO::sort, CRS(COO&): see the entry points below
 // Nothing in the product links against this file.
 #include <chrono>
@@ -76,10 +77,14 @@ int solve_impl(int n, int nnz, const int *rp, const int *ci, const T *v,
   solver.set_miniter(0);
   solver.set_maxiter(static_cast<size_t>(maxiter));
   monolish::equation::Jacobi<monolish::matrix::CRS<T>, T> jac;
+  monolish::equation::SOR<monolish::matrix::CRS<T>, T> sor;
   monolish::equation::none<monolish::matrix::CRS<T>, T> non;
   if (precond == 1) {
     solver.set_create_precond(jac);
     solver.set_apply_precond(jac);
+  } else if (precond == 2) {
+    solver.set_create_precond(sor);
+    solver.set_apply_precond(sor);
   } else {
     solver.set_create_precond(non);
     solver.set_apply_precond(non);
@@ -94,9 +99,73 @@ int solve_impl(int n, int nnz, const int *rp, const int *ci, const T *v,
   return ret;
 }
 
+// equation::SOR::solve (src/equation/sor.cpp:92-162) with the default
+// none preconditioner.
+template <typename T>
+int sor_solve_impl(int n, int nnz, const int *rp, const int *ci, const T *v, const T *b, T *x,
+                   double omega, double tol, long maxiter, long *iters, double *resid,
+                   double *seconds) {
+  auto A = make_crs<T>(n, nnz, rp, ci, v);
+  monolish::vector<T> bv(b, b + n);
+  monolish::vector<T> xv(x, x + n);
+  monolish::equation::SOR<monolish::matrix::CRS<T>, T> solver;
+  monolish::equation::none<monolish::matrix::CRS<T>, T> non;
+  solver.set_tol(tol);
+  solver.set_lib(0);
+  solver.set_miniter(0);
+  solver.set_maxiter(static_cast<size_t>(maxiter));
+  solver.set_omega(static_cast<T>(omega));
+  solver.set_create_precond(non);
+  solver.set_apply_precond(non);
+  double t0 = now_s();
+  int ret = solver.solve(A, xv, bv);
+  double dt = now_s() - t0;
+  std::memcpy(x, xv.data(), sizeof(T) * n);
+  if (iters) *iters = static_cast<long>(solver.get_final_iter());
+  if (resid) *resid = solver.get_final_residual();
+  if (seconds) *seconds = dt;
+  return ret;
+}
+
+// equation::SOR::create_precond + apply_precond (sor.cpp:13-69).
+template <typename T>
+int sor_apply_impl(int n, int nnz, const int *rp, const int *ci, const T *v, double omega,
+                   const T *r, T *z) {
+  auto A = make_crs<T>(n, nnz, rp, ci, v);
+  monolish::vector<T> rv(r, r + n);
+  monolish::vector<T> zv(n, 0.0);
+  monolish::equation::SOR<monolish::matrix::CRS<T>, T> pc;
+  pc.set_omega(static_cast<T>(omega));
+  pc.create_precond(A);
+  pc.apply_precond(rv, zv);
+  std::memcpy(z, zv.data(), sizeof(T) * n);
+  return 0;
+}
+
 } // namespace
 
 extern "C" {
+
+int ref_sor_d(int n, int nnz, const int *rp, const int *ci, const double *v, const double *b,
+              double *x, double omega, double tol, long maxiter, long *iters, double *resid,
+              double *seconds) {
+  return sor_solve_impl<double>(n, nnz, rp, ci, v, b, x, omega, tol, maxiter, iters, resid,
+                                seconds);
+}
+int ref_sor_s(int n, int nnz, const int *rp, const int *ci, const float *v, const float *b,
+              float *x, double omega, double tol, long maxiter, long *iters, double *resid,
+              double *seconds) {
+  return sor_solve_impl<float>(n, nnz, rp, ci, v, b, x, omega, tol, maxiter, iters, resid,
+                               seconds);
+}
+int ref_sor_apply_d(int n, int nnz, const int *rp, const int *ci, const double *v,
+                    double omega, const double *r, double *z) {
+  return sor_apply_impl<double>(n, nnz, rp, ci, v, omega, r, z);
+}
+int ref_sor_apply_s(int n, int nnz, const int *rp, const int *ci, const float *v,
+                    double omega, const float *r, float *z) {
+  return sor_apply_impl<float>(n, nnz, rp, ci, v, omega, r, z);
+}
 
 // y = A^T x through blas::matvec_T (src/blas/matrix/matvec/crs_matvec.hpp:88-98
 // for the OSS path) on an n_rows x n_cols CRS<double>.
