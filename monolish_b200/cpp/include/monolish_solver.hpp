@@ -21,6 +21,10 @@ template <typename MATRIX, typename Float> class precondition {
   vector<Float> M;
   MATRIX *A = nullptr;
   int kind = MLSH_PRECOND_NONE;
+  // SOR / IC / ILU: the bound object and how to build its device
+  // preconditioner for a matrix (its create_precond)
+  void *obj = nullptr;
+  mlsh_precond (*make)(void *obj, MATRIX &A) = nullptr;
   void set_precond_data(vector<Float> &m) { M = m; }
   vector<Float> get_precond_data() { return M; }
 };
@@ -43,20 +47,33 @@ template <typename MATRIX, typename Float> class solver {
   int reorder = 3;
   precondition<MATRIX, Float> precond;
 
+  template <class PRECOND> void bind_precond(PRECOND &p) {
+    precond.kind = PRECOND::precond_kind;
+    if constexpr (PRECOND::precond_kind >= MLSH_PRECOND_SOR) {
+      precond.obj = &p;
+      precond.make = [](void *o, MATRIX &A) -> mlsh_precond {
+        auto &pp = *static_cast<PRECOND *>(o);
+        pp.create_precond(A);
+        return pp.native();
+      };
+    } else {
+      precond.obj = nullptr;
+      precond.make = nullptr;
+    }
+  }
+
  public:
   solver() = default;
   ~solver() {
     if (rhistory_stream != &std::cout && !rhistory_file.empty()) delete rhistory_stream;
   }
 
-  // Bind a preconditioner (equation::Jacobi or equation::none).
+  // Bind a preconditioner (equation::Jacobi, none, SOR, IC or ILU).
   template <class PRECOND> void set_create_precond(PRECOND &p) {
-    (void)p;
-    precond.kind = PRECOND::precond_kind;
+    bind_precond(p);
   }
   template <class PRECOND> void set_apply_precond(PRECOND &p) {
-    (void)p;
-    precond.kind = PRECOND::precond_kind;
+    bind_precond(p);
   }
 
   void set_lib(int l) { lib = l; }

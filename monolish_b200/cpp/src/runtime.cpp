@@ -99,7 +99,7 @@ void log_solver(const char *name, double seconds) {
 
 int krylov_solve(int kind, mlsh_csr_plan plan, const void *d_b, void *d_x, double tol,
                  size_t maxiter, size_t miniter, int precond, std::ostream *hist_out,
-                 size_t *iters, double *resid) {
+                 size_t *iters, double *resid, mlsh_precond pc, double omega) {
   mlsh_solver_opts o;
   mlsh_solver_opts_default(&o);
   o.tol = tol;
@@ -114,9 +114,18 @@ int krylov_solve(int kind, mlsh_csr_plan plan, const void *d_b, void *d_x, doubl
     o.history_len = cap;
   }
   mlsh_solver_result r{};
-  const int st = kind == 0 ? mlsh_cg_solve(handle(), plan, d_b, d_x, &o, &r)
-                           : mlsh_bicgstab_solve(handle(), plan, d_b, d_x, &o, &r);
-  check(st, kind == 0 ? "CG" : "BiCGSTAB");
+  int st;
+  if (kind == 2) {  // the SOR iteration (its own preconditioner: none)
+    o.precond = MLSH_PRECOND_NONE;
+    st = mlsh_sor_solve(handle(), plan, d_b, d_x, omega, &o, &r);
+  } else if (pc) {
+    st = kind == 0 ? mlsh_cg_solve_precond(handle(), plan, pc, d_b, d_x, &o, &r)
+                   : mlsh_bicgstab_solve_precond(handle(), plan, pc, d_b, d_x, &o, &r);
+  } else {
+    st = kind == 0 ? mlsh_cg_solve(handle(), plan, d_b, d_x, &o, &r)
+                   : mlsh_bicgstab_solve(handle(), plan, d_b, d_x, &o, &r);
+  }
+  check(st, kind == 0 ? "CG" : (kind == 1 ? "BiCGSTAB" : "SOR"));
   *iters = (size_t)r.iters;
   *resid = r.final_resid;
   if (hist_out) {

@@ -30,8 +30,14 @@ Cases (all small, so the CPU restatement replays them in seconds):
                row pointer; the (row, col) sequence COO::sort leaves when
                600 duplicates are added (their kept values depend on the
                reference's quicksort order and are not stored).
+  precond      equation::SOR (omega 1.9): create_precond + apply_precond on
+               a 3D 7-point 8^3 Poisson matrix and on a 500-row random
+               nonsymmetric matrix (sorted rows), double and float;
+               SOR::solve on the 16x16 Poisson matrix (b = ones, tol 1e-8 /
+               1e-4); CG and BiCGSTAB preconditioned by SOR on poisson16.
 
-    python tests/golden/make_golden.py setup   # that case only
+    python tests/golden/make_golden.py setup     # that case only
+    python tests/golden/make_golden.py precond   # that case only
 """
 import os
 import sys
@@ -80,11 +86,51 @@ def setup_case(ref):
     return out
 
 
+def random_sorted(n, per_row, seed):
+    """Diagonally dominant nonsymmetric CRS with sorted rows."""
+    rng = np.random.default_rng(seed)
+    rp, ci, v = [0], [], []
+    for i in range(n):
+        cols = np.unique(np.append(rng.choice(n, per_row, replace=False), i))
+        vals = rng.uniform(-1, 1, len(cols))
+        vals[cols == i] = np.abs(vals).sum() + 1.0
+        ci.extend(cols.tolist())
+        v.extend(vals.tolist())
+        rp.append(len(ci))
+    return np.array(rp, np.int32), np.array(ci, np.int32), np.array(v)
+
+
+def precond_case(ref):
+    out = {}
+    _, rp, ci, v = W.poisson3d(8)
+    rr, rc, rv = random_sorted(500, 6, 5)
+    for tag, (a, b, c) in (("p3", (rp, ci, v)), ("rnd", (rr, rc, rv))):
+        n = len(a) - 1
+        r = W.uniform_mt(n, -1.0, 1.0, 51)
+        out[f"{tag}_rp"], out[f"{tag}_ci"], out[f"{tag}_v"], out[f"{tag}_r"] = a, b, c, r
+        out[f"{tag}_z_d"] = ref.sor_apply(a, b, c, r, omega=1.9)
+        out[f"{tag}_z_s"] = ref.sor_apply(a, b, c.astype(np.float32), r.astype(np.float32),
+                                          omega=1.9)
+    n, rp, ci, v = W.poisson2d(16)
+    b = np.ones(n)
+    for sfx, dt, tol in (("d", np.float64, 1e-8), ("s", np.float32, 1e-4)):
+        st, it, res, x, _ = ref.sor(rp, ci, v.astype(dt), b.astype(dt), np.zeros(n, dt), tol,
+                                    5000, omega=1.9)
+        out[f"sor_{sfx}"] = np.array([st, it, res])
+        out[f"sor_{sfx}_x"] = x
+    for solver in ("cg", "bicgstab"):
+        st, it, res, x, _ = getattr(ref, solver)(rp, ci, v, b, np.zeros(n), 1e-8, 2000,
+                                                 precond=2)
+        out[f"{solver}_sor"] = np.array([st, it, res])
+        out[f"{solver}_sor_x"] = x
+    return out
+
+
 def main(only=None):
     ref = oracle.Reference()
     out = {}
-    if only == "setup":
-        out["setup"] = setup_case(ref)
+    if only in ("setup", "precond"):
+        out[only] = setup_case(ref) if only == "setup" else precond_case(ref)
         for name, case in out.items():
             path = os.path.join(HERE, f"{name}.npz")
             np.savez_compressed(path, **case)
@@ -148,6 +194,7 @@ def main(only=None):
                         axpyz=ref.axpyz(0.75, a, c))
 
     out["setup"] = setup_case(ref)
+    out["precond"] = precond_case(ref)
 
     for name, case in out.items():
         path = os.path.join(HERE, f"{name}.npz")

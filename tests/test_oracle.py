@@ -164,3 +164,107 @@ def test_setup_routines_match_reference_live(restatement, reference):
     assert all(np.array_equal(p, q) for p, q in zip(a, b))
     assert np.array_equal(restatement.coo_rowptr(900, a[0]),
                           reference.coo_rowptr(900, 700, *b))
+
+
+# ------------------------------------------------ SOR / IC(0) / ILU(0) ----
+def test_sor_matches_reference_golden(restatement):
+    """SOR create/apply_precond and SOR::solve of the restatement against
+    the reference build's outputs: identical bits (same loops, same order,
+    the backward sweep's double accumulator included); SOR-preconditioned
+    CG / BiCGSTAB: same status and iterations."""
+    g = golden("precond")
+    for tag in ("p3", "rnd"):
+        rp, ci, v, r = g[f"{tag}_rp"], g[f"{tag}_ci"], g[f"{tag}_v"], g[f"{tag}_r"]
+        assert np.array_equal(restatement.precond_apply(rp, ci, v, 2, r), g[f"{tag}_z_d"])
+        zs = restatement.precond_apply(rp, ci, v.astype(np.float32), 2, r.astype(np.float32))
+        assert np.array_equal(zs, g[f"{tag}_z_s"])
+    n, rp, ci, v = W.poisson2d(16)
+    b = np.ones(n)
+    for sfx, dt, tol in (("d", np.float64, 1e-8), ("s", np.float32, 1e-4)):
+        st, it, res, x = restatement.sor(rp, ci, v.astype(dt), b.astype(dt), np.zeros(n, dt),
+                                         tol, 5000)
+        want = g[f"sor_{sfx}"]
+        assert st == want[0] and it == want[1]
+        assert np.array_equal(x, g[f"sor_{sfx}_x"])
+    for solver in ("cg", "bicgstab"):
+        st, it, _, x = getattr(restatement, solver)(rp, ci, v, b, np.zeros(n), 1e-8, 2000,
+                                                    precond=2)
+        want = g[f"{solver}_sor"]
+        assert st == want[0] and it == want[1]
+        assert np.linalg.norm(x - g[f"{solver}_sor_x"]) < 1e-10 * np.linalg.norm(x)
+
+
+def test_sor_matches_reference_live(restatement, reference):
+    n, rp, ci, v = W.convdiff3d(9, peclet=5.0)
+    r = W.uniform_mt(n, -1.0, 1.0, 61)
+    for om in (1.0, 1.5, 1.9):
+        assert np.array_equal(restatement.precond_apply(rp, ci, v, 2, r, omega=om),
+                              reference.sor_apply(rp, ci, v, r, omega=om))
+    b = W.uniform_mt(n, -1.0, 1.0, 62)
+    a = restatement.sor(rp, ci, v, b, np.zeros(n), 1e-9, 3000, omega=1.2)
+    c = reference.sor(rp, ci, v, b, np.zeros(n), 1e-9, 3000, omega=1.2)
+    assert a[0] == c[0] and a[1] == c[1] and np.array_equal(a[3], c[3])
+
+
+def _dense(rp, ci, v):
+    n = len(rp) - 1
+    A = np.zeros((n, n))
+    for i in range(n):
+        A[i, ci[rp[i]:rp[i + 1]]] = v[rp[i]:rp[i + 1]]
+    return A
+
+
+def test_ilu0_ic0_defining_identities(restatement):
+    """The reference runs IC / ILU only through cuSPARSE csric02 /
+    csrilu02, so no reference output exists on the CPU: the restatement is
+    pinned by the identities that define the zero fill-in factorizations --
+    (L U)_ij = a_ij on A's pattern (ILU(0), L unit lower), (L L^T)_ij = a_ij
+    on A's lower pattern (IC(0)) -- and by the reference's own sparse IC /
+    ILU known-answer tests (test/equation/sparse_ic, sparse_ilu: tridiagonal
+    test/test.mtx and test2.mtx, where the factorization is exact)."""
+    rng = np.random.default_rng(8)
+    n, rp, ci, v = W.poisson2d(11, 9)
+    vn = v + rng.uniform(0.0, 0.4, len(v))  # nonsymmetric values, same pattern
+    f, piv = restatement.precond_factor(rp, ci, vn, 4)
+    assert piv == -1
+    F = _dense(rp, ci, f)
+    L, U = np.tril(F, -1) + np.eye(n), np.triu(F)
+    An = _dense(rp, ci, vn)
+    assert np.abs((L @ U - An)[An != 0]).max() < 1e-13
+    f, piv = restatement.precond_factor(rp, ci, v, 3)
+    assert piv == -1
+    L = np.tril(_dense(rp, ci, f))
+    A = _dense(rp, ci, v)
+    assert np.abs((L @ L.T - A)[np.tril(A) != 0]).max() < 1e-13
+    # apply solves the triangular systems exactly
+    r = rng.uniform(-1, 1, n)
+    z = restatement.precond_apply(rp, ci, v, 3, r)
+    assert np.abs(L @ (L.T @ z) - r).max() < 1e-12
+    Ln = np.tril(_dense(rp, ci, restatement.precond_factor(rp, ci, vn, 4)[0]), -1) + np.eye(n)
+    Un = np.triu(_dense(rp, ci, restatement.precond_factor(rp, ci, vn, 4)[0]))
+    z = restatement.precond_apply(rp, ci, vn, 4, r)
+    assert np.abs(Ln @ (Un @ z) - r).max() < 1e-12
+    # known answers: M^{-1} (A 1) = 1 on the reference's tridiagonal tests
+    rp3 = np.array([0, 2, 5, 7], np.int32)
+    ci3 = np.array([0, 1, 0, 1, 2, 1, 2], np.int32)
+    for vals, kinds in (([2, -1, -1, 2, -1, -1, 2.0], (3, 4)), ([2, 1, -1, 2, -1, 1, 2.0], (4,))):
+        v3 = np.array(vals)
+        b3 = _dense(rp3, ci3, v3) @ np.ones(3)
+        for kind in kinds:
+            assert np.allclose(restatement.precond_apply(rp3, ci3, v3, kind, b3), 1.0,
+                               rtol=0, atol=1e-15)
+
+
+def test_zero_pivots_and_unsorted_rows(restatement):
+    rp = np.array([0, 2, 3, 5], np.int32)
+    ci = np.array([0, 1, 0, 1, 2], np.int32)  # row 1 has no diagonal
+    v = np.array([2.0, 1.0, 1.0, 1.0, 3.0])
+    assert restatement.precond_factor(rp, ci, v, 4)[1] == 1
+    assert restatement.precond_factor(rp, ci, v, 3)[1] == 1
+    rp = np.array([0, 2, 4], np.int32)
+    ci = np.array([0, 1, 0, 1], np.int32)
+    v = np.ones(4)  # [[1, 1], [1, 1]]: u_11 = 0, and not positive definite
+    assert restatement.precond_factor(rp, ci, v, 4)[1] == 1
+    assert restatement.precond_factor(rp, ci, v, 3)[1] == 1
+    with pytest.raises(ValueError):
+        restatement.precond_factor(rp, np.array([1, 0, 0, 1], np.int32), v, 4)
