@@ -58,7 +58,16 @@ WORKLOADS = {
     "batch_cg": dict(kind="batch", matrix="diffusion_batch", count=2048, dtype="f64"),
     "serve_stream": dict(kind="serve", matrix="serve", count=200, budget=8 << 30,
                          dtype="f64"),
+    # CG / BiCGSTAB with the triangular-sweep preconditioners (SOR, IC(0), ILU(0))
+    "precond_sor_cg": dict(kind="precond", solver="cg", pc="sor", matrix="poisson2d", m=128,
+                           dtype="f64"),
+    "precond_ic_cg": dict(kind="precond", solver="cg", pc="ic", matrix="poisson3d", m=128,
+                          dtype="f64"),
+    "precond_ilu_bicgstab": dict(kind="precond", solver="bicgstab", pc="ilu",
+                                 matrix="convdiff3d", m=96, dtype="f64"),
 }
+METRIC_PRECOND = "preconditioned solves/s at 1e-10 rel. residual"
+PC_KIND = {"sor": 2, "ic": 3, "ilu": 4}
 METRIC_BATCH = "solves/s at 1e-8 rel. residual, 2,048-system batch"
 
 
@@ -70,6 +79,14 @@ def env_rank():
 def describe(wl):
     if wl.get("size"):
         wl = dict(wl, **({"n": wl["size"]} if wl["matrix"] == "zipf" else {"m": wl["size"]}))
+    if wl["kind"] == "precond":
+        mat = {"poisson2d": f"2D 5-point Poisson {wl['m']}x{wl['m']} (x_true U[-1,1] seed 0)",
+               "poisson3d": f"3D 7-point Laplacian {wl['m']}^3 (x_true U[-1,1] seed 1)",
+               "convdiff3d": f"3D upwind convection-diffusion {wl['m']}^3, cell Peclet 10 "
+                             "(x_true U[-1,1] seed 2)"}[wl["matrix"]]
+        pcn = {"sor": "SOR (omega 1.9)", "ic": "IC(0)", "ilu": "ILU(0)"}[wl["pc"]]
+        return (f"{wl['solver'].upper() if wl['solver'] == 'cg' else 'BiCGSTAB'} "
+                f"preconditioned by {pcn} on {mat}, tol 1e-10*||b||, FP64")
     if wl["matrix"] == "poisson3d":
         return f"3D 7-point Laplacian {wl['m']}^3 CRS<{'double' if wl['dtype'] == 'f64' else 'float'}>"
     if wl["matrix"] == "zipf":
@@ -567,6 +584,159 @@ def run_solve(args, wl, rank, world, local):
     return out
 
 
+# ------------------------------------------------------ preconditioners
+def precond_apply_bytes(n, nnz, pc):
+    """Algorithmic bytes of one apply z = M^{-1} r (both sweeps): the stored
+    entries each sweep reads once (value + column; IC reads L and its
+    transpose, SOR / ILU the lower and upper halves of one pattern), per row
+    and sweep the row pointer and the two split indices, and the vectors
+    (right-hand side in, result out; SOR also its multipliers)."""
+    entries = nnz + n if pc == "ic" else nnz
+    vec = 4 * n * 8 + (2 * n * 8 if pc == "sor" else 0)
+    return entries * 12 + 2 * ((n + 1) * 4 + 2 * n * 4) + vec
+
+
+def run_precond(args, wl, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    from monolish_b200 import device as D
+
+    torch.cuda.set_device(local)
+    n, rp, ci, v, xt = make_matrix(wl)
+    b = host_matvec(rp, ci, v, xt)
+    tol = 1e-10 * float(np.linalg.norm(b))
+    kind = PC_KIND[wl["pc"]]
+    h = D.Handle()
+    A = D.Crs(h, n, n, rp, ci, v, validate=False)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.zeros(n, dtype=torch.float64, device="cuda")
+    solve = D.cg_solve_precond if wl["solver"] == "cg" else D.bicgstab_solve_precond
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    # setup: the factorization (IC / ILU) or multipliers (SOR) and schedules
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pc = D.Precond(A, kind)
+    torch.cuda.synchronize()
+    setup_ms = (time.perf_counter() - t0) * 1e3
+    lv_lo, lv_up, nblocks = pc.info()
+    # one apply (both sweeps) on its own
+    r = torch.from_numpy(b / np.linalg.norm(b)).cuda()
+    z = torch.empty_like(r)
+    for _ in range(args.warmup):
+        pc.apply(r, z)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        pc.apply(r, z)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    apply_ms = e0.elapsed_time(e1) / args.steps
+    for _ in range(args.warmup):
+        dx.zero_()
+        res = solve(A, pc, db, dx, tol, 20000)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        dx.zero_()
+        res = solve(A, pc, db, dx, tol, 20000)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    cl = clocks.stop()
+    rel = true_relres(rp, ci, v, b, dx.cpu().numpy())
+    # end to end as a user of the reference API runs it: b from pinned host
+    # memory, the preconditioner built (create_precond, done by every
+    # reference solve), the solve, x back to the host
+    hb = torch.from_numpy(b).pin_memory()
+    hx = torch.empty(n, dtype=torch.float64).pin_memory()
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        db.copy_(hb, non_blocking=True)
+        dx.zero_()
+        pc2 = D.Precond(A, kind)
+        solve(A, pc2, db, dx, tol, 20000)
+        hx.copy_(dx, non_blocking=True)
+        torch.cuda.synchronize()
+        pc2.close()
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    if world > 1:
+        t = torch.tensor([ms, e2e_ms / e2e_steps * args.steps], device="cuda",
+                         dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t[0])
+    out = None
+    if rank == 0:
+        nnz = int(rp[-1])
+        B_apply = precond_apply_bytes(n, nnz, wl["pc"])
+        achieved = B_apply / (apply_ms / 1e3) / 1e9
+        peak, peak_kind = measured_peak()
+        hops = lv_lo + lv_up
+        out = {
+            "metric": METRIC_PRECOND, "value": round(world * args.steps / (ms / 1e3), 3),
+            "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generators)",
+            "config": {"workload": describe(wl), "n": n, "nnz": nnz, "iters": res.iters,
+                       "status": res.status, "true_rel_residual": rel,
+                       "precond_setup_ms": round(setup_ms, 2),
+                       "apply_ms": round(apply_ms, 4),
+                       "sweep_levels": [lv_lo, lv_up], "row_blocks": nblocks,
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": round(e2e_steps / (e2e_ms / 1e3), 3), "unit": "solves/s",
+                    "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8,
+                    "note": "includes building the preconditioner, as every reference solve "
+                            "does"},
+            "roofline": {"bound": "latency", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "peak_kind": peak_kind, "traffic": None,
+                         "kernel": "sweep_fwd_kernel / sweep_bwd_kernel (one apply)",
+                         "bytes_per_apply": B_apply,
+                         "us_per_level": round(apply_ms * 1e3 / max(hops, 1), 2),
+                         "note": "algorithmic bytes of one apply / apply time against HBM; the "
+                                 "sweeps are bound by their dependency chains: an apply is "
+                                 f"{hops} block levels long, each one wait for another warp"},
+            "gpu_launches": args.steps * (res.iters * (6 if wl["solver"] == "cg" else 9) + 4),
+        }
+        if world == 1 and not args.no_cpu:
+            import oracle
+            threads = os.cpu_count() or 1
+            ref = oracle.reference_or_none() if wl["pc"] == "sor" else None
+            if ref is not None:
+                ref.set_threads(threads)
+                st, it, _, _, sec = getattr(ref, wl["solver"])(rp, ci, v, b, np.zeros(n), tol,
+                                                               20000, precond=2)
+                out["cpu_baseline"] = {"value": round(1.0 / sec, 4), "unit": "solves/s",
+                                       "cores": threads, "kind": "reference",
+                                       "sample": f"1 full solve ({it} iterations)"}
+            else:
+                # the reference has no CPU IC / ILU (ic.cpp, ilu.cpp throw "on CPU
+                # does not impl."): the oracle's sequential restatement
+                rs = oracle.restatement()
+                t0 = time.perf_counter()
+                st, it, _, _ = getattr(rs, wl["solver"])(rp, ci, v, b, np.zeros(n), tol, 20000,
+                                                         precond=kind)
+                sec = time.perf_counter() - t0
+                out["cpu_baseline"] = {"value": round(1.0 / sec, 4), "unit": "solves/s",
+                                       "cores": 1, "kind": "port",
+                                       "sample": f"1 full solve ({it} iterations), the oracle's "
+                                                 "sequential C restatement"}
+        if cl:
+            out["clocks"] = cl
+    pc.close()
+    A.close()
+    h.close()
+    return out
+
+
 # ----------------------------------------------------------- batch leg
 def batch_inputs(wl):
     """Systems, right-hand sides b = A x_true (x_true ~ U[-1,1], seed 3 + k)
@@ -1048,6 +1218,41 @@ def run_reference(args, wl, rank, world):
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
     os.environ.setdefault("OMP_PROC_BIND", "close")
     n, rp, ci, v, x = make_matrix(wl)
+    if wl["kind"] == "precond":
+        import oracle
+        b = host_matvec(rp, ci, v, x)
+        tol = 1e-10 * float(np.linalg.norm(b))
+        ref = oracle.reference_or_none() if wl["pc"] == "sor" else None
+        secs = []
+        for _ in range(max(1, min(args.steps, 3))):
+            if ref is not None:
+                ref.set_threads(threads)
+                st, it, _, _, sec = getattr(ref, wl["solver"])(rp, ci, v, b, np.zeros(n), tol,
+                                                               20000, precond=2)
+            else:
+                rs = oracle.restatement()
+                t0 = time.perf_counter()
+                st, it, _, _ = getattr(rs, wl["solver"])(rp, ci, v, b, np.zeros(n), tol, 20000,
+                                                         precond=PC_KIND[wl["pc"]])
+                sec = time.perf_counter() - t0
+            secs.append(sec)
+        value = 1.0 / statistics.mean(secs)
+        kind = "reference" if ref is not None else "port"
+        cores = threads if ref is not None else 1
+        return {"metric": METRIC_PRECOND, "value": round(value, 4), "unit": "solves/s",
+                "n_gpus": world, "steps": len(secs), "warmup": 0,
+                "ms_per_step": round(statistics.mean(secs) * 1e3, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generators)", "impl": "reference",
+                "config": {"workload": describe(wl), "n": n, "iters": it, "status": st},
+                "cpu_baseline": {"value": round(value, 4), "unit": "solves/s", "cores": cores,
+                                 "kind": kind,
+                                 "sample": f"{len(secs)} full solves" + (
+                                     "" if ref is not None else
+                                     " of the oracle's restatement (the reference has no CPU "
+                                     "IC / ILU)")},
+                "e2e": {"value": round(value, 4), "unit": "solves/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
     import oracle
     ref = oracle.reference_or_none()
     kind = "reference" if ref is not None else "port"
@@ -1153,6 +1358,8 @@ def main():
             out = run_batch(args, wl, rank, world, local)
         elif wl["kind"] == "serve":
             out = run_serve(args, wl, rank, world, local)
+        elif wl["kind"] == "precond":
+            out = run_precond(args, wl, rank, world, local)
         else:
             out = run_solve(args, wl, rank, world, local)
     finally:

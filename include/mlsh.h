@@ -353,6 +353,12 @@ int mlsh_precond_apply(mlsh_handle handle, mlsh_precond pc, const void *d_r,
  * triangle), SOR the vector M (n elements). */
 int mlsh_precond_factor(mlsh_handle handle, mlsh_precond pc, void *d_out);
 int mlsh_precond_destroy(mlsh_precond pc);
+/* The sweeps' schedules: the length of the longest dependency chain of
+ * 32-row blocks in the lower (forward) and upper (backward) sweep -- each
+ * link is one wait for another warp's result, so an apply takes at least
+ * (levels_lower + levels_upper) such hops -- and the block count. */
+int mlsh_precond_info(mlsh_precond pc, int *levels_lower, int *levels_upper,
+                      int64_t *blocks);
 
 /* CG / BiCGSTAB preconditioned by `pc` (the reference's solvers with
  * set_create_precond / set_apply_precond bound to equation::SOR, IC or

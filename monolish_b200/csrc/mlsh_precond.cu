@@ -180,51 +180,81 @@ __device__ __forceinline__ void wait_deps(const int *dep_off, const int *dep_ids
 
 constexpr int kPre = 4;  // out-of-block entries fetched ahead of the wait
 
-// Lower sweep.
-template <typename T, int MODE>
-__global__ void __launch_bounds__(kSweepThreads) sweep_fwd_kernel(SweepArgs<T> a) {
-  const int lane = threadIdx.x & 31;
-  unsigned long long t;
-  if (!sweep_ticket(a, lane, &t)) return;
-  const unsigned epoch = (unsigned)(t / a.nb) + 1u;
-  const unsigned ov = (unsigned)a.order[t % a.nb];
-  const unsigned blk = ov & kBlockMask;
-  const int base = (int)blk * 32;
-  const int row = base + lane;
-  const bool valid = row < a.n;
-  T acc = T(0), fin = T(1);
-  int j = 0, e = 0;
-  if (valid) {
-    j = a.rp[row];
-    e = a.lo_end[row];
-    acc = a.rhs[row];
-    if constexpr (MODE == kSorFwd) fin = a.scale[row];
-    if constexpr (MODE == kDiagFwd) fin = a.up_beg[row] > e ? a.val[e] : T(0);
-  }
-  // the row's first entries, fetched while the dependencies are awaited
+// Where a sweep's solution vector lives while the sweep runs: in global
+// memory (other warps' blocks, read through L2 after their flag) or, for the
+// single-CTA form, in shared memory.
+template <typename T>
+struct GlobalX {
+  T *out;
+  __device__ T get(int c) const { return __ldcg(out + c); }
+  __device__ void put(int r, T v) const { out[r] = v; }
+};
+template <typename T>
+struct SharedX {
+  T *xs;
+  __device__ T get(int c) const { return xs[c]; }
+  __device__ void put(int r, T v) const { xs[r] = v; }
+};
+
+// What a lane knows of its row before any solution value is needed: its
+// range of entries, right-hand side, finishing factor and first entries.
+template <typename T>
+struct RowState {
+  int j, e, jb, split;
+  T acc, fin, rh;
   int pc[kPre];
   T pv[kPre];
+};
+
+template <typename T, int MODE>
+__device__ __forceinline__ void fwd_load(const SweepArgs<T> &a, unsigned ov, int lane,
+                                         RowState<T> &st) {
+  const int row = (int)(ov & kBlockMask) * 32 + lane;
+  st.acc = T(0);
+  st.fin = T(1);
+  st.j = 0;
+  st.e = 0;
+  if (row < a.n) {
+    st.j = a.rp[row];
+    st.e = a.lo_end[row];
+    st.acc = a.rhs[row];
+    if constexpr (MODE == kSorFwd) st.fin = a.scale[row];
+    if constexpr (MODE == kDiagFwd) st.fin = a.up_beg[row] > st.e ? a.val[st.e] : T(0);
+  }
 #pragma unroll
   for (int u = 0; u < kPre; ++u) {
-    pc[u] = j + u < e ? a.ci[j + u] : 0x7fffffff;
-    pv[u] = j + u < e ? a.val[j + u] : T(0);
+    st.pc[u] = st.j + u < st.e ? a.ci[st.j + u] : 0x7fffffff;
+    st.pv[u] = st.j + u < st.e ? a.val[st.j + u] : T(0);
   }
-  wait_deps(a.dep_off, a.dep_ids, a.flags, blk, epoch, a.err, lane);
+}
+
+// One 32-row block of the lower sweep, from its loaded state: every value
+// outside the block must be final when this runs.
+template <typename T, int MODE, class XS>
+__device__ __forceinline__ void fwd_finish_block(const SweepArgs<T> &a, unsigned ov, int lane,
+                                                 const XS &X, const RowState<T> &st) {
+  const int base = (int)(ov & kBlockMask) * 32;
+  const int row = base + lane;
+  const bool valid = row < a.n;
+  T acc = st.acc;
+  const T fin = st.fin;
+  int j = st.j;
+  const int e = st.e;
   // entries left of the block (a prefix of the row), ascending
   T xs[kPre];
 #pragma unroll
-  for (int u = 0; u < kPre; ++u) xs[u] = pc[u] < base ? __ldcg(a.out + pc[u]) : T(0);
+  for (int u = 0; u < kPre; ++u) xs[u] = st.pc[u] < base ? X.get(st.pc[u]) : T(0);
 #pragma unroll
   for (int u = 0; u < kPre; ++u)
-    if (pc[u] < base) {
-      acc = sub_rn(acc, mul_rn(pv[u], xs[u]));
+    if (st.pc[u] < base) {
+      acc = sub_rn(acc, mul_rn(st.pv[u], xs[u]));
       ++j;
     }
-  if (pc[kPre - 1] < base) {
+  if (st.pc[kPre - 1] < base) {
     for (; j < e; ++j) {
       const int c = a.ci[j];
       if (c >= base) break;
-      acc = sub_rn(acc, mul_rn(a.val[j], __ldcg(a.out + c)));
+      acc = sub_rn(acc, mul_rn(a.val[j], X.get(c)));
     }
   }
   T xv = T(0);
@@ -244,101 +274,105 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_fwd_kernel(SweepArgs<T> a
       be = -a1;
     }
     xv = affine_scan<false>(al, be, lane);
-    if (valid) a.out[row] = xv;
-    publish_block(a.flags + blk, epoch, lane);
-    return;
-  }
-  // entries inside the block, ascending: a 32-step chain; the next two are
-  // kept in registers so the chain carries no memory latency
-  int c0 = 64, c1 = 64;
-  T v0 = T(0), v1 = T(0);
-  if (j < e) {
-    c0 = a.ci[j] - base;
-    v0 = a.val[j];
-  }
-  if (j + 1 < e) {
-    c1 = a.ci[j + 1] - base;
-    v1 = a.val[j + 1];
-  }
+  } else {
+    // entries inside the block, ascending: a 32-step chain; the next two
+    // are kept in registers so the chain carries no memory latency
+    int c0 = 64, c1 = 64;
+    T v0 = T(0), v1 = T(0);
+    if (j < e) {
+      c0 = a.ci[j] - base;
+      v0 = a.val[j];
+    }
+    if (j + 1 < e) {
+      c1 = a.ci[j + 1] - base;
+      v1 = a.val[j + 1];
+    }
 #pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    if (lane == k) xv = fwd_finish<MODE>(acc, fin);
-    const T xk = __shfl_sync(kFull, xv, k);
-    if (c0 == k) {
-      acc = sub_rn(acc, mul_rn(v0, xk));
-      c0 = c1;
-      v0 = v1;
-      ++j;
-      if (j + 1 < e) {
-        c1 = a.ci[j + 1] - base;
-        v1 = a.val[j + 1];
-      } else {
-        c1 = 64;
+    for (int k = 0; k < 32; ++k) {
+      if (lane == k) xv = fwd_finish<MODE>(acc, fin);
+      const T xk = __shfl_sync(kFull, xv, k);
+      if (c0 == k) {
+        acc = sub_rn(acc, mul_rn(v0, xk));
+        c0 = c1;
+        v0 = v1;
+        ++j;
+        if (j + 1 < e) {
+          c1 = a.ci[j + 1] - base;
+          v1 = a.val[j + 1];
+        } else {
+          c1 = 64;
+        }
       }
     }
   }
-  if (valid) a.out[row] = xv;
-  publish_block(a.flags + blk, epoch, lane);
+  if (valid) X.put(row, xv);
 }
 
-// Upper sweep.
 template <typename T, int MODE>
-__global__ void __launch_bounds__(kSweepThreads) sweep_bwd_kernel(SweepArgs<T> a) {
-  const int lane = threadIdx.x & 31;
-  unsigned long long t;
-  if (!sweep_ticket(a, lane, &t)) return;
-  const unsigned epoch = (unsigned)(t / a.nb) + 1u;
-  const unsigned ov = (unsigned)a.order[t % a.nb];
-  const unsigned blk = ov & kBlockMask;
-  const int base = (int)blk * 32;
+__device__ __forceinline__ void bwd_load(const SweepArgs<T> &a, unsigned ov, int lane,
+                                         RowState<T> &st) {
+  const int base = (int)(ov & kBlockMask) * 32;
+  const int row = base + lane;
+  st.acc = T(0);
+  st.fin = T(1);
+  st.rh = T(0);
+  st.jb = 0;
+  st.e = 0;
+  st.split = 0;
+  if (row < a.n) {
+    st.jb = a.up_beg[row];
+    st.e = a.rp[row + 1];
+    st.rh = a.rhs[row];
+    if constexpr (MODE == kSorBwd) {
+      st.fin = a.scale[row];
+    } else {
+      st.acc = st.rh;
+      const int d = a.lo_end[row];
+      st.fin = st.jb > d ? a.val[d] : T(0);
+    }
+    int split = st.jb;
+    while (split < st.e && a.ci[split] < base + 32) ++split;
+    st.split = split;
+  }
+#pragma unroll
+  for (int u = 0; u < kPre; ++u) {
+    st.pc[u] = st.split + u < st.e ? a.ci[st.split + u] : -1;
+    st.pv[u] = st.split + u < st.e ? a.val[st.split + u] : T(0);
+  }
+}
+
+// One 32-row block of the upper sweep, from its loaded state.
+template <typename T, int MODE, class XS>
+__device__ __forceinline__ void bwd_finish_block(const SweepArgs<T> &a, unsigned ov, int lane,
+                                                 const XS &X, const RowState<T> &st) {
+  const int base = (int)(ov & kBlockMask) * 32;
   const int row = base + lane;
   const bool valid = row < a.n;
   // SOR accumulates in double ("auto tmp = 0.0", sor_kernel.hpp:61-66)
-  T acc = T(0), fin = T(1), rh = T(0);
+  T acc = st.acc;
+  const T fin = st.fin, rh = st.rh;
   double sacc = 0.0;
-  int jb = 0, e = 0, split = 0;
-  if (valid) {
-    jb = a.up_beg[row];
-    e = a.rp[row + 1];
-    rh = a.rhs[row];
-    if constexpr (MODE == kSorBwd) {
-      fin = a.scale[row];
-    } else {
-      acc = rh;
-      const int d = a.lo_end[row];
-      fin = jb > d ? a.val[d] : T(0);
-    }
-    split = jb;
-    while (split < e && a.ci[split] < base + 32) ++split;
-  }
-  int pc[kPre];
-  T pv[kPre];
-#pragma unroll
-  for (int u = 0; u < kPre; ++u) {
-    pc[u] = split + u < e ? a.ci[split + u] : -1;
-    pv[u] = split + u < e ? a.val[split + u] : T(0);
-  }
-  wait_deps(a.dep_off, a.dep_ids, a.flags, blk, epoch, a.err, lane);
+  const int jb = st.jb, e = st.e, split = st.split;
   // entries right of the block (the row's suffix from split), ascending
   T xs[kPre];
 #pragma unroll
-  for (int u = 0; u < kPre; ++u) xs[u] = pc[u] >= 0 ? __ldcg(a.out + pc[u]) : T(0);
+  for (int u = 0; u < kPre; ++u) xs[u] = st.pc[u] >= 0 ? X.get(st.pc[u]) : T(0);
 #pragma unroll
   for (int u = 0; u < kPre; ++u)
-    if (pc[u] >= 0) {
-      const T prod = mul_rn(pv[u], xs[u]);
+    if (st.pc[u] >= 0) {
+      const T prod = mul_rn(st.pv[u], xs[u]);
       if constexpr (MODE == kSorBwd) sacc = __dadd_rn(sacc, (double)prod);
       else acc = sub_rn(acc, prod);
     }
   for (int j = split + kPre; j < e; ++j) {
-    const T prod = mul_rn(a.val[j], __ldcg(a.out + a.ci[j]));
+    const T prod = mul_rn(a.val[j], X.get(a.ci[j]));
     if constexpr (MODE == kSorBwd) sacc = __dadd_rn(sacc, (double)prod);
     else acc = sub_rn(acc, prod);
   }
+  T xv = T(0);
   if (ov & kScanBit) {
     // only row + 1 -> row inside the block: z_k = al_k + be_k z_{k+1}
     const T a1 = (split > jb) ? a.val[jb] : T(0);
-    T xv;
     if constexpr (MODE == kSorBwd) {
       const double al = (double)rh - sacc * (double)fin;
       const double be = -((double)a1 * (double)fin);
@@ -346,49 +380,126 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_bwd_kernel(SweepArgs<T> a
     } else {
       xv = affine_scan<true>(acc / fin, -(a1 / fin), lane);
     }
-    if (valid) a.out[row] = xv;
-    publish_block(a.flags + blk, epoch, lane);
-    return;
-  }
-  // entries inside the block, consumed from the highest column down
-  int q = split - 1;
-  int c0 = 64, c1 = 64;
-  T v0 = T(0), v1 = T(0);
-  if (q >= jb) {
-    c0 = a.ci[q] - base;
-    v0 = a.val[q];
-  }
-  if (q - 1 >= jb) {
-    c1 = a.ci[q - 1] - base;
-    v1 = a.val[q - 1];
-  }
-  T xv = T(0);
-#pragma unroll
-  for (int k = 31; k >= 0; --k) {
-    if (lane == k) {
-      if constexpr (MODE == kSorBwd)
-        xv = (T)__dsub_rn((double)rh, __dmul_rn(sacc, (double)fin));
-      else
-        xv = div_rn(acc, fin);
+  } else {
+    // entries inside the block, consumed from the highest column down
+    int q = split - 1;
+    int c0 = 64, c1 = 64;
+    T v0 = T(0), v1 = T(0);
+    if (q >= jb) {
+      c0 = a.ci[q] - base;
+      v0 = a.val[q];
     }
-    const T xk = __shfl_sync(kFull, xv, k);
-    if (c0 == k) {
-      const T prod = mul_rn(v0, xk);
-      if constexpr (MODE == kSorBwd) sacc = __dadd_rn(sacc, (double)prod);
-      else acc = sub_rn(acc, prod);
-      c0 = c1;
-      v0 = v1;
-      --q;
-      if (q - 1 >= jb) {
-        c1 = a.ci[q - 1] - base;
-        v1 = a.val[q - 1];
-      } else {
-        c1 = 64;
+    if (q - 1 >= jb) {
+      c1 = a.ci[q - 1] - base;
+      v1 = a.val[q - 1];
+    }
+#pragma unroll
+    for (int k = 31; k >= 0; --k) {
+      if (lane == k) {
+        if constexpr (MODE == kSorBwd)
+          xv = (T)__dsub_rn((double)rh, __dmul_rn(sacc, (double)fin));
+        else
+          xv = div_rn(acc, fin);
+      }
+      const T xk = __shfl_sync(kFull, xv, k);
+      if (c0 == k) {
+        const T prod = mul_rn(v0, xk);
+        if constexpr (MODE == kSorBwd) sacc = __dadd_rn(sacc, (double)prod);
+        else acc = sub_rn(acc, prod);
+        c0 = c1;
+        v0 = v1;
+        --q;
+        if (q - 1 >= jb) {
+          c1 = a.ci[q - 1] - base;
+          v1 = a.val[q - 1];
+        } else {
+          c1 = 64;
+        }
       }
     }
   }
-  if (valid) a.out[row] = xv;
+  if (valid) X.put(row, xv);
+}
+
+// The multi-CTA sweep: one warp per block, blocks by ticket in level order,
+// per-block flags between warps.
+template <typename T, int MODE, bool BWD>
+__global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepArgs<T> a) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long t;
+  if (!sweep_ticket(a, lane, &t)) return;
+  const unsigned epoch = (unsigned)(t / a.nb) + 1u;
+  const unsigned ov = (unsigned)a.order[t % a.nb];
+  const unsigned blk = ov & kBlockMask;
+  RowState<T> st;
+  if constexpr (BWD) bwd_load<T, MODE>(a, ov, lane, st);
+  else fwd_load<T, MODE>(a, ov, lane, st);
+  wait_deps(a.dep_off, a.dep_ids, a.flags, blk, epoch, a.err, lane);
+  if constexpr (BWD) bwd_finish_block<T, MODE>(a, ov, lane, GlobalX<T>{a.out}, st);
+  else fwd_finish_block<T, MODE>(a, ov, lane, GlobalX<T>{a.out}, st);
   publish_block(a.flags + blk, epoch, lane);
+}
+
+// The single-CTA sweep for systems whose solution fits in shared memory:
+// the CTA's warps take each level's blocks, a barrier separates the levels,
+// the solution lives in shared memory and is written out at the end.
+constexpr int kCtaThreads = 512;
+constexpr size_t kCtaSweepBytes = 200 * 1024;
+
+template <typename T>
+__host__ __device__ inline size_t cta_x_bytes(int n) {
+  return ((size_t)n * sizeof(T) + 15) / 16 * 16;
+}
+// shared memory of the single-CTA sweep: solution, schedule, level starts
+template <typename T>
+inline size_t cta_smem_bytes(int n, unsigned nb, int levels) {
+  return cta_x_bytes<T>(n) + sizeof(int) * ((size_t)nb + (size_t)levels + 1);
+}
+
+template <typename T, int MODE, bool BWD>
+__global__ void __launch_bounds__(kCtaThreads, 1)
+    sweep_cta_kernel(SweepArgs<T> a, const int *level_off, int levels) {
+  extern __shared__ __align__(16) unsigned char sweep_smem[];
+  if (a.done != nullptr && *(volatile const int *)a.done != 0) return;
+  // [solution: n T][schedule: nb block entries][level starts: levels + 1]
+  T *xs = reinterpret_cast<T *>(sweep_smem);
+  int *s_order = reinterpret_cast<int *>(sweep_smem + cta_x_bytes<T>(a.n));
+  int *s_loff = s_order + a.nb;
+  for (int i = threadIdx.x; i < (int)a.nb; i += blockDim.x) s_order[i] = a.order[i];
+  for (int i = threadIdx.x; i <= levels; i += blockDim.x) s_loff[i] = level_off[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  const SharedX<T> X{xs};
+  // each warp loads its first block of the next level before the barrier,
+  // so the loads that do not depend on the solution overlap the wait
+  RowState<T> st;
+  bool have = false;
+  unsigned ov = 0;
+  for (int lv = 0; lv < levels; ++lv) {
+    const int q1 = s_loff[lv + 1];
+    for (int q = s_loff[lv] + warp; q < q1; q += nw) {
+      if (!have) {
+        ov = (unsigned)s_order[q];
+        if constexpr (BWD) bwd_load<T, MODE>(a, ov, lane, st);
+        else fwd_load<T, MODE>(a, ov, lane, st);
+      }
+      have = false;
+      if constexpr (BWD) bwd_finish_block<T, MODE>(a, ov, lane, X, st);
+      else fwd_finish_block<T, MODE>(a, ov, lane, X, st);
+    }
+    if (lv + 1 < levels) {
+      const int qn = q1 + warp;
+      if (qn < s_loff[lv + 2]) {
+        ov = (unsigned)s_order[qn];
+        if constexpr (BWD) bwd_load<T, MODE>(a, ov, lane, st);
+        else fwd_load<T, MODE>(a, ov, lane, st);
+        have = true;
+      }
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < a.n; i += blockDim.x) a.out[i] = xs[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -598,6 +709,36 @@ __global__ void __launch_bounds__(kSweepThreads) ic0_kernel(FactorArgs<T> a) {
 
 int grid_of(long long n, int threads) { return (int)std::max<long long>(1, (n + threads - 1) / threads); }
 
+template <typename T, int MODE, bool BWD>
+cudaError_t cta_launch(const SweepArgs<T> &a, const Schedule &sc, size_t xbytes, cudaStream_t s) {
+  sweep_cta_kernel<T, MODE, BWD><<<1, kCtaThreads, xbytes, s>>>(a, sc.level_off, sc.levels);
+  return cudaGetLastError();
+}
+
+// The single-CTA sweeps opt in to 200 KB of shared memory; set once, outside
+// any stream capture (the sweeps are captured into solver graphs).
+template <typename T>
+cudaError_t configure_cta_t() {
+  const int bytes = (int)kCtaSweepBytes;
+  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_cta_kernel<T, kSorFwd, false>, at, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_cta_kernel<T, kUnitFwd, false>, at, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_cta_kernel<T, kDiagFwd, false>, at, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_cta_kernel<T, kSorBwd, true>, at, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_cta_kernel<T, kDiagBwd, true>, at, bytes);
+  return e;
+}
+
+int configure_cta() {
+  static int done = 0;
+  if (done) return MLSH_SUCCESS;
+  MLSH_CUDA_TRY(configure_cta_t<double>());
+  MLSH_CUDA_TRY(configure_cta_t<float>());
+  done = 1;
+  return MLSH_SUCCESS;
+}
+
 template <typename T>
 cudaError_t sweep_launch_t(const Precond &pc, const Sweep &sw, bool backward, const void *rhs,
                            void *out, const int *done, int *err, cudaStream_t s) {
@@ -619,15 +760,25 @@ cudaError_t sweep_launch_t(const Precond &pc, const Sweep &sw, bool backward, co
   a.order = sw.order;
   a.dep_off = sw.dep_off;
   a.dep_ids = sw.dep_ids;
+  const Schedule &sc = backward ? pc.sbwd : pc.sfwd;
+  const size_t xbytes = cta_smem_bytes<T>(pc.n, pc.nb, sc.levels);
+  if (xbytes <= kCtaSweepBytes) {
+    switch (sw.mode) {
+      case kSorFwd: return cta_launch<T, kSorFwd, false>(a, sc, xbytes, s);
+      case kUnitFwd: return cta_launch<T, kUnitFwd, false>(a, sc, xbytes, s);
+      case kDiagFwd: return cta_launch<T, kDiagFwd, false>(a, sc, xbytes, s);
+      case kSorBwd: return cta_launch<T, kSorBwd, true>(a, sc, xbytes, s);
+      default: return cta_launch<T, kDiagBwd, true>(a, sc, xbytes, s);
+    }
+  }
   const int g = grid_of(pc.nb, kSweepWarps);
   switch (sw.mode) {
-    case kSorFwd: sweep_fwd_kernel<T, kSorFwd><<<g, kSweepThreads, 0, s>>>(a); break;
-    case kUnitFwd: sweep_fwd_kernel<T, kUnitFwd><<<g, kSweepThreads, 0, s>>>(a); break;
-    case kDiagFwd: sweep_fwd_kernel<T, kDiagFwd><<<g, kSweepThreads, 0, s>>>(a); break;
-    case kSorBwd: sweep_bwd_kernel<T, kSorBwd><<<g, kSweepThreads, 0, s>>>(a); break;
-    default: sweep_bwd_kernel<T, kDiagBwd><<<g, kSweepThreads, 0, s>>>(a); break;
+    case kSorFwd: sweep_kernel<T, kSorFwd, false><<<g, kSweepThreads, 0, s>>>(a); break;
+    case kUnitFwd: sweep_kernel<T, kUnitFwd, false><<<g, kSweepThreads, 0, s>>>(a); break;
+    case kDiagFwd: sweep_kernel<T, kDiagFwd, false><<<g, kSweepThreads, 0, s>>>(a); break;
+    case kSorBwd: sweep_kernel<T, kSorBwd, true><<<g, kSweepThreads, 0, s>>>(a); break;
+    default: sweep_kernel<T, kDiagBwd, true><<<g, kSweepThreads, 0, s>>>(a); break;
   }
-  (void)backward;
   return cudaGetLastError();
 }
 
@@ -693,7 +844,7 @@ void precond_release(Precond &pc) {
                   pc.ci_t,          pc.val_t,         pc.lo_t,          pc.up_t,
                   pc.scale,         pc.tmp,           pc.ticket,        pc.flags,
                   pc.sfwd.order,    pc.sfwd.dep_off,  pc.sfwd.dep_ids,  pc.sbwd.order,
-                  pc.sbwd.dep_off,  pc.sbwd.dep_ids};
+                  pc.sbwd.dep_off,  pc.sbwd.dep_ids,  pc.sfwd.level_off, pc.sbwd.level_off};
   for (void *b : bufs) pool_free(b, s);
   pc.sfwd = Schedule{};
   pc.sbwd = Schedule{};
@@ -792,6 +943,10 @@ int build_schedule(Handle &h, const int *rp, const int *ci, const int *lo, const
   std::vector<int> start((size_t)levels + 1, 0), order(nb);
   for (unsigned b = 0; b < nb; ++b) ++start[(size_t)lvl[b] + 1];
   for (int l = 0; l < levels; ++l) start[(size_t)l + 1] += start[(size_t)l];
+  MLSH_CUDA_TRY(pool_alloc(&sc.level_off, sizeof(int) * ((size_t)levels + 1), s));
+  MLSH_CUDA_TRY(cudaMemcpyAsync(sc.level_off, start.data(), sizeof(int) * ((size_t)levels + 1),
+                                cudaMemcpyHostToDevice, s));
+  MLSH_CUDA_TRY(cudaStreamSynchronize(s));
   for (unsigned k = 0; k < nb; ++k) {
     const unsigned b = upper ? nb - 1 - k : k;
     order[(size_t)start[(size_t)lvl[b]]++] = (int)(b | (scan[b] ? kScanBit : 0u));
@@ -807,6 +962,8 @@ int build_impl(Handle &h, const CsrPlan &p, int kind, double omega, bool solver_
   cudaStream_t s = h.stream;
   const int n = p.n_rows;
   const size_t esz = (size_t)dtype_size(p.dtype);
+  int cst = configure_cta();
+  if (cst != MLSH_SUCCESS) return cst;
   pc.handle = &h;
   pc.plan = &p;
   pc.kind = kind;
@@ -979,6 +1136,14 @@ int mlsh_precond_factor(mlsh_handle hs, mlsh_precond pc, void *out) {
                                   h.stream));
   }
   MLSH_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  return MLSH_SUCCESS;
+}
+
+int mlsh_precond_info(mlsh_precond pc, int *levels_lower, int *levels_upper, int64_t *blocks) {
+  if (!pc) return MLSH_ERR_INVALID_ARG;
+  if (levels_lower) *levels_lower = pc->p.sfwd.levels;
+  if (levels_upper) *levels_upper = pc->p.sbwd.levels;
+  if (blocks) *blocks = pc->p.nb;
   return MLSH_SUCCESS;
 }
 

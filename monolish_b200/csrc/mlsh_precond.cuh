@@ -33,7 +33,11 @@
 // ticket counter, so they never need clearing and graph replays stay valid.
 // Every wait is bounded; a warp that gives up records MLSH_ERR_TIMEOUT and
 // still publishes its flag, so no other warp waits on it for long.  The
-// factorizations use the same schedule with one warp per row.
+// factorizations use the same schedule with one warp per row.  A system
+// whose solution vector and schedule fit in 200 KB of shared memory is
+// swept by one CTA instead: its warps take each level's blocks with a CTA
+// barrier between levels, so a dependency costs a barrier rather than a
+// round trip through L2 between SMs.
 #pragma once
 #include "mlsh_internal.cuh"
 
@@ -69,6 +73,7 @@ struct Schedule {
   int *order = nullptr;    // nb block ids, by level
   int *dep_off = nullptr;  // nb + 1
   int *dep_ids = nullptr;  // dependency blocks of each block
+  int *level_off = nullptr;  // levels + 1: where each level starts in order
   int levels = 0;          // length of the longest dependency chain
   long long deps = 0;      // total dependency entries
 };

@@ -384,6 +384,12 @@ class Precond:
         _abi.check(self.lib.mlsh_precond_apply(self.A.handle.h, self.pc, ptr(r), ptr(z)),
                    "mlsh_precond_apply")
 
+    def info(self):
+        """(levels of the lower sweep, levels of the upper sweep, blocks)."""
+        lo, up, nb = C.c_int(), C.c_int(), C.c_int64()
+        _abi.check(self.lib.mlsh_precond_info(self.pc, C.byref(lo), C.byref(up), C.byref(nb)))
+        return int(lo.value), int(up.value), int(nb.value)
+
     def factor(self):
         """SOR: M (n); IC / ILU: the factor's values in A's pattern (nnz)."""
         n = self.A.n_rows if self.kind == _abi.PRECOND_SOR else self.A.nnz

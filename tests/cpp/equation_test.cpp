@@ -110,16 +110,21 @@ int main(int argc, char **argv) {
       f, 1e-8, "BiCGSTAB IC d");
   ok &= run<double, equation::BiCGSTAB<CD, double>, equation::ILU<CD, double>>(
       f, 1e-8, "BiCGSTAB ILU d");
-  ok &= run<float, equation::BiCGSTAB<CF, float>, equation::ILU<CF, float>>(
-      f, 1e-4, "BiCGSTAB ILU f");
+  // on the 3x3 tridiagonal matrix ILU(0) is exact: in FP32 the first s =
+  // r - alpha v is exactly 0 and omega = (t,s)/(t,t) = 0/0, so the
+  // reference's recurrence (bicgstab.cpp:91-102) ends with a NaN residual
+  // there; the case runs on the larger matrix only
+  const bool tridiag3 = matrix::COO<double>(f).get_row() == 3;
+  if (!tridiag3)
+    ok &= run<float, equation::BiCGSTAB<CF, float>, equation::ILU<CF, float>>(
+        f, 1e-4, "BiCGSTAB ILU f");
   // the SOR iteration itself (test/equation/iterative/sor.cpp); its test is
   // relative, so x is checked at the accuracy that implies here
   ok &= run<double, equation::SOR<CD, double>, equation::none<CD, double>>(f, 1e-8, "SOR d",
                                                                             1e-5);
   ok &= run<float, equation::SOR<CF, float>, equation::none<CF, float>>(f, 1e-4, "SOR f", 1e-2);
   if (monolish::util::build_with_gpu()) {
-    matrix::COO<double> probe(f);
-    if (probe.get_row() == 3) {  // the reference's tridiagonal test matrix
+    if (tridiag3) {  // the reference's tridiagonal test matrix
       ok &= run_direct<double, equation::IC<CD, double>>(f, 1e-8, "IC solve d");
       ok &= run_direct<float, equation::IC<CF, float>>(f, 1e-5, "IC solve f");
       ok &= run_direct<double, equation::ILU<CD, double>>(f, 1e-8, "ILU solve d");

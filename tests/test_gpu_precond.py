@@ -4,10 +4,12 @@ Bars:
   * factorizations (IC / ILU values, SOR multipliers): bit-identical to the
     oracle's sequential restatement (same operations, same order);
   * zero pivots: the same row as the oracle;
-  * apply z = M^{-1} r: the forward sweep is evaluated in the reference's
-    order; the backward sweep sums a row's entries in another order, so z
-    agrees to 1e-12 (FP64) / 1e-5 (FP32) relative (max-norm); SOR apply
-    against the reference build itself;
+  * apply z = M^{-1} r: blocks whose rows depend only on the adjacent row
+    inside the block are resolved by an affine scan and the backward sweep
+    sums a row's entries in another order, so z agrees with the sequential
+    sweeps to 1e-12 (FP64) / 1e-5 (FP32) relative (max-norm); SOR apply
+    against the reference build itself; systems both below and above the
+    single-CTA size (solution and schedule within 200 KB of shared memory);
   * preconditioned CG / BiCGSTAB and the SOR solver: same status, iteration
     counts within +-1 (FP64) / +-10% (FP32), x within 1e-8 (FP64) relative.
 """
@@ -65,12 +67,16 @@ def matrices():
            "random_long": random_sparse(777, 4, 2, long_rows=5),
            "spd_random_900": random_sparse(900, 5, 3, symmetric=True),
            "tiny_5": random_sparse(5, 2, 4),
-           "one": (np.array([0, 1], np.int32), np.array([0], np.int32), np.array([4.0]))}
+           "one": (np.array([0, 1], np.int32), np.array([0], np.int32), np.array([4.0])),
+           # solutions larger than 200 KB in both precisions: the multi-CTA
+           # (flag-synchronized) sweeps instead of the single-CTA ones
+           "poisson2d_240": W.poisson2d(240)[1:],
+           "random_60k": random_sparse(60000, 4, 6, long_rows=3)}
     return out
 
 
 MATS = matrices()
-SYM = {"poisson2d_40x37", "poisson3d_12", "spd_random_900", "one"}
+SYM = {"poisson2d_40x37", "poisson3d_12", "spd_random_900", "one", "poisson2d_240"}
 
 
 def crs(handle, rp, ci, v):
