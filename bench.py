@@ -610,7 +610,11 @@ def run_precond(args, wl, rank, world, local):
     A = D.Crs(h, n, n, rp, ci, v, validate=False)
     db = torch.from_numpy(b).cuda()
     dx = torch.zeros(n, dtype=torch.float64, device="cuda")
-    solve = D.cg_solve_precond if wl["solver"] == "cg" else D.bicgstab_solve_precond
+    solve_fn = D.cg_solve_precond if wl["solver"] == "cg" else D.bicgstab_solve_precond
+
+    def solve(A_, pc_, b_, x_, tol_, maxiter_):
+        return solve_fn(A_, pc_, b_, x_, tol_, maxiter_, use_graph=not args.eager)
+
     stream = torch.cuda.current_stream()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
