@@ -17,7 +17,10 @@
 //    aligned, fully used bursts, and the copies carry an L2 evict-first
 //    policy so the once-read matrix does not push the gathered x out of L2.
 //  * 8 consumer warps, each owning 32 rows of the tile and working on its
-//    own between the "stage full" barrier and its own stage release:
+//    own: it releases the stage itself and, for plain SpMV, also waits on
+//    the stage's "full" mbarrier itself, so warps run ahead of one another
+//    within the stages in flight (no CTA barrier per tile; only chunk tiles
+//    bring them together; the fused-dot launches keep one barrier per tile):
 //      rows of up to kShortRow entries: one thread each, gathering x and
 //              summing in row order with separately rounded products (the
 //              reference's loop, so those rows are bit-identical to it);
@@ -30,7 +33,9 @@
 //    the last chunk to arrive (atomic counter per long row) sums the
 //    partials in chunk order and writes the row.
 //  * Every wait on an mbarrier is bounded; on timeout the CTA records
-//    MLSH_ERR_TIMEOUT, drains its in-flight copies and exits.
+//    MLSH_ERR_TIMEOUT, drains its in-flight copies and exits (a consumer
+//    warp that gave up keeps walking the tiles only to take part in the
+//    chunk tiles' barriers).
 //  * Variants (pipeline depth x CTAs per SM) trade shared memory against
 //    L1 capacity for the x gathers and against occupancy; the plan keeps
 //    the one its autotuner measured fastest.
@@ -90,8 +95,8 @@ struct SpmvSmem {
 // flags[] in shared memory
 constexpr int kFlagProdAbort = 0;
 constexpr int kFlagConsAbort = 1;
-constexpr int kFlagConsumed = 2;
 constexpr int kFlagLast = 3;
+constexpr int kFlagWarpDone = 4;  // 8 slots: tiles each consumer warp has consumed
 
 template <typename T>
 __device__ __forceinline__ T spmv_mul_rn(T a, T b) {
@@ -222,7 +227,11 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
       }
       if (aborted) {
         atomicExch(a.err, MLSH_ERR_TIMEOUT);
-        const int consumed = flags[kFlagConsumed];
+        // progress of the slowest consumer warp (with fused dots the warps
+        // move together and only the first one reports)
+        int consumed = issued;
+        for (int w = 0; w < (NR == 0 ? kConsumers / 32 : 1); ++w)
+          consumed = min(consumed, (int)flags[kFlagWarpDone + w]);
         for (int kk = consumed; kk < issued; ++kk) {
           const int s = kk % STAGES;
           mbar_wait_bounded(full0 + 8 * s, (uint32_t)((kk / STAGES) & 1), kWaitLimitNs);
@@ -261,7 +270,13 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
     }
   }
 
+  // Plain SpMV (no fused dots): each warp waits for a stage on its own and
+  // releases it on its own, so warps run ahead of one another within the
+  // stages in flight, and only a chunk tile (a CTA-wide sum) brings them
+  // together.  A warp whose wait gives up stops computing but keeps walking
+  // the tiles so that it still takes part in every chunk tile's barrier.
   int k = 0;
+  int nchunk = 0;  // chunk tiles met so far (the same count in every warp)
   for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++k) {
     const int s = k % STAGES;
     const Tile tl = tl_c;
@@ -274,14 +289,39 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
     const int tn = t + (int)gridDim.x;
     Tile tl_n = {0, -1, 0, 0};
     if (tn < a.n_tiles) tl_n = a.tiles[tn];
-    if (ct == 0) {
-      if (!mbar_wait_bounded(full0 + 8 * s, (uint32_t)((k / STAGES) & 1), kWaitLimitNs)) {
-        flags[kFlagConsAbort] = 1;
-        atomicExch(a.err, MLSH_ERR_TIMEOUT);
+    if constexpr (NR == 0) {
+      int ok = 1;
+      if (lane == 0) {
+        // once any warp has given up, the flag sends every warp down the
+        // walking path at its next tile
+        ok = flags[kFlagConsAbort] == 0 &&
+             mbar_wait_bounded(full0 + 8 * s, (uint32_t)((k / STAGES) & 1), kWaitLimitNs);
+        if (!ok && flags[kFlagConsAbort] == 0) {
+          flags[kFlagConsAbort] = 1;
+          atomicExch(a.err, MLSH_ERR_TIMEOUT);
+        }
       }
+      if (__shfl_sync(0xffffffffu, ok, 0) == 0) {
+        tl_c = tl_n;
+        if (!normal) {
+          named_sync(1, kConsumers);  // the chunk tile's barrier
+          ++nchunk;
+        }
+        continue;
+      }
+    } else {
+      // with fused dots (the solvers' launches, at the register limit) the
+      // consumers start each tile together: one thread waits, a CTA-wide
+      // named barrier releases all
+      if (ct == 0) {
+        if (!mbar_wait_bounded(full0 + 8 * s, (uint32_t)((k / STAGES) & 1), kWaitLimitNs)) {
+          flags[kFlagConsAbort] = 1;
+          atomicExch(a.err, MLSH_ERR_TIMEOUT);
+        }
+      }
+      named_sync(1, kConsumers);
+      if (flags[kFlagConsAbort]) break;
     }
-    named_sync(1, kConsumers);
-    if (flags[kFlagConsAbort]) break;
 
     const int nb = tl.nnz_begin, ne = tl.nnz_end, nt = ne - nb;
     unsigned char *st = smem + s * L::kStageBytes;
@@ -352,8 +392,10 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
       }
       // this warp is done with the stage
       __syncwarp();
-      if (lane == 0) mbar_arrive(empty0 + 8 * s);
-      if (ct == 0) flags[kFlagConsumed] = k + 1;
+      if (lane == 0) {
+        mbar_arrive(empty0 + 8 * s);
+        if (NR == 0 || warp == 0) flags[kFlagWarpDone + warp] = k + 1;
+      }
       // ----------------------------------------------------- y and dots
       if (ct < nrows) {
         const int r = rb + ct;
@@ -373,13 +415,24 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
         part = spmv_add_rn(part, spmv_mul_rn(v[j], (VT)__ldg(a.x + col_at(j))));
       prefetch_next();
       part = warp_sum(part);
-      if (lane == 0) red[warp] = (double)part;
+      // slots 16..31 of red, apart from the slots the closing dot reduction
+      // writes; with independent warps double-buffered by chunk count (a
+      // warp can be at most one chunk tile ahead of the thread that reads
+      // the sums: it cannot pass the next chunk's barrier before it)
+      double *cred = red + 16;
+      if constexpr (NR == 0) {
+        cred += (nchunk & 1) * (kConsumers / 32);
+        ++nchunk;
+      }
+      if (lane == 0) cred[warp] = (double)part;
       named_sync(1, kConsumers);
-      if (lane == 0) mbar_arrive(empty0 + 8 * s);
+      if (lane == 0) {
+        mbar_arrive(empty0 + 8 * s);
+        if (NR == 0 || warp == 0) flags[kFlagWarpDone + warp] = k + 1;
+      }
       if (ct == 0) {
-        flags[kFlagConsumed] = k + 1;
         double tot = 0.0;
-        for (int w = 0; w < kConsumers / 32; ++w) tot += red[w];
+        for (int w = 0; w < kConsumers / 32; ++w) tot += cred[w];
         const int li = -tl.row_end - 1;
         const int row = tl.row_begin;
         bool last = true;
