@@ -30,7 +30,7 @@ namespace {
 
 constexpr int kSweepThreads = 256;
 constexpr int kSweepWarps = kSweepThreads / 32;
-constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s per wait
+constexpr unsigned kWaitPolls = 1u << 22;  // polls per wait (seconds)
 constexpr unsigned kFull = 0xffffffffu;
 
 // ---- explicitly rounded arithmetic
@@ -44,22 +44,17 @@ __device__ __forceinline__ double sqrt_rn(double a) { return __dsqrt_rn(a); }
 __device__ __forceinline__ float sqrt_rn(float a) { return __fsqrt_rn(a); }
 
 // Waits until *flag == want.  Gives up (recording MLSH_ERR_TIMEOUT) after
-// kWaitNs, or at once once another warp has recorded an error.
+// kWaitPolls polls, or soon after another warp has recorded an error.  The
+// loop is a bare acquire poll (no timer reads, no sleeps): measured on the
+// sweeps, this keeps the hop from a publishing warp to its waiters about
+// half as long as polls interleaved with sleeps or timer reads.
 __device__ __noinline__ bool wait_flag(const unsigned *flag, unsigned want, int *err) {
-  if (ld_acquire_gpu(flag) == want) return true;
-  const uint64_t t0 = global_timer_ns();
-  unsigned spins = 0;
-  while (true) {
+  for (unsigned it = 0; it < kWaitPolls; ++it) {
     if (ld_acquire_gpu(flag) == want) return true;
-    if ((++spins & 63u) == 0) {
-      if (*(volatile int *)err != 0) return false;
-      if (global_timer_ns() - t0 > kWaitNs) {
-        atomicCAS(err, 0, MLSH_ERR_TIMEOUT);
-        return false;
-      }
-      __nanosleep(64);
-    }
+    if ((it & 1023u) == 1023u && *(volatile int *)err != 0) return false;
   }
+  atomicCAS(err, 0, MLSH_ERR_TIMEOUT);
+  return false;
 }
 
 // ---------------------------------------------------------------------------
@@ -139,8 +134,10 @@ __device__ __forceinline__ bool sweep_ticket(const SweepArgs<T> &a, int lane,
   return !(a.done != nullptr && *(volatile const int *)a.done != 0);
 }
 
+// The lanes' stores are ordered before lane 0's by the warp barrier, and
+// lane 0's release store (cumulative) makes them visible, at GPU scope, to
+// every warp that acquires the flag.
 __device__ __forceinline__ void publish_block(unsigned *flag, unsigned epoch, int lane) {
-  __threadfence();
   __syncwarp();
   if (lane == 0) st_release_gpu(flag, epoch);
 }
@@ -594,8 +591,13 @@ __global__ void __launch_bounds__(kSweepThreads)
 }
 
 // ---------------------------------------------------------------------------
-// Factorizations: one warp per row, rows handed out by a ticket in
-// ascending order, a ready flag per row (1 once the row is final).
+// Factorizations: one warp per 32-row block, blocks in the lower sweep's
+// level order with per-block flags (the sweeps' schedule and protocol).
+// Each lane factors its own row with the sequential algorithm's operations
+// in the sequential order: first the eliminations by rows outside the block
+// (all lanes at once, after the block's dependency blocks are final), then
+// those by rows inside the block as a 32-step chain -- at step s row base+s
+// is final and every lane whose row stores (i, base+s) applies it.
 template <typename T>
 struct FactorArgs {
   const int *rp;
@@ -604,139 +606,112 @@ struct FactorArgs {
   const int *up_beg;
   T *f;  // A's values on entry, the factor on exit
   int n;
+  unsigned nb;
   unsigned long long *ticket;
-  unsigned *rowflag;
+  unsigned *flags;  // nb block flags, zero on entry (one launch: epoch 1)
+  const int *order;
+  const int *dep_off;
+  const int *dep_ids;
   int *err;
   unsigned long long *pivot;  // first zero pivot (min row), ~0 if none
-  const int *order;           // blocks of 32 rows in level order
-  unsigned nb;
 };
 
-// Waits until row k is final; afterwards every lane may read it.
-__device__ __forceinline__ void wait_row(const unsigned *rowflag, int k, int *err, int lane) {
-  if (lane == 0) wait_flag(rowflag + k, 1u, err);
-  __syncwarp();
-  (void)ld_acquire_gpu(rowflag + k);
-}
-
-// First position in ci[lo, hi) whose column is >= c.
-__device__ __forceinline__ int lower_bound_col(const int *ci, int lo, int hi, int c) {
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (ci[mid] < c) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
-}
-
-// Row of this warp: tickets walk the blocks in level order and the rows of
-// a block in ascending order, so every row a row depends on has a smaller
-// ticket.  -1: no row (past the grid or past the last row).
+// ILU(0) elimination of row `row` by row k (the stored (row, k) at q):
+//   a_ik = a_ik / a_kk;  a_ij -= a_ik * a_kj  for stored j > k with a_kj stored
+// (Saad, Iterative Methods for Sparse Linear Systems, 2nd ed., Alg. 10.4);
+// row k's upper part and row i's later entries are merged in column order.
 template <typename T>
-__device__ __forceinline__ int factor_ticket(const FactorArgs<T> &a, int lane) {
+__device__ __forceinline__ void ilu_eliminate(const FactorArgs<T> &a, int row, int q, int k) {
+  T *f = a.f;
+  const int kd = a.lo_end[k], kb = a.up_beg[k], ke = a.rp[k + 1];
+  const T ukk = kb > kd ? __ldcg(f + kd) : T(0);
+  const T l = div_rn(__ldcg(f + q), ukk);
+  f[q] = l;
+  const int re = a.rp[row + 1];
+  int pos = kb;
+  for (int p = q + 1; p < re; ++p) {
+    const int c = a.ci[p];
+    while (pos < ke && a.ci[pos] < c) ++pos;
+    if (pos < ke && a.ci[pos] == c) f[p] = sub_rn(__ldcg(f + p), mul_rn(l, __ldcg(f + pos)));
+  }
+}
+
+// IC(0) entry l_ik = (a_ik - sum_{m<k} l_im l_km) / l_kk over the stored m of
+// both rows, ascending in m.
+template <typename T>
+__device__ __forceinline__ void ic_entry(const FactorArgs<T> &a, int row, int q, int k) {
+  T *f = a.f;
+  T acc = __ldcg(f + q);
+  const int kd = a.lo_end[k];
+  int pk = a.rp[k];
+  for (int p = a.rp[row]; p < q; ++p) {
+    const int m = a.ci[p];
+    while (pk < kd && a.ci[pk] < m) ++pk;
+    if (pk < kd && a.ci[pk] == m) acc = sub_rn(acc, mul_rn(__ldcg(f + p), __ldcg(f + pk)));
+  }
+  const T lkk = a.up_beg[k] > kd ? __ldcg(f + kd) : T(0);
+  f[q] = div_rn(acc, lkk);
+}
+
+// IC(0) diagonal l_ii = sqrt(a_ii - sum_{m<i} l_im^2), ascending in m.
+template <typename T>
+__device__ __forceinline__ void ic_diag(const FactorArgs<T> &a, int row) {
+  T *f = a.f;
+  const int le = a.lo_end[row];
+  const bool has = a.up_beg[row] > le;
+  T d = has ? __ldcg(f + le) : T(0);
+  for (int p = a.rp[row]; p < le; ++p) {
+    const T v = __ldcg(f + p);
+    d = sub_rn(d, mul_rn(v, v));
+  }
+  if (!(d > T(0))) atomicMin(a.pivot, (unsigned long long)row);
+  if (has) f[le] = sqrt_rn(d);
+}
+
+template <typename T, bool IC>
+__global__ void __launch_bounds__(kSweepThreads) factor_kernel(FactorArgs<T> a) {
+  const int lane = threadIdx.x & 31;
   const unsigned gw = blockIdx.x * kSweepWarps + (threadIdx.x >> 5);
-  if (gw >= a.nb * 32u) return -1;
+  if (gw >= a.nb) return;
   unsigned long long v = 0;
   if (lane == 0) v = atomicAdd(a.ticket, 1ull);
   const unsigned long long t = __shfl_sync(kFull, v, 0);
-  const int row = (int)((unsigned)a.order[(unsigned)(t >> 5)] & kBlockMask) * 32 + (int)(t & 31ull);
-  return row < a.n ? row : -1;
-}
-
-// ILU(0), row by row (the IKJ form; Saad, Iterative Methods for Sparse
-// Linear Systems, 2nd ed., Algorithm 10.4):
-//   for each k < i with a_ik stored, ascending:
-//     a_ik = a_ik / a_kk
-//     a_ij = a_ij - a_ik * a_kj   for every stored a_ij, j > k, with a_kj stored
-template <typename T>
-__global__ void __launch_bounds__(kSweepThreads) ilu0_kernel(FactorArgs<T> a) {
-  const int lane = threadIdx.x & 31;
-  const int row = factor_ticket(a, lane);
-  if (row < 0) return;
-  const int rb = a.rp[row], re = a.rp[row + 1], le = a.lo_end[row];
-  T *f = a.f;
-  for (int q = rb; q < le; ++q) {
+  const unsigned epoch = (unsigned)(t / a.nb) + 1u;
+  const unsigned blk = (unsigned)a.order[t % a.nb] & kBlockMask;
+  const int base = (int)blk * 32;
+  const int row = base + lane;
+  const bool valid = row < a.n;
+  wait_deps(a.dep_off, a.dep_ids, a.flags, blk, epoch, a.err, lane);
+  int q = valid ? a.rp[row] : 0;
+  const int le = valid ? a.lo_end[row] : 0;
+  // rows outside the block, ascending
+  for (; q < le; ++q) {
     const int k = a.ci[q];
-    wait_row(a.rowflag, k, a.err, lane);
-    const int kd = a.lo_end[k], kb = a.up_beg[k], ke = a.rp[k + 1];
-    const T ukk = kb > kd ? __ldcg(f + kd) : T(0);
-    const T l = div_rn(__ldcg(f + q), ukk);
-    __syncwarp();
-    if (lane == 0) f[q] = l;
-    for (int p = q + 1 + lane; p < re; p += 32) {
-      const int c = a.ci[p];
-      const int pos = lower_bound_col(a.ci, kb, ke, c);
-      if (pos < ke && a.ci[pos] == c) f[p] = sub_rn(__ldcg(f + p), mul_rn(l, __ldcg(f + pos)));
+    if (k >= base) break;
+    if constexpr (IC) ic_entry(a, row, q, k);
+    else ilu_eliminate(a, row, q, k);
+  }
+  // rows inside the block: the chain
+  for (int st = 0; st < 32; ++st) {
+    if constexpr (IC) {
+      if (lane == st && valid) ic_diag(a, row);
     }
     __syncwarp();
-  }
-  if (lane == 0) {
-    const bool has = a.up_beg[row] > le;
-    if (!has || __ldcg(f + le) == T(0)) atomicMin(a.pivot, (unsigned long long)row);
-  }
-  publish_block(a.rowflag + row, 1u, lane);
-}
-
-// IC(0), row by row on the lower triangle (the row-oriented Cholesky
-// recurrence restricted to A's pattern):
-//   l_ik = (a_ik - sum_{m<k} l_im l_km) / l_kk   for stored a_ik, k < i
-//   l_ii = sqrt(a_ii - sum_{m<i} l_im^2)
-// each sum over the stored positions of both rows, ascending in m.
-template <typename T>
-__global__ void __launch_bounds__(kSweepThreads) ic0_kernel(FactorArgs<T> a) {
-  const int lane = threadIdx.x & 31;
-  const int row = factor_ticket(a, lane);
-  if (row < 0) return;
-  const int rb = a.rp[row], le = a.lo_end[row];
-  const bool has = a.up_beg[row] > le;
-  T *f = a.f;
-  for (int q = rb; q < le; ++q) {
-    const int k = a.ci[q];
-    wait_row(a.rowflag, k, a.err, lane);
-    const int kb = a.rp[k], kd = a.lo_end[k];
-    const bool kh = a.up_beg[k] > kd;
-    T s = __ldcg(f + q);
-    for (int c0 = rb; c0 < q; c0 += 32) {
-      const int p = c0 + lane;
-      T prod = T(0);
-      bool found = false;
-      if (p < q) {
-        const int m = a.ci[p];
-        const int pos = lower_bound_col(a.ci, kb, kd, m);
-        if (pos < kd && a.ci[pos] == m) {
-          prod = mul_rn(__ldcg(f + p), __ldcg(f + pos));
-          found = true;
-        }
-      }
-      const unsigned fm = __ballot_sync(kFull, found);
-#pragma unroll 4
-      for (int u = 0; u < 32; ++u) {
-        const T pu = __shfl_sync(kFull, prod, u);
-        if ((fm >> u) & 1u) s = sub_rn(s, pu);
-      }
+    if (q < le && a.ci[q] == base + st) {
+      if constexpr (IC) ic_entry(a, row, q, base + st);
+      else ilu_eliminate(a, row, q, base + st);
+      ++q;
     }
-    const T lkk = kh ? __ldcg(f + kd) : T(0);
-    const T l = div_rn(s, lkk);
-    __syncwarp();
-    if (lane == 0) f[q] = l;
-    __syncwarp();
   }
-  T d = has ? __ldcg(f + le) : T(0);
-  for (int c0 = rb; c0 < le; c0 += 32) {
-    const int p = c0 + lane;
-    T fp = T(0);
-    if (p < le) fp = __ldcg(f + p);
-    const T prod = mul_rn(fp, fp);
-    const int cnt = min(32, le - c0);
-    for (int u = 0; u < cnt; ++u) d = sub_rn(d, __shfl_sync(kFull, prod, u));
-  }
-  const T lii = sqrt_rn(d);
   __syncwarp();
-  if (lane == 0) {
-    if (!(d > T(0))) atomicMin(a.pivot, (unsigned long long)row);
-    if (has) f[le] = lii;
+  if constexpr (!IC) {
+    if (valid) {
+      const int d = a.lo_end[row];
+      if (!(a.up_beg[row] > d) || __ldcg(a.f + d) == T(0))
+        atomicMin(a.pivot, (unsigned long long)row);
+    }
   }
-  publish_block(a.rowflag + row, 1u, lane);
+  publish_block(a.flags + blk, epoch, lane);
 }
 
 int grid_of(long long n, int threads) { return (int)std::max<long long>(1, (n + threads - 1) / threads); }
@@ -817,11 +792,11 @@ cudaError_t sweep_launch_t(const Precond &pc, const Sweep &sw, bool backward, co
 template <typename T>
 int factor_run(Handle &h, Precond &pc, const int *rp, const int *ci) {
   cudaStream_t s = h.stream;
-  unsigned *rowflag = nullptr;
+  unsigned *rowflag = nullptr;  // block flags of the factorization launch
   unsigned long long *scratch = nullptr;  // [ticket, pivot]
-  MLSH_CUDA_TRY(pool_alloc(&rowflag, sizeof(unsigned) * (size_t)std::max(pc.n, 1), s));
+  MLSH_CUDA_TRY(pool_alloc(&rowflag, sizeof(unsigned) * (size_t)std::max(pc.nb, 1u), s));
   MLSH_CUDA_TRY(pool_alloc(&scratch, 2 * sizeof(unsigned long long), s));
-  MLSH_CUDA_TRY(cudaMemsetAsync(rowflag, 0, sizeof(unsigned) * (size_t)pc.n, s));
+  MLSH_CUDA_TRY(cudaMemsetAsync(rowflag, 0, sizeof(unsigned) * (size_t)std::max(pc.nb, 1u), s));
   MLSH_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), s));
   MLSH_CUDA_TRY(cudaMemsetAsync(scratch + 1, 0xff, sizeof(unsigned long long), s));
   MLSH_CUDA_TRY(cudaMemsetAsync(h.err_flag, 0, sizeof(int), s));
@@ -832,15 +807,17 @@ int factor_run(Handle &h, Precond &pc, const int *rp, const int *ci) {
   a.up_beg = pc.up_beg;
   a.f = static_cast<T *>(pc.fval);
   a.n = pc.n;
+  a.nb = pc.nb;
   a.ticket = scratch;
-  a.rowflag = rowflag;
+  a.flags = rowflag;
+  a.order = pc.sfwd.order;
+  a.dep_off = pc.sfwd.dep_off;
+  a.dep_ids = pc.sfwd.dep_ids;
   a.err = h.err_flag;
   a.pivot = scratch + 1;
-  a.order = pc.sfwd.order;
-  a.nb = pc.nb;
-  const int g = grid_of((long long)pc.nb * 32, kSweepWarps);
-  if (pc.kind == MLSH_PRECOND_IC) ic0_kernel<T><<<g, kSweepThreads, 0, s>>>(a);
-  else ilu0_kernel<T><<<g, kSweepThreads, 0, s>>>(a);
+  const int g = grid_of(pc.nb, kSweepWarps);
+  if (pc.kind == MLSH_PRECOND_IC) factor_kernel<T, true><<<g, kSweepThreads, 0, s>>>(a);
+  else factor_kernel<T, false><<<g, kSweepThreads, 0, s>>>(a);
   MLSH_CUDA_TRY(cudaGetLastError());
   unsigned long long piv = 0;
   int err = 0;
