@@ -230,26 +230,39 @@ struct RowState {
   T pv[kPre];
 };
 
+// Loading a row's state takes two dependent steps: the row's own arrays
+// (stage 1), then what they point to (stage 2).
 template <typename T, int MODE>
-__device__ __forceinline__ void fwd_load(const SweepArgs<T> &a, unsigned ov, int lane,
-                                         RowState<T> &st) {
+__device__ __forceinline__ void fwd_load1(const SweepArgs<T> &a, unsigned ov, int lane,
+                                          RowState<T> &st) {
   const int row = (int)(ov & kBlockMask) * 32 + lane;
   st.acc = T(0);
   st.fin = T(1);
   st.j = 0;
   st.e = 0;
+  st.split = 0;  // kDiagFwd: whether the diagonal is stored
   if (row < a.n) {
     st.j = a.rp[row];
     st.e = a.lo_end[row];
     st.acc = a.rhs[row];
     if constexpr (MODE == kSorFwd) st.fin = a.scale[row];
-    if constexpr (MODE == kDiagFwd) st.fin = a.up_beg[row] > st.e ? a.val[st.e] : T(0);
+    if constexpr (MODE == kDiagFwd) st.split = a.up_beg[row] > st.e;
   }
+}
+template <typename T, int MODE>
+__device__ __forceinline__ void fwd_load2(const SweepArgs<T> &a, RowState<T> &st) {
+  if constexpr (MODE == kDiagFwd) st.fin = st.split ? a.val[st.e] : T(0);
 #pragma unroll
   for (int u = 0; u < kPre; ++u) {
     st.pc[u] = st.j + u < st.e ? a.ci[st.j + u] : 0x7fffffff;
     st.pv[u] = st.j + u < st.e ? a.val[st.j + u] : T(0);
   }
+}
+template <typename T, int MODE>
+__device__ __forceinline__ void fwd_load(const SweepArgs<T> &a, unsigned ov, int lane,
+                                         RowState<T> &st) {
+  fwd_load1<T, MODE>(a, ov, lane, st);
+  fwd_load2<T, MODE>(a, st);
 }
 
 // One 32-row block of the lower sweep, from its loaded state: every value
@@ -334,15 +347,15 @@ __device__ __forceinline__ void fwd_finish_block(const SweepArgs<T> &a, unsigned
 }
 
 template <typename T, int MODE>
-__device__ __forceinline__ void bwd_load(const SweepArgs<T> &a, unsigned ov, int lane,
-                                         RowState<T> &st) {
-  const int base = (int)(ov & kBlockMask) * 32;
-  const int row = base + lane;
+__device__ __forceinline__ void bwd_load1(const SweepArgs<T> &a, unsigned ov, int lane,
+                                          RowState<T> &st) {
+  const int row = (int)(ov & kBlockMask) * 32 + lane;
   st.acc = T(0);
   st.fin = T(1);
   st.rh = T(0);
   st.jb = 0;
   st.e = 0;
+  st.j = -1;  // kDiagBwd: position of the diagonal, -1 if not stored
   st.split = 0;
   if (row < a.n) {
     st.jb = a.up_beg[row];
@@ -353,17 +366,28 @@ __device__ __forceinline__ void bwd_load(const SweepArgs<T> &a, unsigned ov, int
     } else {
       st.acc = st.rh;
       const int d = a.lo_end[row];
-      st.fin = st.jb > d ? a.val[d] : T(0);
+      st.j = st.jb > d ? d : -1;
     }
-    int split = st.jb;
-    while (split < st.e && a.ci[split] < base + 32) ++split;
-    st.split = split;
   }
+}
+template <typename T, int MODE>
+__device__ __forceinline__ void bwd_load2(const SweepArgs<T> &a, unsigned ov, RowState<T> &st) {
+  const int base = (int)(ov & kBlockMask) * 32;
+  if constexpr (MODE != kSorBwd) st.fin = st.j >= 0 ? a.val[st.j] : T(0);
+  int split = st.jb;
+  while (split < st.e && a.ci[split] < base + 32) ++split;
+  st.split = split;
 #pragma unroll
   for (int u = 0; u < kPre; ++u) {
     st.pc[u] = st.split + u < st.e ? a.ci[st.split + u] : -1;
     st.pv[u] = st.split + u < st.e ? a.val[st.split + u] : T(0);
   }
+}
+template <typename T, int MODE>
+__device__ __forceinline__ void bwd_load(const SweepArgs<T> &a, unsigned ov, int lane,
+                                         RowState<T> &st) {
+  bwd_load1<T, MODE>(a, ov, lane, st);
+  bwd_load2<T, MODE>(a, ov, st);
 }
 
 // One 32-row block of the upper sweep, from its loaded state.
@@ -500,31 +524,61 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
   const int nw = blockDim.x >> 5;
   double *scratch = nullptr;  // no polling warps here: shuffle scan
   const SharedX<T> X{xs};
-  // each warp loads its first block of the next level before the barrier,
-  // so the loads that do not depend on the solution overlap the wait
-  RowState<T> st;
-  bool have = false;
-  unsigned ov = 0;
+  // A software pipeline over the levels: while a level runs, each warp
+  // holds its first block of the next level fully loaded and the row arrays
+  // of its first block two levels ahead, so the two dependent loads of a
+  // row's state overlap two levels' work and barriers.
+  auto load1 = [&](unsigned o, RowState<T> &st) {
+    if constexpr (BWD) bwd_load1<T, MODE>(a, o, lane, st);
+    else fwd_load1<T, MODE>(a, o, lane, st);
+  };
+  auto load2 = [&](unsigned o, RowState<T> &st) {
+    if constexpr (BWD) bwd_load2<T, MODE>(a, o, st);
+    else fwd_load2<T, MODE>(a, st);
+  };
+  RowState<T> cur, nxt;
+  unsigned ov_cur = 0, ov_nxt = 0;
+  bool have_cur = false, have_nxt = false;
+  if (levels > 0 && s_loff[0] + warp < s_loff[1]) {
+    ov_cur = (unsigned)s_order[s_loff[0] + warp];
+    load1(ov_cur, cur);
+    load2(ov_cur, cur);
+    have_cur = true;
+  }
+  if (levels > 1 && s_loff[1] + warp < s_loff[2]) {
+    ov_nxt = (unsigned)s_order[s_loff[1] + warp];
+    load1(ov_nxt, nxt);
+    have_nxt = true;
+  }
   for (int lv = 0; lv < levels; ++lv) {
     const int q1 = s_loff[lv + 1];
     for (int q = s_loff[lv] + warp; q < q1; q += nw) {
-      if (!have) {
+      RowState<T> st;
+      unsigned ov;
+      if (q == s_loff[lv] + warp && have_cur) {
+        st = cur;
+        ov = ov_cur;
+      } else {
         ov = (unsigned)s_order[q];
-        if constexpr (BWD) bwd_load<T, MODE>(a, ov, lane, st);
-        else fwd_load<T, MODE>(a, ov, lane, st);
+        load1(ov, st);
+        load2(ov, st);
       }
-      have = false;
       if constexpr (BWD) bwd_finish_block<T, MODE>(a, ov, lane, X, st, scratch);
       else fwd_finish_block<T, MODE>(a, ov, lane, X, st, scratch);
     }
-    if (lv + 1 < levels) {
-      const int qn = q1 + warp;
-      if (qn < s_loff[lv + 2]) {
-        ov = (unsigned)s_order[qn];
-        if constexpr (BWD) bwd_load<T, MODE>(a, ov, lane, st);
-        else fwd_load<T, MODE>(a, ov, lane, st);
-        have = true;
-      }
+    // advance: next level's block gets its second stage, the block two
+    // levels ahead its first
+    have_cur = have_nxt;
+    if (have_nxt) {
+      cur = nxt;
+      ov_cur = ov_nxt;
+      load2(ov_cur, cur);
+    }
+    have_nxt = false;
+    if (lv + 2 < levels && s_loff[lv + 2] + warp < s_loff[lv + 3]) {
+      ov_nxt = (unsigned)s_order[s_loff[lv + 2] + warp];
+      load1(ov_nxt, nxt);
+      have_nxt = true;
     }
     __syncthreads();
   }
