@@ -226,6 +226,7 @@ template <typename T>
 struct RowState {
   int j, e, jb, split;
   T acc, fin, rh;
+  T a1v;  // upper sweep: the row's first upper entry (row + 1 in a scan block)
   int pc[kPre];
   T pv[kPre];
 };
@@ -298,8 +299,17 @@ __device__ __forceinline__ void fwd_finish_block(const SweepArgs<T> &a, unsigned
   T xv = T(0);
   if (ov & kScanBit) {
     // the block's only in-block dependencies are row - 1 -> row: the
-    // recurrence x_k = al_k + be_k x_{k-1} as a 5-step affine scan
-    const T a1 = (j < e) ? a.val[j] : T(0);
+    // recurrence x_k = al_k + be_k x_{k-1} as a 5-step affine scan; the
+    // (row, row - 1) entry is normally among the prefetched ones
+    const int d = j - st.j;
+    T a1 = T(0);
+    if (d < kPre) {
+#pragma unroll
+      for (int u = 0; u < kPre; ++u)
+        if (u == d) a1 = st.pv[u];
+    } else if (j < e) {
+      a1 = a.val[j];
+    }
     T al, be;
     if constexpr (MODE == kSorFwd) {
       al = acc * fin;
@@ -374,6 +384,7 @@ template <typename T, int MODE>
 __device__ __forceinline__ void bwd_load2(const SweepArgs<T> &a, unsigned ov, RowState<T> &st) {
   const int base = (int)(ov & kBlockMask) * 32;
   if constexpr (MODE != kSorBwd) st.fin = st.j >= 0 ? a.val[st.j] : T(0);
+  st.a1v = st.jb < st.e ? a.val[st.jb] : T(0);
   int split = st.jb;
   while (split < st.e && a.ci[split] < base + 32) ++split;
   st.split = split;
@@ -422,7 +433,7 @@ __device__ __forceinline__ void bwd_finish_block(const SweepArgs<T> &a, unsigned
   T xv = T(0);
   if (ov & kScanBit) {
     // only row + 1 -> row inside the block: z_k = al_k + be_k z_{k+1}
-    const T a1 = (split > jb) ? a.val[jb] : T(0);
+    const T a1 = (split > jb) ? st.a1v : T(0);
     if constexpr (MODE == kSorBwd) {
       const double al = (double)rh - sacc * (double)fin;
       const double be = -((double)a1 * (double)fin);
