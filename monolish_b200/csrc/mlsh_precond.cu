@@ -4,16 +4,17 @@
 // follows are described in mlsh_precond.cuh.
 //
 // Arithmetic is written with explicitly rounded operations (no fused
-// multiply-add), so that every value is the one a sequential evaluation in
-// the same order produces:
-//   * the forward sweeps accumulate each row in ascending column order, as
-//     src/equation/kernel/sor_kernel.hpp:50-58 does;
+// multiply-add), so that values follow a sequential evaluation's order:
 //   * the factorizations apply every update to an entry in the order of the
 //     row-by-row (IKJ) algorithms, and sum the IC inner products in
-//     ascending column order;
-//   * the backward sweeps accumulate a row's entries outside its 32-row
-//     block in ascending order, then those inside it in descending order
-//     (the order in which the block's chain produces them).
+//     ascending column order: bit-identical to a sequential factorization;
+//   * the forward sweeps accumulate each row in ascending column order, as
+//     src/equation/kernel/sor_kernel.hpp:50-58 does, and the backward sweeps
+//     a row's entries outside its 32-row block in ascending order, then those
+//     inside it in descending order (the order of the block's chain);
+//   * blocks whose rows depend only on the adjacent row are resolved by an
+//     affine scan instead of the chain: there the rounding differs from the
+//     sequential recurrence's (by a few units in the last place).
 #include <cuda_runtime.h>
 
 #include <algorithm>
