@@ -149,47 +149,20 @@ constexpr unsigned kScanBit = 0x80000000u;
 constexpr unsigned kBlockMask = 0x7fffffffu;
 
 // x_k = al_k + be_k x_{k-1} (REV: x_{k+1}) over the 32 lanes, as a
-// Hillis-Steele scan of affine maps (log2 32 = 5 steps instead of a 32-step
-// chain), exchanged through the warp's shared-memory scratch `sm` (128
-// values, double-buffered): inside a busy sweep this is about twice as fast
-// as the same scan over register shuffles (used when sm is null: the
-// single-CTA sweep).  A lane with be_k == 0 takes nothing from its
-// neighbour, so a non-finite value there does not leak.
-constexpr int kScanScratch = 128;  // values per warp
+// Kogge-Stone scan of affine maps over register shuffles (log2 32 = 5 steps
+// instead of a 32-step chain).  A lane with be_k == 0 takes nothing from its
+// neighbour, so a non-finite value there does not leak into it.
 template <bool REV, typename S>
-__device__ __forceinline__ S affine_scan(S al, S be, int lane, S *sm) {
-  if (sm == nullptr) {
-    // register shuffles: faster when the SM is not shared with polling warps
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const S al2 = REV ? __shfl_down_sync(kFull, al, d) : __shfl_up_sync(kFull, al, d);
-      const S be2 = REV ? __shfl_down_sync(kFull, be, d) : __shfl_up_sync(kFull, be, d);
-      const bool in = REV ? lane + d < 32 : lane >= d;
-      if (in && be != S(0)) {
-        al = al + be * al2;
-        be = be * be2;
-      }
-    }
-    return al;
-  }
-  S *sal = sm, *sbe = sm + 64;
-  int pp = 0;
-  sal[lane] = al;
-  sbe[lane] = be;
-  __syncwarp();
+__device__ __forceinline__ S affine_scan(S al, S be, int lane) {
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
-    const int src = REV ? lane + d : lane - d;
-    const bool in = REV ? src < 32 : src >= 0;
+    const S al2 = REV ? __shfl_down_sync(kFull, al, d) : __shfl_up_sync(kFull, al, d);
+    const S be2 = REV ? __shfl_down_sync(kFull, be, d) : __shfl_up_sync(kFull, be, d);
+    const bool in = REV ? lane + d < 32 : lane >= d;
     if (in && be != S(0)) {
-      const S al2 = sal[pp * 32 + src], be2 = sbe[pp * 32 + src];
       al = al + be * al2;
       be = be * be2;
     }
-    sal[(pp ^ 1) * 32 + lane] = al;
-    sbe[(pp ^ 1) * 32 + lane] = be;
-    pp ^= 1;
-    __syncwarp();
   }
   return al;
 }
@@ -271,8 +244,7 @@ __device__ __forceinline__ void fwd_load(const SweepArgs<T> &a, unsigned ov, int
 // outside the block must be final when this runs.
 template <typename T, int MODE, class XS>
 __device__ __forceinline__ void fwd_finish_block(const SweepArgs<T> &a, unsigned ov, int lane,
-                                                 const XS &X, const RowState<T> &st,
-                                                 double *scratch) {
+                                                 const XS &X, const RowState<T> &st) {
   const int base = (int)(ov & kBlockMask) * 32;
   const int row = base + lane;
   const bool valid = row < a.n;
@@ -322,7 +294,7 @@ __device__ __forceinline__ void fwd_finish_block(const SweepArgs<T> &a, unsigned
       al = acc;
       be = -a1;
     }
-    xv = affine_scan<false>(al, be, lane, reinterpret_cast<T *>(scratch));
+    xv = affine_scan<false>(al, be, lane);
   } else {
     // entries inside the block, ascending: a 32-step chain; the next two
     // are kept in registers so the chain carries no memory latency
@@ -405,8 +377,7 @@ __device__ __forceinline__ void bwd_load(const SweepArgs<T> &a, unsigned ov, int
 // One 32-row block of the upper sweep, from its loaded state.
 template <typename T, int MODE, class XS>
 __device__ __forceinline__ void bwd_finish_block(const SweepArgs<T> &a, unsigned ov, int lane,
-                                                 const XS &X, const RowState<T> &st,
-                                                 double *scratch) {
+                                                 const XS &X, const RowState<T> &st) {
   const int base = (int)(ov & kBlockMask) * 32;
   const int row = base + lane;
   const bool valid = row < a.n;
@@ -438,9 +409,9 @@ __device__ __forceinline__ void bwd_finish_block(const SweepArgs<T> &a, unsigned
     if constexpr (MODE == kSorBwd) {
       const double al = (double)rh - sacc * (double)fin;
       const double be = -((double)a1 * (double)fin);
-      xv = (T)affine_scan<true>(al, be, lane, scratch);
+      xv = (T)affine_scan<true>(al, be, lane);
     } else {
-      xv = affine_scan<true>(acc / fin, -(a1 / fin), lane, reinterpret_cast<T *>(scratch));
+      xv = affine_scan<true>(acc / fin, -(a1 / fin), lane);
     }
   } else {
     // entries inside the block, consumed from the highest column down
@@ -493,14 +464,12 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepArgs<T> a) {
   const unsigned epoch = (unsigned)(t / a.nb) + 1u;
   const unsigned ov = (unsigned)a.order[t % a.nb];
   const unsigned blk = ov & kBlockMask;
-  __shared__ double scan_sm[kSweepWarps * kScanScratch];
-  double *scratch = scan_sm + (threadIdx.x >> 5) * kScanScratch;
   RowState<T> st;
   if constexpr (BWD) bwd_load<T, MODE>(a, ov, lane, st);
   else fwd_load<T, MODE>(a, ov, lane, st);
   wait_deps(a.dep_off, a.dep_ids, a.flags, blk, epoch, a.err, lane);
-  if constexpr (BWD) bwd_finish_block<T, MODE>(a, ov, lane, GlobalX<T>{a.out}, st, scratch);
-  else fwd_finish_block<T, MODE>(a, ov, lane, GlobalX<T>{a.out}, st, scratch);
+  if constexpr (BWD) bwd_finish_block<T, MODE>(a, ov, lane, GlobalX<T>{a.out}, st);
+  else fwd_finish_block<T, MODE>(a, ov, lane, GlobalX<T>{a.out}, st);
   publish_block(a.flags + blk, epoch, lane);
 }
 
@@ -534,7 +503,6 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nw = blockDim.x >> 5;
-  double *scratch = nullptr;  // no polling warps here: shuffle scan
   const SharedX<T> X{xs};
   // A software pipeline over the levels: while a level runs, each warp
   // holds its first block of the next level fully loaded and the row arrays
@@ -575,8 +543,8 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
         load1(ov, st);
         load2(ov, st);
       }
-      if constexpr (BWD) bwd_finish_block<T, MODE>(a, ov, lane, X, st, scratch);
-      else fwd_finish_block<T, MODE>(a, ov, lane, X, st, scratch);
+      if constexpr (BWD) bwd_finish_block<T, MODE>(a, ov, lane, X, st);
+      else fwd_finish_block<T, MODE>(a, ov, lane, X, st);
     }
     // advance: next level's block gets its second stage, the block two
     // levels ahead its first
