@@ -59,14 +59,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 }
 
 // Wait for the phase with the given parity to complete, giving up after
-// `limit_ns` of wall-clock time.  Returns false on timeout.
+// `limit_ns` of wall-clock time.  Returns false on timeout.  The clock is
+// read every 1,024 polls only: timer reads in busy poll loops slow the
+// other warps' shuffles and shared-memory accesses on the SM.
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
                                                   uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
-  while (true) {
+  for (uint32_t it = 1;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (global_timer_ns() - t0 > limit_ns) return false;
+    if ((it & 1023u) == 0 && global_timer_ns() - t0 > limit_ns) return false;
   }
 }
 

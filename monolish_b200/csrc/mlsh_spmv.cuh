@@ -178,10 +178,10 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
           const uint32_t par = (uint32_t)((k / STAGES - 1) & 1);
           const uint64_t t0 = global_timer_ns();
           ok = 0;
-          while (true) {
+          for (uint32_t it = 1;; ++it) {
             if (mbar_try_wait(empty0 + 8 * s, par)) { ok = 1; break; }
-            if (flags[kFlagConsAbort]) break;
-            if (global_timer_ns() - t0 > kWaitLimitNs) {
+            if ((it & 63u) == 0 && flags[kFlagConsAbort]) break;
+            if ((it & 1023u) == 0 && global_timer_ns() - t0 > kWaitLimitNs) {
               atomicExch(a.err, MLSH_ERR_TIMEOUT);
               break;
             }
@@ -218,10 +218,10 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
         const uint32_t par = (uint32_t)((kk / STAGES) & 1);
         const uint64_t t0 = global_timer_ns();
         bool ok = false;
-        while (true) {
+        for (uint32_t it = 1;; ++it) {
           if (mbar_try_wait(empty0 + 8 * s, par)) { ok = true; break; }
-          if (flags[kFlagConsAbort]) break;
-          if (global_timer_ns() - t0 > kWaitLimitNs) break;
+          if ((it & 63u) == 0 && flags[kFlagConsAbort]) break;
+          if ((it & 1023u) == 0 && global_timer_ns() - t0 > kWaitLimitNs) break;
         }
         if (!ok) { aborted = true; break; }
       }
