@@ -708,7 +708,11 @@ def run_precond(args, wl, rank, world, local):
                          "note": "algorithmic bytes of one apply / apply time against HBM; the "
                                  "sweeps are bound by their dependency chains: an apply is "
                                  f"{hops} block levels long, each one wait for another warp"},
-            "gpu_launches": args.steps * (res.iters * (6 if wl["solver"] == "cg" else 9) + 4),
+            # per iteration: CG 6 (SpMV, x/r update, 2 sweeps, z.r, p update),
+            # BiCGSTAB 9 (p, 2 sweeps, SpMV, s, 2 sweeps, SpMV, x/r); set-up of a
+            # solve: CG 4 (SpMV, 2 sweeps, init), BiCGSTAB 2 (SpMV, init)
+            "gpu_launches": args.steps * (res.iters * (6 if wl["solver"] == "cg" else 9) +
+                                          (4 if wl["solver"] == "cg" else 2)),
         }
         if world == 1 and not args.no_cpu:
             import oracle
