@@ -999,11 +999,16 @@ def serve_requests(count, seed=4, lo=1e3, hi=2e6):
     return reqs
 
 
-def serve_stream(D, reqs, rate, budget, lanes, seed, maxiter):
+def serve_stream(D, reqs, rate, budget, lanes, seed, maxiter, start=None):
     """Submit `reqs` at Poisson arrival times (rate req/s) from a producer
     thread; returns per-request results and (serving-kernel launches, lane
-    solves) during the stream."""
+    solves) during the stream.  `start`, if given, is called after the
+    warm-up and before the first arrival (a barrier across ranks)."""
     import threading
+    if not reqs:  # a rank with no share still takes the barrier
+        if start is not None:
+            start()
+        return [], (0, 0)
     srv = D.Server(budget, lanes)
     # warm-up: the smallest request of each kind and precision (serving
     # kernels, lanes, their first launches); not part of the stream
@@ -1026,6 +1031,8 @@ def serve_stream(D, reqs, rate, budget, lanes, seed, maxiter):
             ids[k] = srv.submit(q["kind"], q["rp"], q["ci"], q["v"], q["b"], q["tol"], maxiter,
                                 precision=q["precision"], inner_tol=SERVE_INNER_TOL)
 
+    if start is not None:
+        start()
     l0, s0 = srv.stats()
     th = threading.Thread(target=producer)
     th.start()
@@ -1064,12 +1071,51 @@ def solve_bytes(q, iters):
     return iters * (sp + 13 * n * 8 if q["kind"] == "cg" else 2 * sp + 22 * n * 8)
 
 
+def gather_parts(obj, world):
+    """Every rank's `obj` (a small dict of host results), in rank order;
+    a reporting exchange after the timed region, not part of the solves."""
+    if world == 1:
+        return [obj]
+    import torch.distributed as dist
+    out = [None] * world
+    dist.all_gather_object(out, obj)
+    return out
+
+
+def serve_entry(rate, parts):
+    """One sweep entry of the whole job from the ranks' stream results:
+    latencies pooled, makespan the longest rank's."""
+    lat = np.concatenate([np.asarray(p["lat"], np.float64) for p in parts])
+    span = max(p["span"] for p in parts)
+    return {"rate_req_s": rate, "solves_per_s": round(len(lat) / span, 2),
+            "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
+            "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
+            "makespan_s": round(span, 3),
+            "all_converged": all(p["ok"] for p in parts),
+            "ring_requests": sum(p["ring"] for p in parts),
+            "lane_requests": sum(p["lane"] for p in parts)}
+
+
 def run_serve(args, wl, rank, world, local):
     import torch
     from monolish_b200 import device as D
     torch.cuda.set_device(local)
     count = args.size or wl["count"]
-    reqs = serve_requests(count, seed=4)
+    reqs_all = serve_requests(count, seed=4)
+    reqs, start = reqs_all, None
+    if world > 1:
+        # requests are independent: each rank serves its share (placed by
+        # footprint) as a stream of its own at its share of the arrival
+        # rate; no collective on the data path, the ranks only start each
+        # stream together and merge their results afterwards
+        import torch.distributed as dist
+        from monolish_b200.shard import footprint_bytes, shard_by_footprint
+        nk = np.array([len(q["b"]) for q in reqs_all], np.int64)
+        zk = np.array([int(q["rp"][-1]) for q in reqs_all], np.int64)
+        mine = shard_by_footprint(footprint_bytes(nk, zk), world)[rank]
+        reqs = [reqs_all[i] for i in mine]
+        start = dist.barrier
+    share = len(reqs) / count
     rates = [float(r) for r in args.rates.split(",")]
     budget, lanes, maxiter = int(wl["budget"]), args.lanes, 100000
     h = D.Handle()
@@ -1079,41 +1125,48 @@ def run_serve(args, wl, rank, world, local):
     for k, rate in enumerate(rates):
         if k == len(rates) - 1:
             clocks.start()
-        res, (launches, lane_solves) = serve_stream(D, reqs, rate, budget, lanes, 40 + k,
-                                                    maxiter)
-        lat = np.array([r.t_done - r.t_submit for r in res])
-        span = max(r.t_done for r in res) - min(r.t_submit for r in res)
-        entry = {"rate_req_s": rate, "solves_per_s": round(len(res) / span, 2),
-                 "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
-                 "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
-                 "makespan_s": round(span, 3),
-                 "all_converged": all(r.status == 0 for r in res),
-                 "ring_requests": sum(1 for r in res if r.path == 0),
-                 "lane_requests": sum(1 for r in res if r.path == 1)}
+        res, (launches, lane_solves) = serve_stream(D, reqs, rate * share, budget, lanes,
+                                                    40 + k + 1000 * rank, maxiter, start)
+        part = {"lat": [r.t_done - r.t_submit for r in res],
+                "span": (max(r.t_done for r in res) - min(r.t_submit for r in res)
+                         if res else 0.0),
+                "ok": all(r.status == 0 for r in res),
+                "ring": sum(1 for r in res if r.path == 0),
+                "lane": sum(1 for r in res if r.path == 1)}
+        got = gather_parts(part, world)
+        entry = serve_entry(rate, got)
         sweep.append(entry)
-        head = (res, span, launches, lane_solves, entry)
+        head = (res, launches, lane_solves, entry, max(p["span"] for p in got))
     cl = clocks.stop()
-    res, span, launches, lane_solves, entry = head
+    res, launches, lane_solves, entry, span = head
     loop_s = None
-    if not args.quick:
+    if not args.quick and world == 1:
         loop_s, _ = serve_loop_of_single_solves(D, h, reqs, maxiter)
     h.close()
     # true residual of every request, recomputed on the host in FP64
-    worst = max(true_relres(q["rp"], q["ci"], q["v"], q["b"], r.x) / q["rel"]
-                for q, r in zip(reqs, res))
+    worst_mine = max((true_relres(q["rp"], q["ci"], q["v"], q["b"], r.x) / q["rel"]
+                      for q, r in zip(reqs, res)), default=0.0)
+    bytes_mine = float(sum(solve_bytes(q, r.iters) for q, r in zip(reqs, res)
+                           if q["precision"] == "fp64"))
+    parts = gather_parts({"worst": worst_mine, "bytes": bytes_mine,
+                          "launches": int(launches + lane_solves)}, world)
+    if rank != 0:
+        return None
+    worst = max(p["worst"] for p in parts)
+    bytes_all = sum(p["bytes"] for p in parts)
+    launches_all = sum(p["launches"] for p in parts)
+    reqs = reqs_all
     peak, peak_kind = measured_peak()
-    bytes_all = float(sum(solve_bytes(q, r.iters) for q, r in zip(reqs, res)
-                          if q["precision"] == "fp64"))
     h2d = int(sum(q["rp"].nbytes + q["ci"].nbytes + q["v"].nbytes + q["b"].nbytes
                   for q in reqs))
     d2h = int(sum(q["b"].nbytes for q in reqs))
-    value = len(res) / span
+    value = count / span
     fam = {f: sum(1 for q in reqs if q["family"] == f) for f in ("cg2d", "cg3d", "bicgstab")}
     out = {
         "metric": METRIC_SERVE, "value": round(value, 2), "unit": "solves/s",
         "n_gpus": world, "steps": 1, "warmup": args.warmup,
         "ms_per_step": round(span * 1e3, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64 / f32-inner mixed",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64 / f32-inner mixed",
         "data": "synthetic (seeded generators)",
         "config": {"workload": f"open-loop stream of {count} requests (seed 4): CG on 2D/3D "
                                "variable-coefficient diffusion or BiCGSTAB on convection-"
@@ -1129,7 +1182,9 @@ def run_serve(args, wl, rank, world, local):
                    "worst_true_rel_residual_over_tol": worst,
                    "all_converged": entry["all_converged"],
                    "l2": "no flush: each request's matrix is uploaded from the host",
-                   "parallelism": "one GPU: serving-kernel rings + worker lanes"},
+                   "parallelism": ("one GPU: serving-kernel rings + worker lanes" if world == 1
+                                   else f"requests sharded by footprint over {world} GPUs, "
+                                        "each serving its share at its share of the rate")},
         "sweep": sweep,
         "e2e": {"value": round(value, 2), "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
@@ -1139,7 +1194,7 @@ def run_serve(args, wl, rank, world, local):
                      "frac": round(bytes_all / span / 1e9 / peak, 4), "peak_kind": peak_kind,
                      "traffic": None,
                      "note": "algorithmic solve bytes of the FP64 requests only / makespan"},
-        "gpu_launches": int(launches + lane_solves),
+        "gpu_launches": int(launches_all),
         "gpu_launches_note": "serving-kernel launches + lane solves (a lower bound: each "
                              "lane solve launches one graph or cluster kernel at least)",
     }
@@ -1148,7 +1203,7 @@ def run_serve(args, wl, rank, world, local):
             "value": round(count / loop_s, 2), "unit": "solves/s",
             "speedup_of_server": round(value / (count / loop_s), 2),
             "note": "same requests one at a time, plain FP64, wall time"}
-    if not args.no_cpu:
+    if world == 1 and not args.no_cpu:
         cb = cpu_reference_serve(reqs, seconds=20.0)
         if cb:
             out["cpu_baseline"] = cb
