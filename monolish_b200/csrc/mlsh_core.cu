@@ -178,44 +178,49 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
   a.err = h.err_flag;
   const int v = p.variant;
   const int g = p.spmv_grid[v];
+  cudaError_t e = cudaSuccess;
   if constexpr (sizeof(VT) == 4) {
     if (p.col16 != nullptr) {
       switch (v) {
         case 1:
-          spmv_kernel_ptr<VT, M0, M1, 1, true>()
-              <<<g, kSpmvThreads, spmv_smem_bytes<VT, 1, true>(), stream>>>(a);
+          e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 1, true>(), g, kSpmvThreads,
+                               spmv_smem_bytes<VT, 1, true>(), stream, a);
           break;
         case 2:
-          spmv_kernel_ptr<VT, M0, M1, 2, true>()
-              <<<g, kSpmvThreads, spmv_smem_bytes<VT, 2, true>(), stream>>>(a);
+          e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 2, true>(), g, kSpmvThreads,
+                               spmv_smem_bytes<VT, 2, true>(), stream, a);
           break;
         case 3:
-          spmv_kernel_ptr<VT, M0, M1, 3, true>()
-              <<<g, kSpmvThreads, spmv_smem_bytes<VT, 3, true>(), stream>>>(a);
+          e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 3, true>(), g, kSpmvThreads,
+                               spmv_smem_bytes<VT, 3, true>(), stream, a);
           break;
         default:
-          spmv_kernel_ptr<VT, M0, M1, 0, true>()
-              <<<g, kSpmvThreads, spmv_smem_bytes<VT, 0, true>(), stream>>>(a);
+          e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 0, true>(), g, kSpmvThreads,
+                               spmv_smem_bytes<VT, 0, true>(), stream, a);
           break;
       }
-      return cudaGetLastError();
+      return e;
     }
   }
   switch (v) {
     case 1:
-      spmv_kernel_ptr<VT, M0, M1, 1>()<<<g, kSpmvThreads, spmv_smem_bytes<VT, 1>(), stream>>>(a);
+      e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 1>(), g, kSpmvThreads,
+                           spmv_smem_bytes<VT, 1>(), stream, a);
       break;
     case 2:
-      spmv_kernel_ptr<VT, M0, M1, 2>()<<<g, kSpmvThreads, spmv_smem_bytes<VT, 2>(), stream>>>(a);
+      e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 2>(), g, kSpmvThreads,
+                           spmv_smem_bytes<VT, 2>(), stream, a);
       break;
     case 3:
-      spmv_kernel_ptr<VT, M0, M1, 3>()<<<g, kSpmvThreads, spmv_smem_bytes<VT, 3>(), stream>>>(a);
+      e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 3>(), g, kSpmvThreads,
+                           spmv_smem_bytes<VT, 3>(), stream, a);
       break;
     default:
-      spmv_kernel_ptr<VT, M0, M1, 0>()<<<g, kSpmvThreads, spmv_smem_bytes<VT, 0>(), stream>>>(a);
+      e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 0>(), g, kSpmvThreads,
+                           spmv_smem_bytes<VT, 0>(), stream, a);
       break;
   }
-  return cudaGetLastError();
+  return e;
 }
 
 #define MLSH_INST_SPMV(VT, A, B)                                                 \

@@ -154,6 +154,28 @@ struct CsrPlan {
   int *tile_base = nullptr;       // device, n_tiles
 };
 
+// ------------------------------------------------------------ launches ---
+// Launch kernel `k` as a programmatic dependent of the stream's previous
+// kernel: its CTAs may start while that kernel's last CTAs retire, and the
+// kernel waits (griddepcontrol.wait, first thing) until the previous one has
+// completed and its writes are visible.  Only kernels that make that wait
+// before touching global memory may be launched this way.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dependent(void (*k)(KArgs...), int grid, int block, size_t smem,
+                                    cudaStream_t s, Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, static_cast<Args &&>(args)...);
+}
+
 // -------------------------------------------------------------- errors ---
 void set_last_error(const char *where, cudaError_t e);
 

@@ -717,15 +717,13 @@ cudaError_t run_body(const Handle &h, int64_t n, const Body &b, const int *done,
     constexpr int W = 16 / (int)sizeof(typename Body::elem);
     if (b.aligned()) {
       constexpr auto k = vec_pack_kernel<NR, FIN, W, Body>;
-      k<<<pack_grid<k>(n, W, h.num_sms), kVecThreads, 0, s>>>(n, b, ra);
-    } else {
-      constexpr auto k = vec_pack_kernel<NR, FIN, 1, Body>;
-      k<<<pack_grid<k>(n, 1, h.num_sms), kVecThreads, 0, s>>>(n, b, ra);
+      return launch_dependent(k, pack_grid<k>(n, W, h.num_sms), kVecThreads, 0, s, n, b, ra);
     }
+    constexpr auto k = vec_pack_kernel<NR, FIN, 1, Body>;
+    return launch_dependent(k, pack_grid<k>(n, 1, h.num_sms), kVecThreads, 0, s, n, b, ra);
   } else {
-    vec_kernel<NR, FIN, Body><<<g, kVecThreads, 0, s>>>(n, b, ra);
+    return launch_dependent(vec_kernel<NR, FIN, Body>, g, kVecThreads, 0, s, n, b, ra);
   }
-  return cudaGetLastError();
 }
 
 enum Kind { kCG = 0, kBiCGSTAB = 1, kMixedBiCGSTAB = 3, kSOR = 4 };

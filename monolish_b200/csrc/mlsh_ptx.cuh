@@ -117,4 +117,15 @@ __device__ __forceinline__ void st_release_gpu(uint32_t *p, uint32_t v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Programmatic dependent launch: wait until the preceding kernel of the
+// stream has completed and its memory is visible (returns at once when
+// this kernel was not launched as a programmatic dependent), and let the
+// next kernel, if launched as one, start its CTAs as this grid's retire.
+__device__ __forceinline__ void pdl_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 }  // namespace mlsh

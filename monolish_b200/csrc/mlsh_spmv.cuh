@@ -140,6 +140,8 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
   constexpr int NR = (M0 != kDotNone ? 1 : 0) + (M1 != kDotNone ? 1 : 0);
   using L = SpmvSmem<VT, STAGES, C16 ? 2 : 4>;
   extern __shared__ __align__(128) unsigned char smem[];
+  pdl_wait();
+  pdl_launch_dependents();
   if (a.done != nullptr && *a.done != 0) return;
 
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::kBarOff);

@@ -24,6 +24,8 @@ struct RedArgs {
 template <int NR, bool FIN, typename Body>
 __global__ void __launch_bounds__(kVecThreads)
     vec_kernel(int64_t n, Body body, RedArgs ra) {
+  pdl_wait();
+  pdl_launch_dependents();
   if (ra.done != nullptr && *ra.done != 0) return;
   constexpr int NA = NR > 0 ? NR : 1;
   __shared__ double red[kVecThreads / 32 * NA];
@@ -69,6 +71,8 @@ inline bool al16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 template <int NR, bool FIN, int W, typename Body>
 __global__ void __launch_bounds__(kVecThreads)
     vec_pack_kernel(int64_t n, Body body, RedArgs ra) {
+  pdl_wait();
+  pdl_launch_dependents();
   if (ra.done != nullptr && *ra.done != 0) return;
   constexpr int NA = NR > 0 ? NR : 1;
   __shared__ double red[kVecThreads / 32 * NA];
