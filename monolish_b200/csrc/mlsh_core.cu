@@ -176,7 +176,15 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
   a.dot_out = dot_out;
   a.done = done;
   a.err = h.err_flag;
-  const int v = p.variant;
+  int v = p.variant;
+  // FP64 with two fused dots does not fit 4 CTAs per SM (56 registers: it
+  // spills); it runs the same pipeline depth at 3 CTAs per SM instead
+  if constexpr (sizeof(VT) == 8 && M0 != kDotNone && M1 != kDotNone) {
+    static_assert(kSpmvVariants[2].min_blocks == 4 && kSpmvVariants[1].min_blocks == 3 &&
+                      kSpmvVariants[1].stages == kSpmvVariants[2].stages,
+                  "variant 1 is variant 2 at 3 CTAs per SM");
+    if (v == 2) v = 1;
+  }
   const int g = p.spmv_grid[v];
   cudaError_t e = cudaSuccess;
   if constexpr (sizeof(VT) == 4) {
