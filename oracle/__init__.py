@@ -176,6 +176,8 @@ class Reference:
         if not os.path.exists(path):
             raise OSError(f"reference CPU build not present: {path}")
         os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+        # read by the OpenMP runtime when the library loads
+        os.environ.setdefault("OMP_PROC_BIND", "close")
         self.lib = lib = C.CDLL(path)
         I, L, D = C.c_int, C.c_long, C.c_double
         lib.ref_max_threads.restype = I
