@@ -505,9 +505,11 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
   const int nw = blockDim.x >> 5;
   const SharedX<T> X{xs};
   // A software pipeline over the levels: while a level runs, each warp
-  // holds its first block of the next level fully loaded and the row arrays
-  // of its first block two levels ahead, so the two dependent loads of a
-  // row's state overlap two levels' work and barriers.
+  // holds its first block of the next two levels fully loaded and the row
+  // arrays of its first block three levels ahead, so the two dependent
+  // loads of a row's state overlap two to three levels' work and barriers
+  // (the loads read only the matrix and the sweep's right-hand side, which
+  // no level writes).
   auto load1 = [&](unsigned o, RowState<T> &st) {
     if constexpr (BWD) bwd_load1<T, MODE>(a, o, lane, st);
     else fwd_load1<T, MODE>(a, o, lane, st);
@@ -516,20 +518,27 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
     if constexpr (BWD) bwd_load2<T, MODE>(a, o, st);
     else fwd_load2<T, MODE>(a, st);
   };
-  RowState<T> cur, nxt;
-  unsigned ov_cur = 0, ov_nxt = 0;
-  bool have_cur = false, have_nxt = false;
-  if (levels > 0 && s_loff[0] + warp < s_loff[1]) {
-    ov_cur = (unsigned)s_order[s_loff[0] + warp];
+  // this warp's first block of level lv, if it has one
+  auto first_of = [&](int lv, unsigned &ov) -> bool {
+    if (lv >= levels || s_loff[lv] + warp >= s_loff[lv + 1]) return false;
+    ov = (unsigned)s_order[s_loff[lv] + warp];
+    return true;
+  };
+  RowState<T> cur, nxt, nn;
+  unsigned ov_cur = 0, ov_nxt = 0, ov_nn = 0;
+  const bool have0 = first_of(0, ov_cur);
+  if (have0) {
     load1(ov_cur, cur);
     load2(ov_cur, cur);
-    have_cur = true;
   }
-  if (levels > 1 && s_loff[1] + warp < s_loff[2]) {
-    ov_nxt = (unsigned)s_order[s_loff[1] + warp];
+  bool have_cur = have0;
+  bool have_nxt = first_of(1, ov_nxt);
+  if (have_nxt) {
     load1(ov_nxt, nxt);
-    have_nxt = true;
+    load2(ov_nxt, nxt);
   }
+  bool have_nn = first_of(2, ov_nn);
+  if (have_nn) load1(ov_nn, nn);
   for (int lv = 0; lv < levels; ++lv) {
     const int q1 = s_loff[lv + 1];
     for (int q = s_loff[lv] + warp; q < q1; q += nw) {
@@ -546,20 +555,21 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
       if constexpr (BWD) bwd_finish_block<T, MODE>(a, ov, lane, X, st);
       else fwd_finish_block<T, MODE>(a, ov, lane, X, st);
     }
-    // advance: next level's block gets its second stage, the block two
-    // levels ahead its first
+    // advance: the next level's block is ready, the one after it gets its
+    // second stage, the block three levels ahead its first
     have_cur = have_nxt;
     if (have_nxt) {
       cur = nxt;
       ov_cur = ov_nxt;
-      load2(ov_cur, cur);
     }
-    have_nxt = false;
-    if (lv + 2 < levels && s_loff[lv + 2] + warp < s_loff[lv + 3]) {
-      ov_nxt = (unsigned)s_order[s_loff[lv + 2] + warp];
-      load1(ov_nxt, nxt);
-      have_nxt = true;
+    have_nxt = have_nn;
+    if (have_nn) {
+      nxt = nn;
+      ov_nxt = ov_nn;
+      load2(ov_nxt, nxt);
     }
+    have_nn = first_of(lv + 3, ov_nn);
+    if (have_nn) load1(ov_nn, nn);
     __syncthreads();
   }
   for (int i = threadIdx.x; i < a.n; i += blockDim.x) a.out[i] = xs[i];
