@@ -1241,9 +1241,18 @@ def cpu_reference_serve(reqs, seconds):
 
 
 # ---------------------------------------------------------- reference arm
+ORACLE_GEN_LIB = os.path.join(ROOT, "oracle", "_build", "libmlsh_gen_oracle.so")
+
+
 def run_reference(args, wl, rank, world):
     if rank != 0:
         return None
+    # the reference arm maps no library of the product: its inputs come from
+    # the oracle-side build of the same generator source (same bytes)
+    from monolish_b200 import workloads as W
+    if not os.path.exists(ORACLE_GEN_LIB):
+        subprocess.run(["make", "-s", "gen"], cwd=os.path.join(ROOT, "oracle"), check=True)
+    W.set_library(ORACLE_GEN_LIB)
     if wl["kind"] == "serve":
         reqs = serve_requests(args.size or wl["count"], seed=4)
         cb = cpu_reference_serve(reqs, seconds=60.0)

@@ -6,8 +6,8 @@
 * ``lib/libmonolish_b200.so`` -- the C++ drop-in layer (monolish's class and
   function names) over the C ABI.
 * the checker libraries under ``oracle/`` (``make -C oracle``): the C
-  restatement always, the reference CPU build when the reference tree is
-  present.
+  restatement and the generators' oracle-side copy always, the reference CPU
+  build when ``MONOLISH_REF`` names the reference source tree.
 """
 from __future__ import annotations
 
@@ -80,12 +80,21 @@ def build_facade(force=False):
 
 
 def build_oracle():
-    """Checker libraries (test infrastructure only)."""
+    """Checker libraries (test infrastructure only).
+
+    The C restatement and the oracle-side copy of the generators always; the
+    reference CPU build only when ``MONOLISH_REF`` names a monolish source
+    tree (its ``src/`` is compiled in place, outputs go to ``oracle/_ref``)."""
     oracle = os.path.join(ROOT, "oracle")
-    target = ["restatement"]
-    if os.path.isdir("/root/reference/src"):
+    target = ["restatement", "gen"]
+    ref = os.environ.get("MONOLISH_REF", "")
+    extra = []
+    if ref and os.path.isdir(os.path.join(ref, "src")):
         target.append("ref")
-    _run(["make", "-s", "-j", str(os.cpu_count() or 4), *target], cwd=oracle)
+        extra.append(f"REF={ref}")
+    elif not os.path.exists(os.path.join(oracle, "_ref", "libmlsh_refcapi.so")):
+        print("oracle/_ref not built: set MONOLISH_REF to a monolish source tree", flush=True)
+    _run(["make", "-s", "-j", str(os.cpu_count() or 4), *target, *extra], cwd=oracle)
 
 
 def build_all(force=False):

@@ -21,9 +21,12 @@
 // Host code never hands the array's name to a kernel: on the host that name
 // is only a stand-in, not a device address.
 //
-// Sharing: every call uses the same array and leaves its contents behind;
-// each call clears the arrival counter (cudaMemsetAsync, no allocation)
-// before its kernel runs.  Calls whose kernels overlap on the GPU (e.g. on
+// Sharing: every call uses the same array and leaves its contents behind.
+// A completed launch leaves the arrival counter at zero (the last CTA resets
+// it), but a launch that was aborted partway (an earlier error on the
+// stream, a context that was torn down mid-kernel) can leave it counting, so
+// each call still clears it (cudaMemsetAsync, no allocation) before its
+// kernel runs.  Calls whose kernels overlap on the GPU (e.g. on
 // two streams without ordering between them) race on the array and give
 // wrong results: order them on one stream, or use mlsh_dot_device with one
 // handle per stream.
@@ -33,6 +36,7 @@
 
 #include "mlsh_internal.cuh"
 #include "mlsh_reduce.cuh"
+#include "mlsh_vec.cuh"
 
 namespace mlsh {
 
@@ -43,6 +47,11 @@ constexpr int kNoAllocMaxCtas = 2048;
 constexpr size_t kNoAllocCounterBytes = 256;
 constexpr size_t kNoAllocScratchBytes =
     kNoAllocCounterBytes + sizeof(double) * (size_t)kNoAllocMaxCtas;  // 16,640
+// vec_grid caps the grid at kMaxVecBlocksPerSm CTAs per SM: 148 x 8 = 1,184
+// on a B200, well inside the partials above; a device with more than 256
+// SMs is rejected at call time.
+static_assert(kMaxVecBlocksPerSm * 256 <= kNoAllocMaxCtas,
+              "static scratch must hold the partials of a 256-SM device");
 
 static __device__ __align__(256) unsigned char g_dot_scratch[kNoAllocScratchBytes];
 
@@ -105,14 +114,6 @@ __global__ void __launch_bounds__(kVecThreads)
   }
 }
 
-int grid_for(int64_t n, int num_sms) {
-  int64_t g = (n + (int64_t)kVecThreads * 4 - 1) / ((int64_t)kVecThreads * 4);
-  const int64_t cap = (int64_t)num_sms * kMaxVecBlocksPerSm;
-  if (g > cap) g = cap;
-  if (g < 1) g = 1;
-  return (int)g;
-}
-
 }  // namespace
 }  // namespace mlsh
 
@@ -130,7 +131,7 @@ extern "C" int mlsh_dot_noalloc(int dtype, int64_t n, const void *d_x, const voi
     MLSH_CUDA_TRY(cudaMemsetAsync(d_result, 0, sizeof(double), cs));
     return MLSH_SUCCESS;
   }
-  const int grid = grid_for(n, s.num_sms);
+  const int grid = vec_grid(n, s.num_sms);  // the grid mlsh_dot_device uses
   if (grid > kNoAllocMaxCtas) {
     set_last_error_text(
         "mlsh_dot_noalloc: this device needs more CTA partials than the static scratch "

@@ -31,3 +31,23 @@ def test_reference_arm_json(reference, args):
     if "precond_ilu" in args[1]:
         # the reference has no CPU ILU: the oracle's restatement stands in
         assert out["cpu_baseline"]["kind"] == "port" and out["cpu_baseline"]["cores"] == 1
+
+
+@pytest.mark.parametrize("workload", ["spmv_poisson3d_f64", "cg_poisson2d"])
+def test_reference_arm_maps_no_product_library(reference, workload):
+    """The reference arm runs only the reference build and the oracle-side
+    generator: no library under monolish_b200/lib is mapped."""
+    code = (
+        "import sys, types, bench\n"
+        f"sys.argv = ['bench.py', '--impl', 'reference', '--workload', '{workload}', "
+        "'--size', '16', '--steps', '1', '--warmup', '3']\n"
+        "bench.main()\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "libs = sorted({l.split()[-1] for l in maps.splitlines() if l.endswith('.so')})\n"
+        "print('MAPS', [p for p in libs if '/monolish_b200/' in p or '/oracle/' in p])\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [x for x in r.stdout.splitlines() if x.startswith("MAPS")][-1]
+    assert "monolish_b200/lib" not in line, line
+    assert "libmlsh_gen_oracle.so" in line and "libmonolish_cpu.so" in line, line

@@ -4,8 +4,10 @@ a latency-critical loop that cannot take cudaMalloc's implicit
 synchronisation).  Its scratch is a static device array shared by every
 call, so this test makes two calls in a row (different sizes, so the second
 reuses what the first left in the array) and checks each against the
-allocating entry point mlsh_dot_device, through the C ABI, within the
-tolerance the other dot tests use: |err| <= 1e-14 * sum|x_i y_i|.
+allocating entry point mlsh_dot_device, through the C ABI.  Both run the
+same grid and summation order on the same stream, so their results must be
+identical bit for bit; against numpy's FP64 dot the bar is the one the other
+dot tests use, |err| <= 1e-14 * sum|x_i y_i|.
 
 Named test_zz_* so that pytest collects it last."""
 import ctypes
@@ -47,9 +49,20 @@ def test_dot_noalloc_matches_dot_device_twice(handle):
         got, ref = _dot_pair(handle, lib, x, y, code)
         tol = 1e-14 * np.abs(a.astype(np.float64) * b.astype(np.float64)).sum()
         assert np.isfinite(got)
-        assert abs(got - ref) <= tol, (dt, n, got, ref)
+        assert got == ref, (dt, n, got, ref)
         exact = float(np.dot(a.astype(np.float64), b.astype(np.float64)))
         assert abs(got - exact) <= tol
+
+
+def test_dot_noalloc_empty_is_zero():
+    import torch
+    lib = _abi.load()
+    out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _abi.check(lib.mlsh_dot_noalloc(_abi.F64, 0, None, None, out.data_ptr(), stream),
+               "mlsh_dot_noalloc")
+    torch.cuda.synchronize()
+    assert out.item() == 0.0
 
 
 def test_dot_noalloc_rejects_bad_arguments():
