@@ -36,8 +36,16 @@ Cases (all small, so the CPU restatement replays them in seconds):
                SOR::solve on the 16x16 Poisson matrix (b = ones, tol 1e-8 /
                1e-4); CG and BiCGSTAB preconditioned by SOR on poisson16.
 
+  fullsize     the measured configurations at full size, as summaries:
+               SpMV on the 3D 7-point 256^3 Laplacian and the n = 4,194,304
+               Zipf(2) matrix (FP64 and FP32): sum, sum of |y| and 4,096
+               sampled rows; Jacobi-BiCGSTAB on the 160^3 convection-
+               diffusion system (status, iterations, residuals); Jacobi-CG on
+               each of the 2,048 batch systems (status, iterations).
+
     python tests/golden/make_golden.py setup     # that case only
     python tests/golden/make_golden.py precond   # that case only
+    python tests/golden/make_golden.py fullsize  # that case only (minutes)
 """
 import os
 import sys
@@ -126,11 +134,60 @@ def precond_case(ref):
     return out
 
 
+def sample_rows(n, count=4096):
+    return np.linspace(0, n - 1, count).round().astype(np.int64)
+
+
+def fullsize_case(ref):
+    """The measured configurations at full size.  Only small summaries are
+    stored (the inputs are regenerated from their seeds by the tests):
+    SpMV outputs as their sum, sum of |y| and 4,096 evenly spaced rows;
+    solves as (status, iterations, final residual) per system."""
+    ref.set_threads(os.cpu_count() or 1)
+    out = {}
+    # C2a / C2b SpMV, FP64 and FP32 (x as in the bench: U[-1,1], seed 1)
+    for tag, gen in (("lap256", lambda: W.poisson3d(256)),
+                     ("zipf4m", lambda: W.zipf(4194304, seed=1))):
+        n, rp, ci, v = gen()
+        x = W.uniform_fast(n, -1.0, 1.0, 1)
+        rows = sample_rows(n)
+        for sfx, dt in (("d", np.float64), ("s", np.float32)):
+            y = ref.spmv(rp, ci, v.astype(dt), x.astype(dt))[0].astype(np.float64)
+            out[f"{tag}_{sfx}_rows"] = rows
+            out[f"{tag}_{sfx}_y"] = y[rows]
+            out[f"{tag}_{sfx}_sum"] = np.array([y.sum(), np.abs(y).sum()])
+        del rp, ci, v, x
+        print(tag, "done", flush=True)
+    # C3: Jacobi-BiCGSTAB on the 160^3 convection-diffusion system, FP64
+    n, rp, ci, v = W.convdiff3d(160, peclet=10.0)
+    xt = W.uniform_mt(n, -1.0, 1.0, 2)
+    b = ref.spmv(rp, ci, v, xt)[0]
+    nb = float(np.linalg.norm(b))
+    st, it, res, x, sec = ref.bicgstab(rp, ci, v, b, np.zeros(n), 1e-10 * nb, 20000, precond=1)
+    r = b - ref.spmv(rp, ci, v, x)[0]
+    out["convdiff160_bicgstab"] = np.array([st, it, res, np.linalg.norm(r) / nb, nb])
+    out["convdiff160_b_sum"] = np.array([b.sum(), np.abs(b).sum()])
+    print("convdiff160", st, it, np.linalg.norm(r) / nb, f"{sec:.1f}s", flush=True)
+    # C4: the 2,048-system diffusion batch, Jacobi-CG to 1e-8 (x_true seed 3 + k)
+    systems = W.diffusion_batch(2048, seed=3)
+    rec = np.zeros((len(systems), 4))
+    for k, (rp, ci, v) in enumerate(systems):
+        nk = len(rp) - 1
+        b = ref.spmv(rp, ci, v, W.uniform_mt(nk, -1.0, 1.0, 3 + k))[0]
+        nb = float(np.linalg.norm(b))
+        st, it, res, x, _ = ref.cg(rp, ci, v, b, np.zeros(nk), 1e-8 * nb, 20000, precond=1)
+        rec[k] = (st, it, res, nb)
+    out["batch2048_cg"] = rec
+    print("batch2048 iters", int(rec[:, 1].sum()), flush=True)
+    return out
+
+
 def main(only=None):
     ref = oracle.Reference()
     out = {}
-    if only in ("setup", "precond"):
-        out[only] = setup_case(ref) if only == "setup" else precond_case(ref)
+    if only in ("setup", "precond", "fullsize"):
+        out[only] = {"setup": setup_case, "precond": precond_case,
+                     "fullsize": fullsize_case}[only](ref)
         for name, case in out.items():
             path = os.path.join(HERE, f"{name}.npz")
             np.savez_compressed(path, **case)

@@ -268,3 +268,31 @@ def test_zero_pivots_and_unsorted_rows(restatement):
     assert restatement.precond_factor(rp, ci, v, 3)[1] == 1
     with pytest.raises(ValueError):
         restatement.precond_factor(rp, np.array([1, 0, 0, 1], np.int32), v, 4)
+
+
+@pytest.mark.parametrize("tag", ["lap256", "zipf4m"])
+def test_fullsize_spmv_matches_reference_golden(restatement, tag):
+    """The restatement's SpMV at the measured sizes against the reference
+    build's (sampled rows and sums, FP64 and FP32)."""
+    g = golden("fullsize")
+    n, rp, ci, v = W.poisson3d(256) if tag == "lap256" else W.zipf(4194304, seed=1)
+    x = W.uniform_fast(n, -1.0, 1.0, 1)
+    for sfx, dt in (("d", np.float64), ("s", np.float32)):
+        y = restatement.spmv(rp, ci, v.astype(dt), x.astype(dt)).astype(np.float64)
+        rows = g[f"{tag}_{sfx}_rows"]
+        assert np.array_equal(y[rows], g[f"{tag}_{sfx}_y"])
+        assert np.array_equal(np.array([y.sum(), np.abs(y).sum()]), g[f"{tag}_{sfx}_sum"])
+
+
+def test_fullsize_batch_sample_matches_reference_golden(restatement):
+    """Every 64th system of the 2,048-system batch: the restatement's Jacobi-CG
+    iteration count equals the reference build's."""
+    g = golden("fullsize")["batch2048_cg"]
+    sizes = W.loguniform_sizes(2048, 1e3, 1e5, 3)
+    for k in range(0, 2048, 64):
+        nx, ny = W.grid2d_for(int(sizes[k]))
+        n, rp, ci, v = W.vardiff2d(nx, ny, 3, k)
+        b = restatement.spmv(rp, ci, v, W.uniform_mt(n, -1.0, 1.0, 3 + k))
+        st, it, _, _ = restatement.cg(rp, ci, v, b, np.zeros(n), 1e-8 * np.linalg.norm(b),
+                                      20000)
+        assert (st, it) == (int(g[k, 0]), int(g[k, 1])), (k, st, it, g[k])
