@@ -255,12 +255,17 @@ def run_spmv(args, wl, rank, world, local):
     A = D.Crs(h, n, n, rp, ci, v, validate=False)
     dx = torch.from_numpy(x).cuda()
     dy = torch.empty(n, dtype=dx.dtype, device="cuda")
+    # consecutive timed launches read two different copies of x, so no
+    # launch finds the x of the one before it in L2
+    dx2 = dx.clone()
     stream = torch.cuda.current_stream()
     lib, hh, plan = h.lib, h.h, A.plan
-    xp, yp = dx.data_ptr(), dy.data_ptr()
+    xps, yp = (dx.data_ptr(), dx2.data_ptr()), dy.data_ptr()
+    nlaunch = [0]
 
     def launch():
-        st = lib.mlsh_spmv(hh, plan, 1.0, xp, 0.0, yp)
+        st = lib.mlsh_spmv(hh, plan, 1.0, xps[nlaunch[0] & 1], 0.0, yp)
+        nlaunch[0] += 1
         if st != 0:
             raise _abi.MlshError(st, "spmv")
 
@@ -299,15 +304,20 @@ def run_spmv(args, wl, rank, world, local):
     h.sync()
 
     # ---- end to end through the C ABI with host buffers: every step copies
-    # its x in from pinned memory, runs the SpMV and copies its y out.  Two
-    # device buffer pairs and separate copy streams let step k+1's copy-in
-    # run while step k computes and copies out (PCIe is full duplex).
+    # its x in from pinned memory, runs the SpMV and copies its y out, the
+    # copies through the library's own stream-ordered mlsh_memcpy_*_async on
+    # handles bound to a copy-in and a copy-out stream.  Two device buffer
+    # pairs let step k+1's copy-in run while step k computes and copies out
+    # (PCIe is full duplex).
+    del dx2
     hx = torch.from_numpy(x).pin_memory()
     hys = [torch.empty(n, dtype=dx.dtype).pin_memory() for _ in range(2)]
     hy = hys[0]
     xs = [dx, torch.empty_like(dx)]
     ys = [dy, torch.empty_like(dy)]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    h_in, h_out = D.Handle(stream=s_in.cuda_stream), D.Handle(stream=s_out.cuda_stream)
+    xbytes = n * dx.element_size()
     ev_in = [torch.cuda.Event() for _ in range(2)]
     ev_sp = [torch.cuda.Event() for _ in range(2)]
     ev_out = [torch.cuda.Event() for _ in range(2)]
@@ -316,11 +326,11 @@ def run_spmv(args, wl, rank, world, local):
 
     def e2e_step(k):
         j = k % 2
-        with torch.cuda.stream(s_in):
-            if k >= 2:
-                s_in.wait_event(ev_sp[j])      # x_j no longer read by step k-2
-            xs[j].copy_(hx, non_blocking=True)
-            ev_in[j].record(s_in)
+        if k >= 2:
+            s_in.wait_event(ev_sp[j])          # x_j no longer read by step k-2
+        _abi.check(lib.mlsh_memcpy_h2d_async(h_in.h, xs[j].data_ptr(), hx.data_ptr(),
+                                             xbytes), "memcpy_h2d_async")
+        ev_in[j].record(s_in)
         stream.wait_event(ev_in[j])
         if k >= 2:
             stream.wait_event(ev_out[j])       # y_j copied out by step k-2
@@ -328,10 +338,10 @@ def run_spmv(args, wl, rank, world, local):
         if st != 0:
             raise _abi.MlshError(st, "spmv")
         ev_sp[j].record(stream)
-        with torch.cuda.stream(s_out):
-            s_out.wait_event(ev_sp[j])
-            hys[j].copy_(ys[j], non_blocking=True)
-            ev_out[j].record(s_out)
+        s_out.wait_event(ev_sp[j])
+        _abi.check(lib.mlsh_memcpy_d2h_async(h_out.h, hys[j].data_ptr(), ys[j].data_ptr(),
+                                             xbytes), "memcpy_d2h_async")
+        ev_out[j].record(s_out)
         return j
 
     if e2e_steps:
@@ -355,6 +365,8 @@ def run_spmv(args, wl, rank, world, local):
             dist.barrier()
     else:
         hy.copy_(dy)
+    h_in.close()
+    h_out.close()
 
     # correctness spot check: FP64 numpy row dots on a sample of rows
     y = hy.numpy()
@@ -393,13 +405,16 @@ def run_spmv(args, wl, rank, world, local):
             "data": "synthetic (seeded generators)",
             "config": {"workload": describe(wl), "n": n, "nnz": nnz,
                        "bytes_per_step": B, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (no flush needed)",
+                       "l2": "inputs larger than L2 (the matrix streamed L2 "
+                             "evict-first); consecutive launches read two different "
+                             "copies of x, so none finds the previous launch's x in L2",
                        "n_tiles": info["n_tiles"], "n_long_rows": info["n_long_rows"],
                        "spmv_variant": variant},
             "e2e": {"value": round(e2e_value, 2), "unit": "GB/s",
                     "h2d_bytes_per_step": n * vsz, "d2h_bytes_per_step": n * vsz,
                     "steps": e2e_steps,
-                    "note": "x in from pinned host memory and y out every step; step k+1's "
+                    "note": "x in from pinned host memory and y out every step through "
+                            "mlsh_memcpy_h2d_async / mlsh_memcpy_d2h_async; step k+1's "
                             "copy-in overlaps step k's SpMV and copy-out (two buffer pairs)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
@@ -548,7 +563,7 @@ def run_solve(args, wl, rank, world, local):
                 # iteration's attainable accuracy is about u32 * cond(A D^-1),
                 # so inner tolerances near it cost extra FP32 iterations
                 sweep = []
-                for itol in (1e-1, 1e-2, 1e-3):
+                for itol in (() if getattr(args, "no_sweep", False) else (1e-1, 1e-2, 1e-3)):
                     if itol == inner_tol:
                         continue
                     for _ in range(2):
@@ -567,7 +582,8 @@ def run_solve(args, wl, rank, world, local):
                                   "true_rel_residual": true_relres(rp, ci, v, b,
                                                                    dx.cpu().numpy()),
                                   "speedup_vs_plain_fp64": round(plain_ms / mt, 3)})
-                out["inner_tol_sweep"] = sweep
+                if sweep:
+                    out["inner_tol_sweep"] = sweep
         if world == 1 and not args.no_cpu:
             import oracle
             ref = oracle.reference_or_none()
@@ -1375,6 +1391,71 @@ def run_reference(args, wl, rank, world):
                     "d2h_bytes_per_step": 0}}
 
 
+def solve_records(args, rank, world, local):
+    """The solves/s half of the metric, measured in the same run as the
+    default SpMV line: 128x128 Jacobi-CG; 160^3 Jacobi-BiCGSTAB plain FP64
+    against mixed FP32/FP64 at inner tol 1e-4; the 2,048-system batch
+    (FP64 and mixed) against a loop of single plain solves.  Each record
+    carries its own timing (CUDA events, warm-up 3), iterations, true
+    relative residual and roofline fraction."""
+    def sub(**kw):
+        a = argparse.Namespace(**vars(args))
+        a.size, a.engine, a.cluster_rows, a.eager, a.inner_tol = 0, "auto", 0, False, None
+        a.variant, a.no_sweep, a.warmup = -1, True, 3
+        for k, val in kw.items():
+            setattr(a, k, val)
+        return a
+
+    def pick(o, *keys):
+        return {k: o[k] for k in keys if k in o}
+
+    recs = {}
+    o = run_solve(sub(steps=20, precision="fp64"), dict(WORKLOADS["cg_poisson2d"]), rank, world,
+                  local)
+    if o is not None:
+        recs["cg_poisson2d_128"] = dict(
+            pick(o, "value", "unit", "ms_per_step", "cpu_baseline"),
+            workload=o["config"]["workload"], iters=o["config"]["iters"],
+            status=o["config"]["status"], true_rel_residual=o["config"]["true_rel_residual"],
+            roofline_frac=o["roofline"]["frac"], gpu_launches=o["gpu_launches"])
+    o = run_solve(sub(steps=5, precision="mixed"), dict(WORKLOADS["bicgstab_convdiff"]), rank,
+                  world, local)
+    if o is not None:
+        pl = o.get("plain_fp64", {})
+        recs["bicgstab_convdiff160"] = {
+            "workload": o["config"]["workload"],
+            "plain_fp64": dict(pl, ms_per_step=round(1e3 / pl["value"], 3) if pl else None),
+            "mixed": dict(pick(o, "value", "unit", "ms_per_step"), iters=o["config"]["iters"],
+                          outer_steps=o["config"]["outer_steps"],
+                          inner_tol=o["config"]["inner_tol"], status=o["config"]["status"],
+                          true_rel_residual=o["config"]["true_rel_residual"],
+                          roofline_frac=o["roofline"]["frac"]),
+            "mixed_over_plain": pl.get("speedup_of_mixed"),
+            "cpu_baseline": o.get("cpu_baseline")}
+    for prec in ("fp64", "mixed"):
+        o = run_batch(sub(steps=3, precision=prec, quick=(prec == "mixed"),
+                          no_cpu=args.no_cpu or prec == "mixed"),
+                      dict(WORKLOADS["batch_cg"]), rank, world, local)
+        if o is None:
+            continue
+        c = o["config"]
+        r = dict(pick(o, "value", "unit", "ms_per_step", "cpu_baseline"),
+                 iters_total=c["iters_total"], all_converged=c["all_converged"],
+                 worst_true_rel_residual_sampled=c["worst_true_rel_residual_sampled"],
+                 roofline_frac=o["roofline"]["frac"])
+        if prec == "fp64":
+            lo = o.get("loop_of_single_solves", {})
+            r["loop_of_single_solves"] = pick(lo, "value", "unit", "iters_match")
+            recs["batch2048"] = {"workload": c["workload"], "fp64": r,
+                                 "batch_over_loop": lo.get("speedup_of_batch")}
+        elif "batch2048" in recs:
+            recs["batch2048"]["mixed"] = r
+            loop = recs["batch2048"]["fp64"]["loop_of_single_solves"].get("value")
+            if loop:
+                recs["batch2048"]["mixed_batch_over_loop"] = round(o["value"] / loop, 2)
+    return recs
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1402,6 +1483,9 @@ def main():
     ap.add_argument("--eager", action="store_true",
                     help="solver workloads: launch iterations one by one instead of a graph "
                          "(kernel-level profiling)")
+    ap.add_argument("--no-solves", action="store_true",
+                    help="default SpMV workload: skip the solves/s records (CG 128^2, "
+                         "BiCGSTAB 160^3 plain vs mixed, 2,048-system batch vs loop)")
     ap.add_argument("--quick", action="store_true",
                     help="timed steps only: no clock soak, no e2e, no CPU leg (profiling)")
     args = ap.parse_args()
@@ -1427,6 +1511,11 @@ def main():
     try:
         if wl["kind"] == "spmv":
             out = run_spmv(args, wl, rank, world, local)
+            if (args.workload == "spmv_poisson3d_f64" and not args.size and not args.quick
+                    and not args.no_solves):
+                recs = solve_records(args, rank, world, local)
+                if out is not None:
+                    out["solves"] = recs
         elif wl["kind"] == "batch":
             out = run_batch(args, wl, rank, world, local)
         elif wl["kind"] == "serve":

@@ -93,6 +93,16 @@ int mlsh_memcpy_h2d(mlsh_handle handle, void *d_dst, const void *h_src,
                     size_t bytes);
 int mlsh_memcpy_d2h(mlsh_handle handle, void *h_dst, const void *d_src,
                     size_t bytes);
+/* The same copies without the host wait, ordered on the handle's stream:
+ * they return once the copy is queued.  The host buffer must stay valid and
+ * unchanged (h2d) or unread (d2h) until the stream reaches the copy; from
+ * page-locked host memory the copy runs asynchronously and can overlap
+ * kernels and copies on other streams.  A pipelined form of send()/recv()
+ * (gpu_comm.cpp:8-73) for callers that stream inputs in and results out. */
+int mlsh_memcpy_h2d_async(mlsh_handle handle, void *d_dst, const void *h_src,
+                          size_t bytes);
+int mlsh_memcpy_d2h_async(mlsh_handle handle, void *h_dst, const void *d_src,
+                          size_t bytes);
 /* Device-to-device copy, asynchronous on the handle's stream. */
 int mlsh_memcpy_d2d(mlsh_handle handle, void *d_dst, const void *d_src,
                     size_t bytes);

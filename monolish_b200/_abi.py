@@ -81,6 +81,8 @@ SIGNATURES = {
     "mlsh_memcpy_h2d": (i32, [vp, vp, vp, C.c_size_t]),
     "mlsh_memcpy_d2h": (i32, [vp, vp, vp, C.c_size_t]),
     "mlsh_memcpy_d2d": (i32, [vp, vp, vp, C.c_size_t]),
+    "mlsh_memcpy_h2d_async": (i32, [vp, vp, vp, C.c_size_t]),
+    "mlsh_memcpy_d2h_async": (i32, [vp, vp, vp, C.c_size_t]),
     "mlsh_csr_plan_create": (i32, [vp, i32, i32, i32, vp, vp, vp, i32, vp, i32, C.POINTER(vp)]),
     "mlsh_csr_plan_destroy": (i32, [vp]),
     "mlsh_csr_plan_values_changed": (i32, [vp]),

@@ -434,6 +434,20 @@ int mlsh_memcpy_d2h(mlsh_handle hs, void *h, const void *d, size_t bytes) {
   return MLSH_SUCCESS;
 }
 
+int mlsh_memcpy_h2d_async(mlsh_handle hs, void *d, const void *h, size_t bytes) {
+  if (!hs || ((!d || !h) && bytes)) return MLSH_ERR_INVALID_ARG;
+  if (!bytes) return MLSH_SUCCESS;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, hs->h.stream));
+  return MLSH_SUCCESS;
+}
+
+int mlsh_memcpy_d2h_async(mlsh_handle hs, void *h, const void *d, size_t bytes) {
+  if (!hs || ((!d || !h) && bytes)) return MLSH_ERR_INVALID_ARG;
+  if (!bytes) return MLSH_SUCCESS;
+  MLSH_CUDA_TRY(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, hs->h.stream));
+  return MLSH_SUCCESS;
+}
+
 int mlsh_memcpy_d2d(mlsh_handle hs, void *dst, const void *src, size_t bytes) {
   if (!hs || ((!dst || !src) && bytes)) return MLSH_ERR_INVALID_ARG;
   if (!bytes) return MLSH_SUCCESS;
