@@ -523,10 +523,16 @@ def run_solve(args, wl, rank, world, local):
         if args.precision == "mixed":
             # inner iterations in FP32 (V = X = 4 bytes), one FP64 residual
             # (SpMV + x update) per outer step
-            B_A32 = nnz * 8 + (n + 1) * 4
+            # the FP32 copy's matrix bytes per SpMV in the layout it uses
+            import ctypes
+            lay, mb = ctypes.c_int(), ctypes.c_int64()
+            h.lib.mlsh_csr_plan_storage(A.plan, 1, ctypes.byref(lay), ctypes.byref(mb))
+            B_A32 = int(mb.value) if mb.value > 0 else nnz * 8 + (n + 1) * 4
             B_A64 = nnz * 12 + (n + 1) * 4
-            B_it32 = (B_A32 + 13 * n * 4) if wl["kind"] == "cg" else (2 * B_A32 + 22 * n * 4)
+            # BiCGSTAB with D^-1 folded into the FP32 values: 19 vector passes
+            B_it32 = (B_A32 + 13 * n * 4) if wl["kind"] == "cg" else (2 * B_A32 + 19 * n * 4)
             total_bytes = B_it32 * r.iters + (r.outer + 1) * (B_A64 + 5 * n * 8)
+            fp32_layout = {0: "CRS", 1: "offset slots"}.get(lay.value, "none")
         achieved = total_bytes / per_solve_s / 1e9
         peak, peak_kind = measured_peak()
         out = {
@@ -550,9 +556,13 @@ def run_solve(args, wl, rank, world, local):
         if args.precision == "mixed":
             out["dtype"] = "f32 inner / f64 refinement"
             out["config"]["precision"] = "mixed: FP32 inner (tol 1e-4 rel), FP64 outer"
+            out["config"]["fp32_layout"] = fp32_layout
+            out["config"]["fp32_matrix_bytes_per_spmv"] = B_A32
             out["config"]["outer_steps"] = r.outer
-            out["roofline"]["note"] = ("algorithmic bytes: FP32 inner iterations (V = X = 4) "
-                                       "plus an FP64 residual per outer step, / solve time")
+            out["roofline"]["note"] = ("algorithmic bytes: FP32 inner iterations (the FP32 "
+                                       "copy's matrix bytes in its layout + 19 vector passes "
+                                       "of 4 bytes) plus an FP64 residual per outer step, / "
+                                       "solve time")
             out["config"]["inner_tol"] = inner_tol
             if plain_ms is not None:
                 out["plain_fp64"] = {"value": round(1e3 / plain_ms, 3), "unit": "solves/s",
@@ -1429,6 +1439,7 @@ def solve_records(args, rank, world, local):
                           outer_steps=o["config"]["outer_steps"],
                           inner_tol=o["config"]["inner_tol"], status=o["config"]["status"],
                           true_rel_residual=o["config"]["true_rel_residual"],
+                          fp32_layout=o["config"].get("fp32_layout"),
                           roofline_frac=o["roofline"]["frac"]),
             "mixed_over_plain": pl.get("speedup_of_mixed"),
             "cpu_baseline": o.get("cpu_baseline")}

@@ -144,6 +144,29 @@ int mlsh_csr_plan_set_variant(mlsh_csr_plan plan, int variant);
 int mlsh_csr_plan_get_variant(mlsh_csr_plan plan, int *variant,
                               int *n_variants);
 
+/* Storage layout of an FP32 plan's SpMV (no counterpart in the reference,
+ * whose matvec reads the CRS arrays, crs_matvec.hpp:101-108).
+ * MLSH_LAYOUT_CRS: the caller's CRS arrays.  MLSH_LAYOUT_SLOTS: a derived
+ * copy in which each slice of 256 rows stores at most 8 column offsets
+ * (col - row) once and its values slot by slot, with a one-byte presence
+ * mask per row -- stencil matrices on structured grids need no column
+ * indices at all.  It applies only when every row is sorted, has no repeated
+ * column and at most 8 entries; each row is then summed exactly as the CRS
+ * kernel sums it, so y is the same in both layouts.  *applied (optional)
+ * reports whether the requested layout is in use.  The mixed-precision
+ * solvers pick the slot layout for their FP32 copy by themselves.  The copy
+ * is dropped by mlsh_csr_plan_values_changed.  Synchronous. */
+#define MLSH_LAYOUT_CRS 0
+#define MLSH_LAYOUT_SLOTS 1
+int mlsh_csr_plan_set_layout(mlsh_csr_plan plan, int layout, int *applied);
+/* The matrix bytes one SpMV reads in the layout in use (values, indices, row
+ * pointers or masks): of the plan itself (which = 0), or of the FP32 copy
+ * the mixed-precision solvers keep with an FP64 plan (which = 1; *layout =
+ * -1 and 0 bytes until a mixed solve has built it).  For roofline
+ * accounting. */
+int mlsh_csr_plan_storage(mlsh_csr_plan plan, int which, int *layout,
+                          int64_t *matrix_bytes);
+
 /* y = alpha*A*x + beta*y.  Replaces blas::matvec(A,x,y) and the
  * matvec(a,A,x,b,y) overload (src/blas/matrix/matvec/matvec_blas.cpp:3849-3877,
  * core src/blas/matrix/matvec/crs_matvec.hpp:8-114).  beta == 0 does not

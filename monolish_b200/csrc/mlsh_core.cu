@@ -188,6 +188,9 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
   const int g = p.spmv_grid[v];
   cudaError_t e = cudaSuccess;
   if constexpr (sizeof(VT) == 4) {
+    if (p.slots != nullptr)
+      return launch_spmv_slots<M0, M1>(p, h, alpha, x, beta, y_in, y_out, w0, w1, dot_out,
+                                       done, stream);
     if (p.col16 != nullptr) {
       switch (v) {
         case 1:
@@ -541,6 +544,7 @@ int mlsh_csr_plan_destroy(mlsh_csr_plan ps) {
   cudaStream_t s = p.handle ? p.handle->stream : nullptr;
   if (p.handle) cudaStreamSynchronize(s);
   release_plan_extras(p);
+  slots_release(p);
   for (void *d : {(void *)p.tiles, (void *)p.longs, (void *)p.chunk_part, (void *)p.long_cnt,
                   (void *)p.long_dot, p.inv_diag, (void *)p.col16, (void *)p.tile_base})
     pool_free(d, s);
@@ -553,6 +557,7 @@ int mlsh_csr_plan_values_changed(mlsh_csr_plan ps) {
   if (!ps) return MLSH_ERR_INVALID_ARG;
   ps->p.inv_diag_valid = false;
   invalidate_plan_extras(ps->p);
+  slots_release(ps->p);
   return MLSH_SUCCESS;
 }
 

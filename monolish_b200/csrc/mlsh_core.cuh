@@ -22,6 +22,17 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
                           const VT *w0, const VT *w1, double *dot_out,
                           const int *done, cudaStream_t stream);
 
+// Offset-slot layout of an FP32 plan (mlsh_slots.cu): built when the
+// structure qualifies (else p.slots stays null), released with the plan or
+// when its values change.  launch_spmv_t uses it whenever it is present.
+int slots_build(CsrPlan &p, cudaStream_t s);
+void slots_release(CsrPlan &p);
+template <int M0, int M1>
+cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, const float *x,
+                              double beta, const float *y_in, float *y_out, const float *w0,
+                              const float *w1, double *dot_out, const int *done,
+                              cudaStream_t stream);
+
 int plan_diag(const CsrPlan &p, void *out, bool invert, cudaStream_t stream);
 int plan_inv_diag(CsrPlan &p, cudaStream_t stream, const void **out);
 

@@ -125,6 +125,22 @@ struct Handle {
   void *host_cluster = nullptr;       // pinned record for the cluster engine
 };
 
+// Offset-slot layout of an FP32 copy (mlsh_slots.cu): rows in slices of
+// kSlotRows, each slice with at most kMaxSlots distinct column offsets
+// (col - row), values stored slot-major so every slot is one coalesced run.
+constexpr int kSlotRows = 256;
+constexpr int kMaxSlots = 8;
+struct SlotFormat {
+  float *vals = nullptr;     // n_slices * K * kSlotRows (0 where a row lacks the slot)
+  uint8_t *mask = nullptr;   // n_slices * kSlotRows: bit k = the row has slot k
+  int *offs = nullptr;       // n_slices * kMaxSlots, ascending, INT32_MIN = unused
+  int K = 0;                 // stored slots per slice
+  int unit = 0;              // 1: every diagonal value is exactly 1 and not stored
+  int n_slices = 0;
+  int grid = 0;              // CTAs of the SpMV launch
+  int64_t bytes() const { return (int64_t)n_slices * kSlotRows * (4 * (int64_t)K + 1); }
+};
+
 struct CsrPlan {
   Handle *handle = nullptr;
   int n_rows = 0, n_cols = 0, nnz = 0;
@@ -152,6 +168,8 @@ struct CsrPlan {
   // 16-bit column format (FP32 plans made for the mixed solver)
   uint16_t *col16 = nullptr;      // device, nnz: col - tile_base[tile]
   int *tile_base = nullptr;       // device, n_tiles
+  // offset-slot layout (FP32 plans made for the mixed solver), or null
+  SlotFormat *slots = nullptr;
 };
 
 // ------------------------------------------------------------ launches ---

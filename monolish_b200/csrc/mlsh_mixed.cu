@@ -6,8 +6,9 @@
 //     stop when ||r|| < tol       (the true residual, not a recurrence)
 //     s = ||r||;  r32 = r / s     rounded to FP32
 //     A32 d = r32                 CG / BiCGSTAB in FP32 on an FP32 copy of the
-//                                 values (and 16-bit column offsets when the
-//                                 structure allows), to inner tolerance
+//                                 values (in the offset-slot layout, or with
+//                                 16-bit column offsets, when the structure
+//                                 allows: mlsh_slots.cu), to inner tolerance
 //                                 (relative; ||r32|| = 1); dots and norms are
 //                                 still accumulated in FP64
 //     x += s * d                  FP64 update
@@ -197,9 +198,11 @@ int ensure_extras(mlsh_handle hs, CsrPlan &p, MixedExtras **out, const double *d
   const int want = dinv != nullptr ? 1 : 0;
   if (m->valid) {
     if (m->scaled != want) {
-      const int st = fill_val32(h, p, m, dinv);
+      int st = fill_val32(h, p, m, dinv);
       if (st != MLSH_SUCCESS) return st;
       mlsh_csr_plan_values_changed(m->plan32);
+      st = slots_build(m->plan32->p, h.stream);
+      if (st != MLSH_SUCCESS) return st;
       m->scaled = want;
     }
     *out = m;
@@ -226,8 +229,13 @@ int ensure_extras(mlsh_handle hs, CsrPlan &p, MixedExtras **out, const double *d
   if (st != MLSH_SUCCESS) return st;
   CsrPlan &q = m->plan32->p;
   q.variant = p.variant;
-  st = build_col16(q, h.stream);
+  // the offset-slot layout where the structure allows, else 16-bit columns
+  st = slots_build(q, h.stream);
   if (st != MLSH_SUCCESS) return st;
+  if (q.slots == nullptr) {
+    st = build_col16(q, h.stream);
+    if (st != MLSH_SUCCESS) return st;
+  }
   m->valid = true;
   *out = m;
   return MLSH_SUCCESS;
@@ -379,6 +387,34 @@ int mlsh_cg_solve_mixed(mlsh_handle hs, mlsh_csr_plan ps, const void *d_b, void 
                         const mlsh_solver_opts *opts, double inner_tol,
                         mlsh_solver_result *result) {
   return mixed_solve(0, hs, ps, d_b, d_x, opts, inner_tol, result);
+}
+
+static void storage_of(const CsrPlan &p, int *layout, int64_t *bytes) {
+  if (p.slots) {
+    *layout = MLSH_LAYOUT_SLOTS;
+    *bytes = p.slots->bytes() + (int64_t)p.slots->n_slices * kMaxSlots * 4;
+    return;
+  }
+  *layout = MLSH_LAYOUT_CRS;
+  const int64_t V = dtype_size(p.dtype);
+  const int64_t C = p.col16 ? 2 : 4;
+  *bytes = (int64_t)p.nnz * (V + C) + ((int64_t)p.n_rows + 1) * 4 +
+           (p.col16 ? (int64_t)p.n_tiles * 4 : 0);
+}
+
+int mlsh_csr_plan_storage(mlsh_csr_plan ps, int which, int *layout, int64_t *matrix_bytes) {
+  if (!ps || (which != 0 && which != 1)) return MLSH_ERR_INVALID_ARG;
+  int lay = -1;
+  int64_t b = 0;
+  if (which == 0) {
+    storage_of(ps->p, &lay, &b);
+  } else {
+    const MixedExtras *m = static_cast<const MixedExtras *>(ps->p.extras);
+    if (m && m->valid && m->plan32) storage_of(m->plan32->p, &lay, &b);
+  }
+  if (layout) *layout = lay;
+  if (matrix_bytes) *matrix_bytes = b;
+  return MLSH_SUCCESS;
 }
 
 int mlsh_bicgstab_solve_mixed(mlsh_handle hs, mlsh_csr_plan ps, const void *d_b, void *d_x,

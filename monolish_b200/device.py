@@ -160,6 +160,13 @@ class Crs:
     def set_variant(self, v):
         _abi.check(self.lib.mlsh_csr_plan_set_variant(self.plan, int(v)), "set_variant")
 
+    def set_layout(self, layout) -> bool:
+        """0: CRS, 1: offset-slot layout (FP32 plans); True if it is in use."""
+        applied = C.c_int()
+        _abi.check(self.lib.mlsh_csr_plan_set_layout(self.plan, int(layout), C.byref(applied)),
+                   "set_layout")
+        return bool(applied.value)
+
     def variant(self):
         v, nv = C.c_int(), C.c_int()
         _abi.check(self.lib.mlsh_csr_plan_get_variant(self.plan, C.byref(v), C.byref(nv)),
