@@ -156,10 +156,32 @@ struct SlotArgs {
   const int *done;
 };
 
-// One thread per row; a persistent grid walks the slices.  The fused dots
-// accumulate in a fixed per-thread order and are reduced like the vector
-// kernels' sums (fixed order, last CTA finalises).
-template <int M0, int M1>
+// One thread per row; a persistent grid walks the slices.  The next
+// slice's mask, offsets and values are loaded while the current slice's x
+// gathers are in flight, so HBM always has a slice's stream outstanding
+// (without that the kernel waits on each slice's loads, then on its
+// gathers).  KS = the plan's slot count.  The fused dots accumulate in a
+// fixed per-thread order and are reduced like the vector kernels' sums
+// (fixed order, last CTA finalises).
+template <int KS>
+struct SlotRow {
+  unsigned m;
+  int off[KS > 0 ? KS : 1];
+  float v[KS > 0 ? KS : 1];
+};
+
+template <int KS>
+__device__ __forceinline__ void slot_load(const SlotArgs &a, int sl, SlotRow<KS> &s) {
+  const bool in = sl < a.n_slices;
+  s.m = in ? (unsigned)__ldcs(a.mask + (size_t)sl * kSlotRows + threadIdx.x) : 0u;
+#pragma unroll
+  for (int k = 0; k < KS; ++k) {
+    s.off[k] = in ? __ldg(a.offs + sl * kMaxSlots + k) : 0;
+    s.v[k] = in ? __ldcs(a.vals + ((size_t)sl * KS + k) * kSlotRows + threadIdx.x) : 0.0f;
+  }
+}
+
+template <int KS, int M0, int M1>
 __global__ void __launch_bounds__(kSlotRows, 4) spmv_slots_kernel(const SlotArgs a) {
   constexpr int NR = (M0 != kDotNone ? 1 : 0) + (M1 != kDotNone ? 1 : 0);
   constexpr int NA = NR > 0 ? NR : 1;
@@ -171,31 +193,28 @@ __global__ void __launch_bounds__(kSlotRows, 4) spmv_slots_kernel(const SlotArgs
   double acc[NA];
 #pragma unroll
   for (int q = 0; q < NA; ++q) acc[q] = 0.0;
-  const int K = a.K;
+  SlotRow<KS> nxt;
+  slot_load<KS>(a, blockIdx.x, nxt);
   for (int sl = blockIdx.x; sl < a.n_slices; sl += gridDim.x) {
+    const SlotRow<KS> cur = nxt;
     const int r = sl * kSlotRows + (int)threadIdx.x;
     const bool live = r < a.n_rows;
-    int off[kMaxSlots];
-    float v[kMaxSlots], xx[kMaxSlots];
-    const unsigned m = live ? (unsigned)__ldcs(a.mask + (size_t)sl * kSlotRows + threadIdx.x) : 0u;
+    float xx[KS > 0 ? KS : 1];
 #pragma unroll
-    for (int k = 0; k < kMaxSlots; ++k) {
-      off[k] = k < K ? __ldg(a.offs + sl * kMaxSlots + k) : INT_MAX;
-      v[k] = k < K ? __ldcs(a.vals + ((size_t)sl * K + k) * kSlotRows + threadIdx.x) : 0.0f;
-    }
-#pragma unroll
-    for (int k = 0; k < kMaxSlots; ++k) xx[k] = ((m >> k) & 1u) ? __ldg(a.x + r + off[k]) : 0.0f;
+    for (int k = 0; k < KS; ++k)
+      xx[k] = ((cur.m >> k) & 1u) ? __ldg(a.x + r + cur.off[k]) : 0.0f;
     const float xd = (a.unit && live) ? __ldg(a.x + r) : 0.0f;
+    slot_load<KS>(a, sl + (int)gridDim.x, nxt);
     // ascending columns, products rounded separately: the CRS row loop
     float sum = 0.0f;
     bool placed = a.unit == 0;
 #pragma unroll
-    for (int k = 0; k < kMaxSlots; ++k) {
-      if (!placed && off[k] > 0) {
+    for (int k = 0; k < KS; ++k) {
+      if (!placed && cur.off[k] > 0) {
         sum = __fadd_rn(sum, xd);
         placed = true;
       }
-      if ((m >> k) & 1u) sum = __fadd_rn(sum, __fmul_rn(v[k], xx[k]));
+      if ((cur.m >> k) & 1u) sum = __fadd_rn(sum, __fmul_rn(cur.v[k], xx[k]));
     }
     if (!placed) sum = __fadd_rn(sum, xd);
     if (live) {
@@ -224,22 +243,22 @@ __global__ void __launch_bounds__(kSlotRows, 4) spmv_slots_kernel(const SlotArgs
   }
 }
 
-template <int M0, int M1>
-int slots_grid(int n_slices, int num_sms) {
+template <int KS, int M0, int M1>
+cudaError_t launch_slots_ks(const SlotArgs &a, int num_sms, cudaStream_t stream) {
   static int per_sm = 0;
+  constexpr auto k = spmv_slots_kernel<KS, M0, M1>;
   if (per_sm == 0) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, spmv_slots_kernel<M0, M1>, kSlotRows,
-                                                      0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kSlotRows, 0) != cudaSuccess ||
         b < 1) {
       cudaGetLastError();
       b = 1;
     }
     per_sm = b;
   }
-  int g = std::min(n_slices, per_sm * num_sms);
-  g = std::min(g, kMaxPartialBlocks);
-  return std::max(g, 1);
+  int g = std::min(a.n_slices, per_sm * num_sms);
+  g = std::max(std::min(g, kMaxPartialBlocks), 1);
+  return launch_dependent(k, g, kSlotRows, 0, stream, a);
 }
 
 }  // namespace
@@ -333,8 +352,17 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
   a.counter = h.counters;
   a.dot_out = dot_out;
   a.done = done;
-  return launch_dependent(spmv_slots_kernel<M0, M1>, slots_grid<M0, M1>(f.n_slices, h.num_sms),
-                          kSlotRows, 0, stream, a);
+  switch (f.K) {
+    case 0: return launch_slots_ks<0, M0, M1>(a, h.num_sms, stream);
+    case 1: return launch_slots_ks<1, M0, M1>(a, h.num_sms, stream);
+    case 2: return launch_slots_ks<2, M0, M1>(a, h.num_sms, stream);
+    case 3: return launch_slots_ks<3, M0, M1>(a, h.num_sms, stream);
+    case 4: return launch_slots_ks<4, M0, M1>(a, h.num_sms, stream);
+    case 5: return launch_slots_ks<5, M0, M1>(a, h.num_sms, stream);
+    case 6: return launch_slots_ks<6, M0, M1>(a, h.num_sms, stream);
+    case 7: return launch_slots_ks<7, M0, M1>(a, h.num_sms, stream);
+    default: return launch_slots_ks<8, M0, M1>(a, h.num_sms, stream);
+  }
 }
 
 #define MLSH_INST_SLOTS(A, B)                                                              \
