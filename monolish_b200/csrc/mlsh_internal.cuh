@@ -127,18 +127,23 @@ struct Handle {
 
 // Offset-slot layout of an FP32 copy (mlsh_slots.cu): rows in slices of
 // kSlotRows, each slice with at most kMaxSlots distinct column offsets
-// (col - row), values stored slot-major so every slot is one coalesced run.
+// (col - row).  A slice is one contiguous record of rec_bytes(K) bytes:
+//   int32 offs[kMaxSlots]   ascending offsets (INT32_MIN = unused)
+//   uint8 mask[kSlotRows]   bit k = the row has an entry at offs[k]
+//   float vals[K][kSlotRows] values slot-major (0 where absent)
+// so one bulk copy moves a slice into shared memory.
 constexpr int kSlotRows = 256;
 constexpr int kMaxSlots = 8;
+constexpr int kSlotHeadBytes = 4 * kMaxSlots + kSlotRows;  // 288, a multiple of 16
+__host__ __device__ constexpr int slot_rec_bytes(int K) {
+  return kSlotHeadBytes + 4 * kSlotRows * K;
+}
 struct SlotFormat {
-  float *vals = nullptr;     // n_slices * K * kSlotRows (0 where a row lacks the slot)
-  uint8_t *mask = nullptr;   // n_slices * kSlotRows: bit k = the row has slot k
-  int *offs = nullptr;       // n_slices * kMaxSlots, ascending, INT32_MIN = unused
-  int K = 0;                 // stored slots per slice
-  int unit = 0;              // 1: every diagonal value is exactly 1 and not stored
+  unsigned char *recs = nullptr;  // n_slices records
+  int K = 0;                      // stored slots per slice
+  int unit = 0;                   // 1: every diagonal value is exactly 1 and not stored
   int n_slices = 0;
-  int grid = 0;              // CTAs of the SpMV launch
-  int64_t bytes() const { return (int64_t)n_slices * kSlotRows * (4 * (int64_t)K + 1); }
+  int64_t bytes() const { return (int64_t)n_slices * slot_rec_bytes(K); }
 };
 
 struct CsrPlan {

@@ -392,7 +392,7 @@ int mlsh_cg_solve_mixed(mlsh_handle hs, mlsh_csr_plan ps, const void *d_b, void 
 static void storage_of(const CsrPlan &p, int *layout, int64_t *bytes) {
   if (p.slots) {
     *layout = MLSH_LAYOUT_SLOTS;
-    *bytes = p.slots->bytes() + (int64_t)p.slots->n_slices * kMaxSlots * 4;
+    *bytes = p.slots->bytes();
     return;
   }
   *layout = MLSH_LAYOUT_CRS;

@@ -5,16 +5,21 @@
 // FP32, Jacobi folded in); its layout is this library's choice.  Matrices
 // whose rows, in slices of kSlotRows consecutive rows, use at most
 // kMaxSlots distinct column offsets (col - row) -- stencil matrices on
-// structured grids, boundary rows included -- are stored as:
-//   offs[slice][k]      the slice's offsets, ascending (k < K)
-//   vals[slice][k][r]   value of row r's entry at offset offs[k] (0 if absent)
-//   mask[slice][r]      bit k set when row r has an entry at offs[k]
-// so the column indices cost nothing per entry, every slot of a slice is one
-// coalesced 1 KB run of values, and a row costs 4 K + 1 bytes (a 7-point
+// structured grids, boundary rows included -- are stored as one contiguous
+// record per slice (mlsh_internal.cuh: the slice's ascending offsets, a
+// presence mask byte per row, then the values slot by slot), so column
+// indices cost nothing per entry and a row costs 4 K + 1 bytes (a 7-point
 // row: 25 with the unit diagonal implicit, against 46 in CRS with 16-bit
 // columns).  When every diagonal value of the copy is exactly 1 (Jacobi
 // folded in: a_ii * (1 / a_ii) rounds to 1 in FP32) the diagonal is not
 // stored and x_i is added in its place.
+//
+// The SpMV streams the records like the CRS kernel streams its tiles: a
+// producer warp moves each slice's record into a ring of shared-memory
+// stages with one 1-D bulk copy (L2 evict-first) completing on an mbarrier,
+// and 8 consumer warps, one thread per row, read the row from shared
+// memory, release the stage, gather x and write y.  With 4 stages and 4
+// CTAs per SM about 100 KB per SM is in flight.
 //
 // A matrix qualifies only if every row is sorted, has no repeated column
 // and at most kShortRow entries: then each row is summed by one thread in
@@ -98,10 +103,11 @@ __global__ void __launch_bounds__(kSlotRows)
 }
 
 __global__ void __launch_bounds__(kSlotRows)
-    slots_fill(int n, const int *rp, const int *ci, const float *val, int *offs, int K,
-               int unit, float *vals, uint8_t *mask) {
+    slots_fill(int n, const int *rp, const int *ci, const float *val, const int *offs, int K,
+               int unit, unsigned char *recs) {
   __shared__ int tab[kMaxSlots];
   const int slice = blockIdx.x;
+  unsigned char *rec = recs + (size_t)slice * slot_rec_bytes(K);
   if (threadIdx.x == 0) {
     int k = 0;
     for (int s = 0; s < kMaxSlots; ++s) {
@@ -112,7 +118,7 @@ __global__ void __launch_bounds__(kSlotRows)
     for (int s = k; s < kMaxSlots; ++s) tab[s] = kSlotUnused;
   }
   __syncthreads();
-  if (threadIdx.x < kMaxSlots) offs[slice * kMaxSlots + threadIdx.x] = tab[threadIdx.x];
+  if (threadIdx.x < kMaxSlots) reinterpret_cast<int *>(rec)[threadIdx.x] = tab[threadIdx.x];
   const int r = slice * kSlotRows + (int)threadIdx.x;
   float v[kMaxSlots];
 #pragma unroll
@@ -130,17 +136,15 @@ __global__ void __launch_bounds__(kSlotRows)
         }
     }
   }
+  rec[4 * kMaxSlots + threadIdx.x] = (unsigned char)m;
+  float *vals = reinterpret_cast<float *>(rec + kSlotHeadBytes);
 #pragma unroll
   for (int s = 0; s < kMaxSlots; ++s)
-    if (s < K) vals[((size_t)slice * K + s) * kSlotRows + threadIdx.x] = v[s];
-  mask[(size_t)slice * kSlotRows + threadIdx.x] = (uint8_t)m;
+    if (s < K) vals[s * kSlotRows + threadIdx.x] = v[s];
 }
 
 struct SlotArgs {
-  const float *vals;
-  const uint8_t *mask;
-  const int *offs;
-  int K;
+  const unsigned char *recs;
   int unit;
   int n_rows;
   int n_slices;
@@ -154,67 +158,164 @@ struct SlotArgs {
   unsigned *counter;
   double *dot_out;
   const int *done;
+  int *err;  // set to MLSH_ERR_TIMEOUT if a wait gives up
 };
 
-// One thread per row; a persistent grid walks the slices.  The next
-// slice's mask, offsets and values are loaded while the current slice's x
-// gathers are in flight, so HBM always has a slice's stream outstanding
-// (without that the kernel waits on each slice's loads, then on its
-// gathers).  KS = the plan's slot count.  The fused dots accumulate in a
-// fixed per-thread order and are reduced like the vector kernels' sums
-// (fixed order, last CTA finalises).
+constexpr int kSlotStages = 4;
+constexpr int kSlotConsumers = kSlotRows;            // one thread per row
+constexpr int kSlotThreads = kSlotConsumers + 32;   // + the producer warp
+
 template <int KS>
-struct SlotRow {
-  unsigned m;
-  int off[KS > 0 ? KS : 1];
-  float v[KS > 0 ? KS : 1];
+struct SlotSmem {
+  static constexpr int kRec = slot_rec_bytes(KS);
+  static constexpr int kBarOff = kSlotStages * kRec;  // kRec is a multiple of 16
+  static constexpr int kRedOff = kBarOff + 2 * kSlotStages * 8;
+  static constexpr int kFlagOff = kRedOff + 32 * 8;
+  static constexpr int kBytes = kFlagOff + 16 * 4;
 };
+constexpr int kSlotFlagAbort = 0;
+constexpr int kSlotFlagLast = 1;
+constexpr int kSlotFlagWarpDone = 2;  // 8 slots: stages each consumer warp has read
 
-template <int KS>
-__device__ __forceinline__ void slot_load(const SlotArgs &a, int sl, SlotRow<KS> &s) {
-  const bool in = sl < a.n_slices;
-  s.m = in ? (unsigned)__ldcs(a.mask + (size_t)sl * kSlotRows + threadIdx.x) : 0u;
-#pragma unroll
-  for (int k = 0; k < KS; ++k) {
-    s.off[k] = in ? __ldg(a.offs + sl * kMaxSlots + k) : 0;
-    s.v[k] = in ? __ldcs(a.vals + ((size_t)sl * KS + k) * kSlotRows + threadIdx.x) : 0.0f;
-  }
-}
-
+// A persistent grid walks the slices; KS = the plan's slot count.  The
+// fused dots accumulate in a fixed per-thread order and are reduced like
+// the vector kernels' sums (fixed order, last CTA finalises).  Every wait
+// is bounded: a consumer warp that gives up records MLSH_ERR_TIMEOUT and
+// stops; the producer then waits for its copies still in flight and exits.
 template <int KS, int M0, int M1>
-__global__ void __launch_bounds__(kSlotRows, 4) spmv_slots_kernel(const SlotArgs a) {
+__global__ void __launch_bounds__(kSlotThreads, 4) spmv_slots_kernel(const SlotArgs a) {
   constexpr int NR = (M0 != kDotNone ? 1 : 0) + (M1 != kDotNone ? 1 : 0);
   constexpr int NA = NR > 0 ? NR : 1;
-  __shared__ double red[kSlotRows / 32 * NA];
-  __shared__ int last_flag;
+  using L = SlotSmem<KS>;
+  extern __shared__ __align__(128) unsigned char smem[];
   pdl_wait();
   pdl_launch_dependents();
   if (a.done != nullptr && *a.done != 0) return;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::kBarOff);
+  double *red = reinterpret_cast<double *>(smem + L::kRedOff);
+  volatile int *flags = reinterpret_cast<volatile int *>(smem + L::kFlagOff);
+  const int tid = threadIdx.x;
+  const uint32_t full0 = smem_addr(bars);
+  const uint32_t empty0 = smem_addr(bars + kSlotStages);
+  if (tid == 0) {
+    for (int s = 0; s < kSlotStages; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, kSlotConsumers / 32);  // one arrival per consumer warp
+    }
+    for (int f = 0; f < 16; ++f) flags[f] = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (tid < 32) {
+    // ------------------------------------------------------- producer ---
+    if (tid != 0) return;
+    const uint64_t policy = l2_evict_first_policy();
+    int k = 0;
+    bool aborted = false;
+    for (int sl = blockIdx.x; sl < a.n_slices; sl += gridDim.x, ++k) {
+      const int s = k % kSlotStages;
+      if (k >= kSlotStages) {
+        const uint32_t par = (uint32_t)((k / kSlotStages - 1) & 1);
+        const uint64_t t0 = global_timer_ns();
+        bool ok = false;
+        for (uint32_t it = 1;; ++it) {
+          if (mbar_try_wait(empty0 + 8 * s, par)) { ok = true; break; }
+          if ((it & 63u) == 0 && flags[kSlotFlagAbort]) break;
+          if ((it & 1023u) == 0 && global_timer_ns() - t0 > kWaitLimitNs) {
+            atomicExch(a.err, MLSH_ERR_TIMEOUT);
+            break;
+          }
+        }
+        if (!ok) { aborted = true; break; }
+      }
+      const uint32_t bar = full0 + 8 * s;
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(bar, (uint32_t)L::kRec);
+      bulk_g2s_hint(smem_addr(smem + s * L::kRec), a.recs + (size_t)sl * L::kRec,
+                    (uint32_t)L::kRec, bar, policy);
+    }
+    const int issued = k;
+    // Tail: the consumers release every issued stage; if they gave up, wait
+    // for the copies themselves so that none is in flight at exit.
+    for (int kk = issued - kSlotStages < 0 ? 0 : issued - kSlotStages; kk < issued && !aborted;
+         ++kk) {
+      const int s = kk % kSlotStages;
+      const uint32_t par = (uint32_t)((kk / kSlotStages) & 1);
+      const uint64_t t0 = global_timer_ns();
+      for (uint32_t it = 1;; ++it) {
+        if (mbar_try_wait(empty0 + 8 * s, par)) break;
+        if (((it & 63u) == 0 && flags[kSlotFlagAbort]) ||
+            ((it & 1023u) == 0 && global_timer_ns() - t0 > kWaitLimitNs)) {
+          aborted = true;
+          break;
+        }
+      }
+    }
+    if (aborted) {
+      atomicExch(a.err, MLSH_ERR_TIMEOUT);
+      int consumed = issued;
+      for (int w = 0; w < kSlotConsumers / 32; ++w)
+        consumed = min(consumed, (int)flags[kSlotFlagWarpDone + w]);
+      for (int kk = consumed; kk < issued; ++kk)
+        mbar_wait_bounded(full0 + 8 * (kk % kSlotStages), (uint32_t)((kk / kSlotStages) & 1),
+                          kWaitLimitNs);
+    }
+    return;
+  }
+
+  // ---------------------------------------------------------- consumers ---
+  const int ct = tid - 32;
+  const int lane = ct & 31, warp = ct >> 5;
   double acc[NA];
 #pragma unroll
   for (int q = 0; q < NA; ++q) acc[q] = 0.0;
-  SlotRow<KS> nxt;
-  slot_load<KS>(a, blockIdx.x, nxt);
-  for (int sl = blockIdx.x; sl < a.n_slices; sl += gridDim.x) {
-    const SlotRow<KS> cur = nxt;
-    const int r = sl * kSlotRows + (int)threadIdx.x;
+  int k = 0;
+  for (int sl = blockIdx.x; sl < a.n_slices; sl += gridDim.x, ++k) {
+    const int s = k % kSlotStages;
+    int ok = 1;
+    if (lane == 0) {
+      ok = flags[kSlotFlagAbort] == 0 &&
+           mbar_wait_bounded(full0 + 8 * s, (uint32_t)((k / kSlotStages) & 1), kWaitLimitNs);
+      if (!ok && flags[kSlotFlagAbort] == 0) {
+        flags[kSlotFlagAbort] = 1;
+        atomicExch(a.err, MLSH_ERR_TIMEOUT);
+      }
+    }
+    if (__shfl_sync(0xffffffffu, ok, 0) == 0) break;
+    const unsigned char *rec = smem + s * L::kRec;
+    const int *offs = reinterpret_cast<const int *>(rec);
+    const float *vals = reinterpret_cast<const float *>(rec + kSlotHeadBytes);
+    const unsigned m = rec[4 * kMaxSlots + ct];
+    int off[KS > 0 ? KS : 1];
+    float v[KS > 0 ? KS : 1];
+#pragma unroll
+    for (int q = 0; q < KS; ++q) {
+      off[q] = offs[q];
+      v[q] = vals[q * kSlotRows + ct];
+    }
+    // the warp is done with the stage
+    __syncwarp();
+    if (lane == 0) {
+      mbar_arrive(empty0 + 8 * s);
+      flags[kSlotFlagWarpDone + warp] = k + 1;
+    }
+    const int r = sl * kSlotRows + ct;
     const bool live = r < a.n_rows;
     float xx[KS > 0 ? KS : 1];
 #pragma unroll
-    for (int k = 0; k < KS; ++k)
-      xx[k] = ((cur.m >> k) & 1u) ? __ldg(a.x + r + cur.off[k]) : 0.0f;
+    for (int q = 0; q < KS; ++q) xx[q] = ((m >> q) & 1u) ? __ldg(a.x + r + off[q]) : 0.0f;
     const float xd = (a.unit && live) ? __ldg(a.x + r) : 0.0f;
-    slot_load<KS>(a, sl + (int)gridDim.x, nxt);
     // ascending columns, products rounded separately: the CRS row loop
     float sum = 0.0f;
     bool placed = a.unit == 0;
 #pragma unroll
-    for (int k = 0; k < KS; ++k) {
-      if (!placed && cur.off[k] > 0) {
+    for (int q = 0; q < KS; ++q) {
+      if (!placed && off[q] > 0) {
         sum = __fadd_rn(sum, xd);
         placed = true;
       }
-      if ((cur.m >> k) & 1u) sum = __fadd_rn(sum, __fmul_rn(cur.v[k], xx[k]));
+      if ((m >> q) & 1u) sum = __fadd_rn(sum, __fmul_rn(v[q], xx[q]));
     }
     if (!placed) sum = __fadd_rn(sum, xd);
     if (live) {
@@ -229,13 +330,13 @@ __global__ void __launch_bounds__(kSlotRows, 4) spmv_slots_kernel(const SlotArgs
     }
   }
   if constexpr (NR > 0) {
-    group_sum<NA>(acc, red, threadIdx.x, kSlotRows, 0);
-    if (publish_partials<NA>(acc, a.partials, a.counter, &last_flag, threadIdx.x, kSlotRows,
-                             0)) {
+    group_sum<NA>(acc, red, ct, kSlotConsumers, 1);
+    int *sflag = const_cast<int *>(flags + kSlotFlagLast);
+    if (publish_partials<NA>(acc, a.partials, a.counter, sflag, ct, kSlotConsumers, 1)) {
       double tot[NA];
-      reduce_partials<NA>(tot, a.partials, (int)gridDim.x, nullptr, 0, NA, a.counter, red,
-                          threadIdx.x, kSlotRows, 0);
-      if (threadIdx.x == 0) {
+      reduce_partials<NA>(tot, a.partials, (int)gridDim.x, nullptr, 0, NA, a.counter, red, ct,
+                          kSlotConsumers, 1);
+      if (ct == 0) {
 #pragma unroll
         for (int q = 0; q < NR; ++q) a.dot_out[q] = tot[q];
       }
@@ -247,9 +348,12 @@ template <int KS, int M0, int M1>
 cudaError_t launch_slots_ks(const SlotArgs &a, int num_sms, cudaStream_t stream) {
   static int per_sm = 0;
   constexpr auto k = spmv_slots_kernel<KS, M0, M1>;
+  constexpr int smem = SlotSmem<KS>::kBytes;
+  static_assert(smem <= 48 * 1024, "slot stages fit the default shared-memory limit");
   if (per_sm == 0) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kSlotRows, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kSlotThreads, smem) !=
+            cudaSuccess ||
         b < 1) {
       cudaGetLastError();
       b = 1;
@@ -258,7 +362,7 @@ cudaError_t launch_slots_ks(const SlotArgs &a, int num_sms, cudaStream_t stream)
   }
   int g = std::min(a.n_slices, per_sm * num_sms);
   g = std::max(std::min(g, kMaxPartialBlocks), 1);
-  return launch_dependent(k, g, kSlotRows, 0, stream, a);
+  return launch_dependent(k, g, kSlotThreads, smem, stream, a);
 }
 
 }  // namespace
@@ -266,9 +370,7 @@ cudaError_t launch_slots_ks(const SlotArgs &a, int num_sms, cudaStream_t stream)
 void slots_release(CsrPlan &p) {
   if (!p.slots) return;
   cudaStream_t s = p.handle ? p.handle->stream : nullptr;
-  pool_free(p.slots->vals, s);
-  pool_free(p.slots->mask, s);
-  pool_free(p.slots->offs, s);
+  pool_free(p.slots->recs, s);
   delete p.slots;
   p.slots = nullptr;
 }
@@ -290,7 +392,7 @@ int slots_build(CsrPlan &p, cudaStream_t s) {
   slots_scan<<<n_slices, kSlotRows, 0, s>>>(n, p.row_ptr, p.col_ind, val, offs, flags);
   int hf[4] = {0, 0, 0, 0};
   cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, s);
-  const cudaError_t e = cudaStreamSynchronize(s);
+  cudaError_t e = cudaStreamSynchronize(s);
   pool_free(flags, s);
   if (e != cudaSuccess) {
     pool_free(offs, s);
@@ -308,21 +410,25 @@ int slots_build(CsrPlan &p, cudaStream_t s) {
     pool_free(offs, s);
     return MLSH_ERR_OOM;
   }
-  f->offs = offs;
   f->K = K;
   f->unit = unit;
   f->n_slices = n_slices;
-  if (pool_alloc(&f->vals, sizeof(float) * (size_t)n_slices * std::max(K, 1) * kSlotRows, s) !=
-          cudaSuccess ||
-      pool_alloc(&f->mask, (size_t)n_slices * kSlotRows, s) != cudaSuccess) {
+  if (pool_alloc(&f->recs, (size_t)f->bytes(), s) != cudaSuccess) {
     cudaGetLastError();
-    p.slots = f;
-    slots_release(p);
-    return MLSH_SUCCESS;
+    pool_free(offs, s);
+    delete f;
+    return MLSH_SUCCESS;  // no room: the CRS kernel stays
   }
   slots_fill<<<n_slices, kSlotRows, 0, s>>>(n, p.row_ptr, p.col_ind, val, offs, K, unit,
-                                            f->vals, f->mask);
-  MLSH_CUDA_TRY(cudaGetLastError());
+                                            f->recs);
+  e = cudaGetLastError();
+  pool_free(offs, s);
+  if (e != cudaSuccess) {
+    pool_free(f->recs, s);
+    delete f;
+    set_last_error("slot layout fill", e);
+    return MLSH_ERR_CUDA;
+  }
   p.slots = f;
   return MLSH_SUCCESS;
 }
@@ -334,10 +440,7 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
                               cudaStream_t stream) {
   const SlotFormat &f = *p.slots;
   SlotArgs a;
-  a.vals = f.vals;
-  a.mask = f.mask;
-  a.offs = f.offs;
-  a.K = f.K;
+  a.recs = f.recs;
   a.unit = f.unit;
   a.n_rows = p.n_rows;
   a.n_slices = f.n_slices;
@@ -352,6 +455,7 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
   a.counter = h.counters;
   a.dot_out = dot_out;
   a.done = done;
+  a.err = h.err_flag;
   switch (f.K) {
     case 0: return launch_slots_ks<0, M0, M1>(a, h.num_sms, stream);
     case 1: return launch_slots_ks<1, M0, M1>(a, h.num_sms, stream);
