@@ -125,22 +125,23 @@ struct Handle {
   void *host_cluster = nullptr;       // pinned record for the cluster engine
 };
 
-// Offset-slot layout of an FP32 copy (mlsh_slots.cu): rows in slices of
-// kSlotRows, each slice with at most kMaxSlots distinct column offsets
-// (col - row).  A slice is one contiguous record of rec_bytes(K) bytes:
-//   int32 offs[kMaxSlots]   ascending offsets (INT32_MIN = unused)
-//   uint8 mask[kSlotRows]   bit k = the row has an entry at offs[k]
-//   float vals[K][kSlotRows] values slot-major (0 where absent)
+// Offset-slot layout of an FP32 copy (mlsh_slots.cu): the matrix uses at
+// most kMaxSlots distinct column offsets (col - row), held once in `offs`;
+// rows are cut into slices of kSlotRows, and a slice is one contiguous
+// record of slot_rec_bytes(K) bytes:
+//   uint8 mask[kSlotRows]     bit k = the row has an entry at offs[k]
+//   float vals[K][kSlotRows]  values slot-major (0 where absent)
 // so one bulk copy moves a slice into shared memory.
 constexpr int kSlotRows = 256;
 constexpr int kMaxSlots = 8;
-constexpr int kSlotHeadBytes = 4 * kMaxSlots + kSlotRows;  // 288, a multiple of 16
+constexpr int kSlotHeadBytes = kSlotRows;  // the mask; a multiple of 16
 __host__ __device__ constexpr int slot_rec_bytes(int K) {
   return kSlotHeadBytes + 4 * kSlotRows * K;
 }
 struct SlotFormat {
   unsigned char *recs = nullptr;  // n_slices records
-  int K = 0;                      // stored slots per slice
+  int offs[kMaxSlots] = {0, 0, 0, 0, 0, 0, 0, 0};  // ascending; the first K are used
+  int K = 0;                      // stored slots
   int unit = 0;                   // 1: every diagonal value is exactly 1 and not stored
   int n_slices = 0;
   int64_t bytes() const { return (int64_t)n_slices * slot_rec_bytes(K); }

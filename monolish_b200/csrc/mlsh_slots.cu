@@ -3,12 +3,12 @@
 //
 // The FP32 copy is data derived from the caller's CRS (values rounded to
 // FP32, Jacobi folded in); its layout is this library's choice.  Matrices
-// whose rows, in slices of kSlotRows consecutive rows, use at most
-// kMaxSlots distinct column offsets (col - row) -- stencil matrices on
-// structured grids, boundary rows included -- are stored as one contiguous
-// record per slice (mlsh_internal.cuh: the slice's ascending offsets, a
-// presence mask byte per row, then the values slot by slot), so column
-// indices cost nothing per entry and a row costs 4 K + 1 bytes (a 7-point
+// that use at most kMaxSlots distinct column offsets (col - row) in all --
+// stencil matrices on structured grids, boundary rows included -- keep the
+// offsets once and store each slice of kSlotRows rows as one contiguous
+// record (mlsh_internal.cuh: a presence mask byte per row, then the values
+// slot by slot), so column indices cost nothing per entry and a row costs
+// 4 K + 1 bytes (a 7-point
 // row: 25 with the unit diagonal implicit, against 46 in CRS with 16-bit
 // columns).  When every diagonal value of the copy is exactly 1 (Jacobi
 // folded in: a_ii * (1 / a_ii) rounds to 1 in FP32) the diagonal is not
@@ -16,7 +16,8 @@
 //
 // The SpMV needs no gathers: for each slot k the x values a slice reads are
 // one contiguous run, x[r0 + offs[k] .. r0 + offs[k] + 255] (r0 = the
-// slice's first row).  So the producer warp moves, per slice, the record
+// slice's first row), and the offsets are launch parameters.  So the
+// producer warp moves, per slice, the record
 // and those runs (plus x[r0..] for an implicit diagonal and the fused dots'
 // weight vectors) into a ring of shared-memory stages, one 1-D bulk copy
 // per lane, all completing on the stage's mbarrier; 8 consumer warps, one
@@ -33,6 +34,7 @@
 #include <algorithm>
 #include <climits>
 #include <new>
+#include <vector>
 
 #include "mlsh_core.cuh"
 
@@ -105,23 +107,15 @@ __global__ void __launch_bounds__(kSlotRows)
   }
 }
 
+struct SlotTable {
+  int offs[kMaxSlots];
+};
+
 __global__ void __launch_bounds__(kSlotRows)
-    slots_fill(int n, const int *rp, const int *ci, const float *val, const int *offs, int K,
+    slots_fill(int n, const int *rp, const int *ci, const float *val, SlotTable tab, int K,
                int unit, unsigned char *recs) {
-  __shared__ int tab[kMaxSlots];
   const int slice = blockIdx.x;
   unsigned char *rec = recs + (size_t)slice * slot_rec_bytes(K);
-  if (threadIdx.x == 0) {
-    int k = 0;
-    for (int s = 0; s < kMaxSlots; ++s) {
-      const int o = offs[slice * kMaxSlots + s];
-      if (o == kSlotUnused || (unit && o == 0)) continue;
-      tab[k++] = o;
-    }
-    for (int s = k; s < kMaxSlots; ++s) tab[s] = kSlotUnused;
-  }
-  __syncthreads();
-  if (threadIdx.x < kMaxSlots) reinterpret_cast<int *>(rec)[threadIdx.x] = tab[threadIdx.x];
   const int r = slice * kSlotRows + (int)threadIdx.x;
   float v[kMaxSlots];
 #pragma unroll
@@ -133,13 +127,13 @@ __global__ void __launch_bounds__(kSlotRows)
       if (unit && off == 0) continue;
 #pragma unroll
       for (int s = 0; s < kMaxSlots; ++s)
-        if (tab[s] == off) {
+        if (s < K && tab.offs[s] == off) {
           v[s] = val[j];
           m |= 1u << s;
         }
     }
   }
-  rec[4 * kMaxSlots + threadIdx.x] = (unsigned char)m;
+  rec[threadIdx.x] = (unsigned char)m;
   float *vals = reinterpret_cast<float *>(rec + kSlotHeadBytes);
 #pragma unroll
   for (int s = 0; s < kMaxSlots; ++s)
@@ -148,6 +142,7 @@ __global__ void __launch_bounds__(kSlotRows)
 
 struct SlotArgs {
   const unsigned char *recs;
+  SlotTable tab;  // the matrix's offsets (the first K used)
   int unit;
   int n_rows;
   int n_slices;
@@ -247,21 +242,17 @@ __global__ void __launch_bounds__(kSlotThreads, 3) spmv_slots_kernel(const SlotA
   if (tid < 32) {
     // ------------------------------------------------------- producer ---
     // lane 0 copies the record; lane 1 + j copies run j (slot runs, the
-    // diagonal's, the weights'), for the slice's offsets held in lanes 0..7
+    // diagonal's, the weights')
     const int lane = tid;
     const uint64_t policy = l2_evict_first_policy();
     const float *wv = (M0 == kDotW) ? a.w0 : a.w1;   // first weight run
     const float *wv2 = a.w1;                          // second (both dots weighted)
+    const int j = lane - 1;
+    const int offj = (j >= 0 && j < KS) ? a.tab.offs[j] : 0;
     int k = 0;
     bool aborted = false;
-    auto load_offs = [&](int sl) -> int {
-      if (sl >= a.n_slices || lane >= kMaxSlots) return kSlotUnused;
-      return __ldg(reinterpret_cast<const int *>(a.recs + (size_t)sl * L::kRec) + lane);
-    };
-    int offs_next = load_offs(blockIdx.x);
     for (int sl = blockIdx.x; sl < a.n_slices; sl += gridDim.x, ++k) {
       const int s = k % kSlotStages;
-      const int offs_cur = offs_next;
       if (k >= kSlotStages) {
         int ok = 1;
         if (lane == 0) {
@@ -281,8 +272,6 @@ __global__ void __launch_bounds__(kSlotThreads, 3) spmv_slots_kernel(const SlotA
       }
       // this lane's copy
       const long long r0 = (long long)sl * kSlotRows;
-      const int j = lane - 1;
-      const int offj = __shfl_sync(0xffffffffu, offs_cur, j < 0 ? 0 : (j < KS ? j : 0));
       uint32_t bytes = 0;
       uintptr_t src = 0;
       int s0;
@@ -290,7 +279,7 @@ __global__ void __launch_bounds__(kSlotThreads, 3) spmv_slots_kernel(const SlotA
         bytes = (uint32_t)L::kRec;
         src = (uintptr_t)(a.recs + (size_t)sl * L::kRec);
       } else if (j < KS) {
-        if (offj != kSlotUnused) bytes = run_range(a.x, r0 + offj, a.n_rows, &s0, &src);
+        bytes = run_range(a.x, r0 + offj, a.n_rows, &s0, &src);
       } else if (j == KS) {
         if (a.unit) bytes = run_range(a.x, r0, a.n_rows, &s0, &src);
       } else if (j == KS + 1 && NW >= 1) {
@@ -312,7 +301,6 @@ __global__ void __launch_bounds__(kSlotThreads, 3) spmv_slots_kernel(const SlotA
         bulk_g2s_hint(smem_addr(st), (const void *)src, bytes, bar, policy);
       else if (bytes)
         bulk_g2s(smem_addr(st + L::kRunOff + j * kRunBytes), (const void *)src, bytes, bar);
-      offs_next = load_offs(sl + (int)gridDim.x);
     }
     if (lane != 0) return;
     const int issued = k;
@@ -364,10 +352,9 @@ __global__ void __launch_bounds__(kSlotThreads, 3) spmv_slots_kernel(const SlotA
     }
     if (__shfl_sync(0xffffffffu, ok, 0) == 0) break;
     const unsigned char *st = smem + s * L::kStage;
-    const int *offs = reinterpret_cast<const int *>(st);
     const float *vals = reinterpret_cast<const float *>(st + kSlotHeadBytes);
     const float *runs = reinterpret_cast<const float *>(st + L::kRunOff);
-    const unsigned m = st[4 * kMaxSlots + ct];
+    const unsigned m = st[ct];
     const int r0 = sl * kSlotRows;
     const int r = r0 + ct;
     const bool live = r < a.n_rows;
@@ -375,7 +362,7 @@ __global__ void __launch_bounds__(kSlotThreads, 3) spmv_slots_kernel(const SlotA
     float v[KS > 0 ? KS : 1], xx[KS > 0 ? KS : 1];
 #pragma unroll
     for (int q = 0; q < KS; ++q) {
-      off[q] = offs[q];
+      off[q] = a.tab.offs[q];
       v[q] = vals[q * kSlotRows + ct];
       xx[q] = 0.0f;
       if ((m >> q) & 1u) {
@@ -531,31 +518,43 @@ int slots_build(CsrPlan &p, cudaStream_t s) {
     return MLSH_SUCCESS;
   }
   const int unit = hf[3] == 0 ? 1 : 0;
-  const int K = unit ? hf[1] : hf[0];
+  // the offsets of all slices together (a slice's are a subset of these)
+  std::vector<int> all((size_t)n_slices * kMaxSlots);
+  e = cudaMemcpyAsync(all.data(), offs, sizeof(int) * all.size(), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  pool_free(offs, s);
+  if (e != cudaSuccess) {
+    set_last_error("slot layout offsets", e);
+    return MLSH_ERR_CUDA;
+  }
+  std::vector<int> uni;
+  for (int o : all)
+    if (o != kSlotUnused && !(unit && o == 0)) uni.push_back(o);
+  std::sort(uni.begin(), uni.end());
+  uni.erase(std::unique(uni.begin(), uni.end()), uni.end());
+  if ((int)uni.size() > kMaxSlots) return MLSH_SUCCESS;  // not this layout
+  const int K = (int)uni.size();
+  SlotTable tab;
+  for (int q = 0; q < kMaxSlots; ++q) tab.offs[q] = q < K ? uni[q] : 0;
   e = slots_prepare(K);
   if (e != cudaSuccess) {
-    pool_free(offs, s);
     set_last_error("slot SpMV set-up", e);
     return MLSH_ERR_CUDA;
   }
   SlotFormat *f = new (std::nothrow) SlotFormat();
-  if (!f) {
-    pool_free(offs, s);
-    return MLSH_ERR_OOM;
-  }
+  if (!f) return MLSH_ERR_OOM;
+  for (int q = 0; q < kMaxSlots; ++q) f->offs[q] = tab.offs[q];
   f->K = K;
   f->unit = unit;
   f->n_slices = n_slices;
   if (pool_alloc(&f->recs, (size_t)f->bytes(), s) != cudaSuccess) {
     cudaGetLastError();
-    pool_free(offs, s);
     delete f;
     return MLSH_SUCCESS;  // no room: the CRS kernel stays
   }
-  slots_fill<<<n_slices, kSlotRows, 0, s>>>(n, p.row_ptr, p.col_ind, val, offs, K, unit,
+  slots_fill<<<n_slices, kSlotRows, 0, s>>>(n, p.row_ptr, p.col_ind, val, tab, K, unit,
                                             f->recs);
   e = cudaGetLastError();
-  pool_free(offs, s);
   if (e != cudaSuccess) {
     pool_free(f->recs, s);
     delete f;
@@ -574,6 +573,7 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
   const SlotFormat &f = *p.slots;
   SlotArgs a;
   a.recs = f.recs;
+  for (int q = 0; q < kMaxSlots; ++q) a.tab.offs[q] = f.offs[q];
   a.unit = f.unit;
   a.n_rows = p.n_rows;
   a.n_slices = f.n_slices;
