@@ -14,16 +14,14 @@
 // folded in: a_ii * (1 / a_ii) rounds to 1 in FP32) the diagonal is not
 // stored and x_i is added in its place.
 //
-// The SpMV needs no gathers: for each slot k the x values a slice reads are
-// one contiguous run, x[r0 + offs[k] .. r0 + offs[k] + 255] (r0 = the
-// slice's first row), and the offsets are launch parameters.  So the
-// producer warp moves, per slice, the record
-// and those runs (plus x[r0..] for an implicit diagonal and the fused dots'
-// weight vectors) into a ring of shared-memory stages, one 1-D bulk copy
-// per lane, all completing on the stage's mbarrier; 8 consumer warps, one
-// thread per row, read everything from shared memory, release the stage
-// and write y.  The record stream is marked L2 evict-first so x stays in
-// L2 across the runs that reread it.
+// The SpMV streams the records like the CRS kernel streams its tiles: a
+// producer warp moves each slice's record into a ring of shared-memory
+// stages with one 1-D bulk copy (L2 evict-first, so the gathered x stays in
+// L2) completing on an mbarrier, and 8 consumer warps, one thread per row,
+// read the row from shared memory, release the stage, gather x (the
+// offsets are launch parameters) and write y.  (Staging each slot's x run
+// with a bulk copy of its own, nine 1 KB copies per slice, measured slower:
+// the copies' issue rate, not HBM, then bounds the kernel.)
 //
 // A matrix qualifies only if every row is sorted, has no repeated column
 // and at most kShortRow entries: then each row is summed by one thread in
@@ -163,46 +161,14 @@ constexpr int kSlotStages = 4;
 constexpr int kSlotConsumers = kSlotRows;            // one thread per row
 constexpr int kSlotThreads = kSlotConsumers + 32;   // + the producer warp
 
-// Shared-memory stage: the record, then KS + 1 x runs (slot k's run, then
-// the diagonal's), then NW weight runs (w0, w1 of the fused dots).  A run is
-// 256 values plus the rounding of its ends to 16-byte boundaries.
-constexpr int kRunBytes = 4 * kSlotRows + 16;
-
-template <int KS, int NW>
+template <int KS>
 struct SlotSmem {
   static constexpr int kRec = slot_rec_bytes(KS);
-  static constexpr int kRunOff = kRec;  // kRec is a multiple of 16
-  static constexpr int kNRuns = KS + 1 + NW;
-  static constexpr int kStage = kRec + kNRuns * kRunBytes;
-  static constexpr int kBarOff = kSlotStages * kStage;
+  static constexpr int kBarOff = kSlotStages * kRec;  // kRec is a multiple of 16
   static constexpr int kRedOff = kBarOff + 2 * kSlotStages * 8;
   static constexpr int kFlagOff = kRedOff + 32 * 8;
   static constexpr int kBytes = kFlagOff + 16 * 4;
 };
-
-// Run [a, a + 256) of v clipped to [0, n): the first element s0, the bytes
-// of the 16-byte-rounded copy (0 if empty) and its source address.  The
-// rounded range never leaves the 16-byte chunks holding elements s0 and
-// e0 - 1, so it stays inside the memory that holds v.
-__device__ __forceinline__ uint32_t run_range(const float *v, long long a, int n, int *s0,
-                                              uintptr_t *src) {
-  const long long lo = a < 0 ? 0 : a;
-  const long long hi = a + kSlotRows > n ? n : a + kSlotRows;
-  *s0 = (int)lo;
-  if (hi <= lo) {
-    *src = 0;
-    return 0;
-  }
-  const uintptr_t b = (uintptr_t)(v + lo) & ~(uintptr_t)15;
-  const uintptr_t e = ((uintptr_t)(v + hi) + 15) & ~(uintptr_t)15;
-  *src = b;
-  return (uint32_t)(e - b);
-}
-// Element offset of v[s0] in its staged run.
-__device__ __forceinline__ int run_head(const float *v, int s0) {
-  return (int)(((uintptr_t)(v + s0) & 15u) >> 2);
-}
-
 constexpr int kSlotFlagAbort = 0;
 constexpr int kSlotFlagLast = 1;
 constexpr int kSlotFlagWarpDone = 2;  // 8 slots: stages each consumer warp has read
@@ -213,12 +179,10 @@ constexpr int kSlotFlagWarpDone = 2;  // 8 slots: stages each consumer warp has 
 // is bounded: a consumer warp that gives up records MLSH_ERR_TIMEOUT and
 // stops; the producer then waits for its copies still in flight and exits.
 template <int KS, int M0, int M1>
-__global__ void __launch_bounds__(kSlotThreads, 3) spmv_slots_kernel(const SlotArgs a) {
+__global__ void __launch_bounds__(kSlotThreads, 4) spmv_slots_kernel(const SlotArgs a) {
   constexpr int NR = (M0 != kDotNone ? 1 : 0) + (M1 != kDotNone ? 1 : 0);
   constexpr int NA = NR > 0 ? NR : 1;
-  constexpr int NW = (M0 == kDotW ? 1 : 0) + (M1 == kDotW ? 1 : 0);
-  using L = SlotSmem<KS, NW>;
-  static_assert(L::kNRuns + 1 <= 32, "one producer lane per copy");
+  using L = SlotSmem<KS>;
   extern __shared__ __align__(128) unsigned char smem[];
   pdl_wait();
   pdl_launch_dependents();
@@ -241,68 +205,32 @@ __global__ void __launch_bounds__(kSlotThreads, 3) spmv_slots_kernel(const SlotA
 
   if (tid < 32) {
     // ------------------------------------------------------- producer ---
-    // lane 0 copies the record; lane 1 + j copies run j (slot runs, the
-    // diagonal's, the weights')
-    const int lane = tid;
+    if (tid != 0) return;
     const uint64_t policy = l2_evict_first_policy();
-    const float *wv = (M0 == kDotW) ? a.w0 : a.w1;   // first weight run
-    const float *wv2 = a.w1;                          // second (both dots weighted)
-    const int j = lane - 1;
-    const int offj = (j >= 0 && j < KS) ? a.tab.offs[j] : 0;
     int k = 0;
     bool aborted = false;
     for (int sl = blockIdx.x; sl < a.n_slices; sl += gridDim.x, ++k) {
       const int s = k % kSlotStages;
       if (k >= kSlotStages) {
-        int ok = 1;
-        if (lane == 0) {
-          const uint32_t par = (uint32_t)((k / kSlotStages - 1) & 1);
-          const uint64_t t0 = global_timer_ns();
-          ok = 0;
-          for (uint32_t it = 1;; ++it) {
-            if (mbar_try_wait(empty0 + 8 * s, par)) { ok = 1; break; }
-            if ((it & 63u) == 0 && flags[kSlotFlagAbort]) break;
-            if ((it & 1023u) == 0 && global_timer_ns() - t0 > kWaitLimitNs) {
-              atomicExch(a.err, MLSH_ERR_TIMEOUT);
-              break;
-            }
+        const uint32_t par = (uint32_t)((k / kSlotStages - 1) & 1);
+        const uint64_t t0 = global_timer_ns();
+        bool ok = false;
+        for (uint32_t it = 1;; ++it) {
+          if (mbar_try_wait(empty0 + 8 * s, par)) { ok = true; break; }
+          if ((it & 63u) == 0 && flags[kSlotFlagAbort]) break;
+          if ((it & 1023u) == 0 && global_timer_ns() - t0 > kWaitLimitNs) {
+            atomicExch(a.err, MLSH_ERR_TIMEOUT);
+            break;
           }
         }
-        if (__shfl_sync(0xffffffffu, ok, 0) == 0) { aborted = true; break; }
+        if (!ok) { aborted = true; break; }
       }
-      // this lane's copy
-      const long long r0 = (long long)sl * kSlotRows;
-      uint32_t bytes = 0;
-      uintptr_t src = 0;
-      int s0;
-      if (lane == 0) {
-        bytes = (uint32_t)L::kRec;
-        src = (uintptr_t)(a.recs + (size_t)sl * L::kRec);
-      } else if (j < KS) {
-        bytes = run_range(a.x, r0 + offj, a.n_rows, &s0, &src);
-      } else if (j == KS) {
-        if (a.unit) bytes = run_range(a.x, r0, a.n_rows, &s0, &src);
-      } else if (j == KS + 1 && NW >= 1) {
-        bytes = run_range(wv, r0, a.n_rows, &s0, &src);
-      } else if (j == KS + 2 && NW >= 2) {
-        bytes = run_range(wv2, r0, a.n_rows, &s0, &src);
-      }
-      uint32_t total = bytes;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
       const uint32_t bar = full0 + 8 * s;
-      unsigned char *st = smem + s * L::kStage;
-      if (lane == 0) {
-        fence_proxy_async_smem();
-        mbar_arrive_expect_tx(bar, total);
-      }
-      __syncwarp();
-      if (lane == 0)  // the record: read once, evict first
-        bulk_g2s_hint(smem_addr(st), (const void *)src, bytes, bar, policy);
-      else if (bytes)
-        bulk_g2s(smem_addr(st + L::kRunOff + j * kRunBytes), (const void *)src, bytes, bar);
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(bar, (uint32_t)L::kRec);
+      bulk_g2s_hint(smem_addr(smem + s * L::kRec), a.recs + (size_t)sl * L::kRec,
+                    (uint32_t)L::kRec, bar, policy);
     }
-    if (lane != 0) return;
     const int issued = k;
     // Tail: the consumers release every issued stage; if they gave up, wait
     // for the copies themselves so that none is in flight at exit.
@@ -351,42 +279,28 @@ __global__ void __launch_bounds__(kSlotThreads, 3) spmv_slots_kernel(const SlotA
       }
     }
     if (__shfl_sync(0xffffffffu, ok, 0) == 0) break;
-    const unsigned char *st = smem + s * L::kStage;
+    const unsigned char *st = smem + s * L::kRec;
     const float *vals = reinterpret_cast<const float *>(st + kSlotHeadBytes);
-    const float *runs = reinterpret_cast<const float *>(st + L::kRunOff);
     const unsigned m = st[ct];
-    const int r0 = sl * kSlotRows;
-    const int r = r0 + ct;
-    const bool live = r < a.n_rows;
-    int off[KS > 0 ? KS : 1];
-    float v[KS > 0 ? KS : 1], xx[KS > 0 ? KS : 1];
+    float v[KS > 0 ? KS : 1];
 #pragma unroll
-    for (int q = 0; q < KS; ++q) {
-      off[q] = a.tab.offs[q];
-      v[q] = vals[q * kSlotRows + ct];
-      xx[q] = 0.0f;
-      if ((m >> q) & 1u) {
-        const long long aq = (long long)r0 + off[q];
-        const int s0 = aq < 0 ? 0 : (int)aq;
-        xx[q] = runs[q * (kRunBytes / 4) + (r + off[q] - s0) + run_head(a.x, s0)];
-      }
-    }
-    const float xd = (a.unit && live) ? runs[KS * (kRunBytes / 4) + ct + run_head(a.x, r0)]
-                                      : 0.0f;
-    float wa = 0.0f, wb = 0.0f;
-    if constexpr (NW >= 1) {
-      const float *wv = (M0 == kDotW) ? a.w0 : a.w1;
-      if (live) wa = runs[(KS + 1) * (kRunBytes / 4) + ct + run_head(wv, r0)];
-    }
-    if constexpr (NW >= 2) {
-      if (live) wb = runs[(KS + 2) * (kRunBytes / 4) + ct + run_head(a.w1, r0)];
-    }
+    for (int q = 0; q < KS; ++q) v[q] = vals[q * kSlotRows + ct];
     // the warp is done with the stage
     __syncwarp();
     if (lane == 0) {
       mbar_arrive(empty0 + 8 * s);
       flags[kSlotFlagWarpDone + warp] = k + 1;
     }
+    const int r = sl * kSlotRows + ct;
+    const bool live = r < a.n_rows;
+    int off[KS > 0 ? KS : 1];
+    float xx[KS > 0 ? KS : 1];
+#pragma unroll
+    for (int q = 0; q < KS; ++q) {
+      off[q] = a.tab.offs[q];
+      xx[q] = ((m >> q) & 1u) ? __ldg(a.x + r + off[q]) : 0.0f;
+    }
+    const float xd = (a.unit && live) ? __ldg(a.x + r) : 0.0f;
     // ascending columns, products rounded separately: the CRS row loop
     float sum = 0.0f;
     bool placed = a.unit == 0;
@@ -404,9 +318,9 @@ __global__ void __launch_bounds__(kSlotThreads, 3) spmv_slots_kernel(const SlotA
       const float out = (a.beta == 0.0) ? (float)(a.alpha * ds)
                                         : (float)(a.alpha * ds + a.beta * (double)a.y_in[r]);
       a.y_out[r] = out;
-      if constexpr (M0 == kDotW) acc[0] += (double)wa * (double)out;
+      if constexpr (M0 == kDotW) acc[0] += (double)a.w0[r] * (double)out;
       if constexpr (M0 == kDotSelf) acc[0] += (double)out * (double)out;
-      if constexpr (M1 == kDotW) acc[1] += (double)(M0 == kDotW ? wb : wa) * (double)out;
+      if constexpr (M1 == kDotW) acc[1] += (double)a.w1[r] * (double)out;
       if constexpr (M1 == kDotSelf) acc[1] += (double)out * (double)out;
     }
   }
@@ -430,9 +344,8 @@ __global__ void __launch_bounds__(kSlotThreads, 3) spmv_slots_kernel(const SlotA
 // the CTAs per SM.
 template <int KS, int M0, int M1>
 struct SlotLaunch {
-  static constexpr int kNW = (M0 == kDotW ? 1 : 0) + (M1 == kDotW ? 1 : 0);
-  static constexpr int kSmem = SlotSmem<KS, kNW>::kBytes;
-  static_assert(kSmem <= 100 * 1024, "two CTAs of slot stages fit an SM");
+  static constexpr int kSmem = SlotSmem<KS>::kBytes;
+  static_assert(kSmem <= 48 * 1024, "slot stages fit the default shared-memory limit");
   static int per_sm;
   static cudaError_t prepare() {
     if (per_sm > 0) return cudaSuccess;
