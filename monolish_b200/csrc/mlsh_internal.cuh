@@ -138,12 +138,31 @@ constexpr int kSlotHeadBytes = kSlotRows;  // the mask; a multiple of 16
 __host__ __device__ constexpr int slot_rec_bytes(int K) {
   return kSlotHeadBytes + 4 * kSlotRows * K;
 }
+// The SpMV moves kSlotGroup consecutive slices per pipeline stage: their
+// records, and x as a few windows -- offsets closer than kSlotMergeGap share
+// one window x[R0 + lo .. R0 + hi + kSlotGroup * kSlotRows), R0 the stage's
+// first row.
+constexpr int kSlotGroup = 4;
+constexpr int kSlotMergeGap = 1024;
+constexpr int kMaxSlotWin = kMaxSlots + 1;  // the slots' windows + the diagonal's
+constexpr int kMaxSlotStages = 4;
 struct SlotFormat {
   unsigned char *recs = nullptr;  // n_slices records
   int offs[kMaxSlots] = {0, 0, 0, 0, 0, 0, 0, 0};  // ascending; the first K are used
   int K = 0;                      // stored slots
   int unit = 0;                   // 1: every diagonal value is exactly 1 and not stored
   int n_slices = 0;
+  // stage plan
+  int n_win = 0;
+  int win_lo[kMaxSlotWin] = {};   // window start, relative to the stage's first row
+  int win_len[kMaxSlotWin] = {};  // window length in elements
+  int win_off[kMaxSlotWin] = {};  // byte offset of the window in a stage
+  int slot_win[kMaxSlots] = {};   // the window holding slot k's x values
+  int diag_win = -1;              // the window holding x_i (unit diagonal)
+  int w_off = 0;                  // byte offset of the dot weights' runs in a stage
+  int stage_bytes = 0;
+  int stages = 0;
+  int grid_per_sm = 0;            // CTAs per SM of the launch
   int64_t bytes() const { return (int64_t)n_slices * slot_rec_bytes(K); }
 };
 

@@ -140,10 +140,20 @@ __global__ void __launch_bounds__(kSlotRows)
 
 struct SlotArgs {
   const unsigned char *recs;
-  SlotTable tab;  // the matrix's offsets (the first K used)
+  int offs[kMaxSlots];      // the matrix's offsets (the first KS used)
+  int slot_win[kMaxSlots];  // window of each slot
+  int win_lo[kMaxSlotWin];
+  int win_len[kMaxSlotWin];
+  int win_off[kMaxSlotWin];
+  int n_win;
+  int diag_win;
+  int w_off;
+  int stage_bytes;
+  int stages;
   int unit;
   int n_rows;
   int n_slices;
+  int n_groups;
   const float *x;
   float *y_out;
   const float *y_in;  // read only when beta != 0
@@ -157,44 +167,67 @@ struct SlotArgs {
   int *err;  // set to MLSH_ERR_TIMEOUT if a wait gives up
 };
 
-constexpr int kSlotStages = 4;
-constexpr int kSlotConsumers = kSlotRows;            // one thread per row
+constexpr int kSlotConsumers = kSlotRows;            // one thread per row of a slice
 constexpr int kSlotThreads = kSlotConsumers + 32;   // + the producer warp
-
-template <int KS>
-struct SlotSmem {
-  static constexpr int kRec = slot_rec_bytes(KS);
-  static constexpr int kBarOff = kSlotStages * kRec;  // kRec is a multiple of 16
-  static constexpr int kRedOff = kBarOff + 2 * kSlotStages * 8;
-  static constexpr int kFlagOff = kRedOff + 32 * 8;
-  static constexpr int kBytes = kFlagOff + 16 * 4;
-};
+constexpr int kGroupRows = kSlotGroup * kSlotRows;
+constexpr int kWRunBytes = 4 * kGroupRows + 16;     // a weight run, rounded ends
+// after the stages: mbarriers, reduction scratch, flags
+constexpr int kSlotTailBytes = 2 * kMaxSlotStages * 8 + 32 * 8 + 16 * 4;
 constexpr int kSlotFlagAbort = 0;
 constexpr int kSlotFlagLast = 1;
 constexpr int kSlotFlagWarpDone = 2;  // 8 slots: stages each consumer warp has read
 
-// A persistent grid walks the slices; KS = the plan's slot count.  The
-// fused dots accumulate in a fixed per-thread order and are reduced like
-// the vector kernels' sums (fixed order, last CTA finalises).  Every wait
-// is bounded: a consumer warp that gives up records MLSH_ERR_TIMEOUT and
-// stops; the producer then waits for its copies still in flight and exits.
+// Elements [a, a + len) of v clipped to [0, n): the first element s0, the
+// bytes of the 16-byte-rounded copy (0 if empty) and its source.  The
+// rounded range never leaves the 16-byte chunks holding elements s0 and
+// e0 - 1, so it stays inside the memory that holds v.
+__device__ __forceinline__ uint32_t clip_range(const float *v, long long a, int len, int n,
+                                               uintptr_t *src) {
+  const long long lo = a < 0 ? 0 : a;
+  const long long hi = a + len > n ? n : a + len;
+  if (hi <= lo) {
+    *src = 0;
+    return 0;
+  }
+  const uintptr_t b = (uintptr_t)(v + lo) & ~(uintptr_t)15;
+  const uintptr_t e = ((uintptr_t)(v + hi) + 15) & ~(uintptr_t)15;
+  *src = b;
+  return (uint32_t)(e - b);
+}
+// Element index (of v) of the first staged element of the copy of [a, ...).
+__device__ __forceinline__ long long staged_base(const float *v, long long a) {
+  const long long lo = a < 0 ? 0 : a;
+  return lo - (long long)(((uintptr_t)(v + lo) & 15u) >> 2);
+}
+
+// A persistent grid walks the stages (kSlotGroup slices each); KS = the
+// plan's slot count.  Consumer thread ct handles row ct of each slice of a
+// stage, reading mask, values, x and the dot weights from shared memory.
+// The fused dots accumulate in a fixed per-thread order and are reduced
+// like the vector kernels' sums (fixed order, last CTA finalises).  Every
+// wait is bounded: a consumer warp that gives up records MLSH_ERR_TIMEOUT
+// and stops; the producer then waits for its copies in flight and exits.
 template <int KS, int M0, int M1>
-__global__ void __launch_bounds__(kSlotThreads, 4) spmv_slots_kernel(const SlotArgs a) {
+__global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotArgs a) {
   constexpr int NR = (M0 != kDotNone ? 1 : 0) + (M1 != kDotNone ? 1 : 0);
   constexpr int NA = NR > 0 ? NR : 1;
-  using L = SlotSmem<KS>;
+  constexpr int NW = (M0 == kDotW ? 1 : 0) + (M1 == kDotW ? 1 : 0);
   extern __shared__ __align__(128) unsigned char smem[];
   pdl_wait();
   pdl_launch_dependents();
   if (a.done != nullptr && *a.done != 0) return;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::kBarOff);
-  double *red = reinterpret_cast<double *>(smem + L::kRedOff);
-  volatile int *flags = reinterpret_cast<volatile int *>(smem + L::kFlagOff);
+  const int STG = a.stages;
+  const int rec_bytes = slot_rec_bytes(KS);
+  unsigned char *tail = smem + STG * a.stage_bytes;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(tail);
+  double *red = reinterpret_cast<double *>(tail + 2 * kMaxSlotStages * 8);
+  volatile int *flags =
+      reinterpret_cast<volatile int *>(tail + 2 * kMaxSlotStages * 8 + 32 * 8);
   const int tid = threadIdx.x;
   const uint32_t full0 = smem_addr(bars);
-  const uint32_t empty0 = smem_addr(bars + kSlotStages);
+  const uint32_t empty0 = smem_addr(bars + kMaxSlotStages);
   if (tid == 0) {
-    for (int s = 0; s < kSlotStages; ++s) {
+    for (int s = 0; s < STG; ++s) {
       mbar_init(full0 + 8 * s, 1);
       mbar_init(empty0 + 8 * s, kSlotConsumers / 32);  // one arrival per consumer warp
     }
@@ -202,42 +235,78 @@ __global__ void __launch_bounds__(kSlotThreads, 4) spmv_slots_kernel(const SlotA
     fence_mbar_init();
   }
   __syncthreads();
+  const float *wv0 = (M0 == kDotW) ? a.w0 : a.w1;  // first weight run
+  const float *wv1 = a.w1;                          // second (both dots weighted)
 
   if (tid < 32) {
     // ------------------------------------------------------- producer ---
-    if (tid != 0) return;
+    // lane 0 copies the stage's records; lane 1 + w window w; then the
+    // weight runs
+    const int lane = tid;
     const uint64_t policy = l2_evict_first_policy();
     int k = 0;
     bool aborted = false;
-    for (int sl = blockIdx.x; sl < a.n_slices; sl += gridDim.x, ++k) {
-      const int s = k % kSlotStages;
-      if (k >= kSlotStages) {
-        const uint32_t par = (uint32_t)((k / kSlotStages - 1) & 1);
-        const uint64_t t0 = global_timer_ns();
-        bool ok = false;
-        for (uint32_t it = 1;; ++it) {
-          if (mbar_try_wait(empty0 + 8 * s, par)) { ok = true; break; }
-          if ((it & 63u) == 0 && flags[kSlotFlagAbort]) break;
-          if ((it & 1023u) == 0 && global_timer_ns() - t0 > kWaitLimitNs) {
-            atomicExch(a.err, MLSH_ERR_TIMEOUT);
-            break;
+    for (int g = blockIdx.x; g < a.n_groups; g += gridDim.x, ++k) {
+      const int s = k % STG;
+      if (k >= STG) {
+        int ok = 1;
+        if (lane == 0) {
+          const uint32_t par = (uint32_t)((k / STG - 1) & 1);
+          const uint64_t t0 = global_timer_ns();
+          ok = 0;
+          for (uint32_t it = 1;; ++it) {
+            if (mbar_try_wait(empty0 + 8 * s, par)) { ok = 1; break; }
+            if ((it & 63u) == 0 && flags[kSlotFlagAbort]) break;
+            if ((it & 1023u) == 0 && global_timer_ns() - t0 > kWaitLimitNs) {
+              atomicExch(a.err, MLSH_ERR_TIMEOUT);
+              break;
+            }
           }
         }
-        if (!ok) { aborted = true; break; }
+        if (__shfl_sync(0xffffffffu, ok, 0) == 0) { aborted = true; break; }
       }
+      const int sl0 = g * kSlotGroup;
+      const long long R0 = (long long)sl0 * kSlotRows;
+      unsigned char *st = smem + s * a.stage_bytes;
+      uint32_t bytes = 0, dst = 0;
+      uintptr_t src = 0;
+      const int j = lane - 1;
+      if (lane == 0) {
+        const int ns = min(kSlotGroup, a.n_slices - sl0);
+        bytes = (uint32_t)(ns * rec_bytes);
+        src = (uintptr_t)(a.recs + (size_t)sl0 * rec_bytes);
+        dst = smem_addr(st);
+      } else if (j < a.n_win) {
+        bytes = clip_range(a.x, R0 + a.win_lo[j], a.win_len[j], a.n_rows, &src);
+        dst = smem_addr(st + a.win_off[j]);
+      } else if (j == a.n_win && NW >= 1) {
+        bytes = clip_range(wv0, R0, kGroupRows, a.n_rows, &src);
+        dst = smem_addr(st + a.w_off);
+      } else if (j == a.n_win + 1 && NW >= 2) {
+        bytes = clip_range(wv1, R0, kGroupRows, a.n_rows, &src);
+        dst = smem_addr(st + a.w_off + kWRunBytes);
+      }
+      uint32_t total = bytes;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
       const uint32_t bar = full0 + 8 * s;
-      fence_proxy_async_smem();
-      mbar_arrive_expect_tx(bar, (uint32_t)L::kRec);
-      bulk_g2s_hint(smem_addr(smem + s * L::kRec), a.recs + (size_t)sl * L::kRec,
-                    (uint32_t)L::kRec, bar, policy);
+      if (lane == 0) {
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(bar, total);
+      }
+      __syncwarp();
+      if (lane == 0)  // the records: read once, evict first (x stays in L2)
+        bulk_g2s_hint(dst, (const void *)src, bytes, bar, policy);
+      else if (bytes)
+        bulk_g2s(dst, (const void *)src, bytes, bar);
     }
+    if (lane != 0) return;
     const int issued = k;
     // Tail: the consumers release every issued stage; if they gave up, wait
     // for the copies themselves so that none is in flight at exit.
-    for (int kk = issued - kSlotStages < 0 ? 0 : issued - kSlotStages; kk < issued && !aborted;
-         ++kk) {
-      const int s = kk % kSlotStages;
-      const uint32_t par = (uint32_t)((kk / kSlotStages) & 1);
+    for (int kk = issued - STG < 0 ? 0 : issued - STG; kk < issued && !aborted; ++kk) {
+      const int s = kk % STG;
+      const uint32_t par = (uint32_t)((kk / STG) & 1);
       const uint64_t t0 = global_timer_ns();
       for (uint32_t it = 1;; ++it) {
         if (mbar_try_wait(empty0 + 8 * s, par)) break;
@@ -254,8 +323,7 @@ __global__ void __launch_bounds__(kSlotThreads, 4) spmv_slots_kernel(const SlotA
       for (int w = 0; w < kSlotConsumers / 32; ++w)
         consumed = min(consumed, (int)flags[kSlotFlagWarpDone + w]);
       for (int kk = consumed; kk < issued; ++kk)
-        mbar_wait_bounded(full0 + 8 * (kk % kSlotStages), (uint32_t)((kk / kSlotStages) & 1),
-                          kWaitLimitNs);
+        mbar_wait_bounded(full0 + 8 * (kk % STG), (uint32_t)((kk / STG) & 1), kWaitLimitNs);
     }
     return;
   }
@@ -266,62 +334,88 @@ __global__ void __launch_bounds__(kSlotThreads, 4) spmv_slots_kernel(const SlotA
   double acc[NA];
 #pragma unroll
   for (int q = 0; q < NA; ++q) acc[q] = 0.0;
+  int off[KS > 0 ? KS : 1], woff[KS > 0 ? KS : 1];
+#pragma unroll
+  for (int q = 0; q < KS; ++q) {
+    off[q] = a.offs[q];
+    woff[q] = a.win_off[a.slot_win[q]];
+  }
+  const int dwoff = a.diag_win >= 0 ? a.win_off[a.diag_win] : 0;
   int k = 0;
-  for (int sl = blockIdx.x; sl < a.n_slices; sl += gridDim.x, ++k) {
-    const int s = k % kSlotStages;
+  for (int g = blockIdx.x; g < a.n_groups; g += gridDim.x, ++k) {
+    const int s = k % STG;
     int ok = 1;
     if (lane == 0) {
       ok = flags[kSlotFlagAbort] == 0 &&
-           mbar_wait_bounded(full0 + 8 * s, (uint32_t)((k / kSlotStages) & 1), kWaitLimitNs);
+           mbar_wait_bounded(full0 + 8 * s, (uint32_t)((k / STG) & 1), kWaitLimitNs);
       if (!ok && flags[kSlotFlagAbort] == 0) {
         flags[kSlotFlagAbort] = 1;
         atomicExch(a.err, MLSH_ERR_TIMEOUT);
       }
     }
     if (__shfl_sync(0xffffffffu, ok, 0) == 0) break;
-    const unsigned char *st = smem + s * L::kRec;
-    const float *vals = reinterpret_cast<const float *>(st + kSlotHeadBytes);
-    const unsigned m = st[ct];
-    float v[KS > 0 ? KS : 1];
+    const unsigned char *st = smem + s * a.stage_bytes;
+    const int sl0 = g * kSlotGroup;
+    const long long R0 = (long long)sl0 * kSlotRows;
+    // per slot: its window's first staged element, relative to R0 (small)
+    int ib[KS > 0 ? KS : 1];
 #pragma unroll
-    for (int q = 0; q < KS; ++q) v[q] = vals[q * kSlotRows + ct];
+    for (int q = 0; q < KS; ++q)
+      ib[q] = (int)(staged_base(a.x, R0 + a.win_lo[a.slot_win[q]]) - R0);
+    const int idb = a.diag_win >= 0 ? (int)(staged_base(a.x, R0 + a.win_lo[a.diag_win]) - R0) : 0;
+    const int iw0 = (int)(staged_base(wv0, R0) - R0), iw1 = (int)(staged_base(wv1, R0) - R0);
+    const int ns = min(kSlotGroup, a.n_slices - sl0);
+    for (int gs = 0; gs < ns; ++gs) {
+      const unsigned char *rec = st + gs * rec_bytes;
+      const float *vals = reinterpret_cast<const float *>(rec + kSlotHeadBytes);
+      const unsigned m = rec[ct];
+      const int lr = gs * kSlotRows + ct;  // row within the stage
+      const long long r = R0 + lr;
+      const bool live = r < a.n_rows;
+      float v[KS > 0 ? KS : 1], xx[KS > 0 ? KS : 1];
+#pragma unroll
+      for (int q = 0; q < KS; ++q) {
+        v[q] = vals[q * kSlotRows + ct];
+        xx[q] = ((m >> q) & 1u)
+                    ? *reinterpret_cast<const float *>(st + woff[q] + 4 * (lr + off[q] - ib[q]))
+                    : 0.0f;
+      }
+      const float xd = (a.unit && live)
+                           ? *reinterpret_cast<const float *>(st + dwoff + 4 * (lr - idb))
+                           : 0.0f;
+      // ascending columns, products rounded separately: the CRS row loop
+      float sum = 0.0f;
+      bool placed = a.unit == 0;
+#pragma unroll
+      for (int q = 0; q < KS; ++q) {
+        if (!placed && off[q] > 0) {
+          sum = __fadd_rn(sum, xd);
+          placed = true;
+        }
+        if ((m >> q) & 1u) sum = __fadd_rn(sum, __fmul_rn(v[q], xx[q]));
+      }
+      if (!placed) sum = __fadd_rn(sum, xd);
+      if (live) {
+        const double ds = (double)sum;
+        const float out = (a.beta == 0.0) ? (float)(a.alpha * ds)
+                                          : (float)(a.alpha * ds + a.beta * (double)a.y_in[r]);
+        a.y_out[r] = out;
+        float wa = 0.0f, wbv = 0.0f;
+        if constexpr (NW >= 1)
+          wa = *reinterpret_cast<const float *>(st + a.w_off + 4 * (lr - iw0));
+        if constexpr (NW >= 2)
+          wbv = *reinterpret_cast<const float *>(st + a.w_off + kWRunBytes + 4 * (lr - iw1));
+        if constexpr (M0 == kDotW) acc[0] += (double)wa * (double)out;
+        if constexpr (M0 == kDotSelf) acc[0] += (double)out * (double)out;
+        if constexpr (M1 == kDotW) acc[1] += (double)(M0 == kDotW ? wbv : wa) * (double)out;
+        if constexpr (M1 == kDotSelf) acc[1] += (double)out * (double)out;
+      }
+    }
     // the warp is done with the stage
     __syncwarp();
     if (lane == 0) {
       mbar_arrive(empty0 + 8 * s);
       flags[kSlotFlagWarpDone + warp] = k + 1;
-    }
-    const int r = sl * kSlotRows + ct;
-    const bool live = r < a.n_rows;
-    int off[KS > 0 ? KS : 1];
-    float xx[KS > 0 ? KS : 1];
-#pragma unroll
-    for (int q = 0; q < KS; ++q) {
-      off[q] = a.tab.offs[q];
-      xx[q] = ((m >> q) & 1u) ? __ldg(a.x + r + off[q]) : 0.0f;
-    }
-    const float xd = (a.unit && live) ? __ldg(a.x + r) : 0.0f;
-    // ascending columns, products rounded separately: the CRS row loop
-    float sum = 0.0f;
-    bool placed = a.unit == 0;
-#pragma unroll
-    for (int q = 0; q < KS; ++q) {
-      if (!placed && off[q] > 0) {
-        sum = __fadd_rn(sum, xd);
-        placed = true;
-      }
-      if ((m >> q) & 1u) sum = __fadd_rn(sum, __fmul_rn(v[q], xx[q]));
-    }
-    if (!placed) sum = __fadd_rn(sum, xd);
-    if (live) {
-      const double ds = (double)sum;
-      const float out = (a.beta == 0.0) ? (float)(a.alpha * ds)
-                                        : (float)(a.alpha * ds + a.beta * (double)a.y_in[r]);
-      a.y_out[r] = out;
-      if constexpr (M0 == kDotW) acc[0] += (double)a.w0[r] * (double)out;
-      if constexpr (M0 == kDotSelf) acc[0] += (double)out * (double)out;
-      if constexpr (M1 == kDotW) acc[1] += (double)a.w1[r] * (double)out;
-      if constexpr (M1 == kDotSelf) acc[1] += (double)out * (double)out;
     }
   }
   if constexpr (NR > 0) {
@@ -339,57 +433,105 @@ __global__ void __launch_bounds__(kSlotThreads, 4) spmv_slots_kernel(const SlotA
   }
 }
 
-// Launch geometry of one instantiation, set up once (outside any stream
-// capture: slots_build calls slots_prepare): the shared-memory opt-in and
-// the CTAs per SM.
+// Largest dynamic shared memory a slot launch may ask for, and what two
+// CTAs on one SM may use together (228 KB per SM, 1 KB reserved per CTA).
+constexpr int kSlotSmemMax = 220 * 1024;
+constexpr int kSlotSmemPerSm = 226 * 1024;
+
+// Per instantiation, once (outside any stream capture: slots_build calls
+// slots_prepare): the shared-memory opt-in.
 template <int KS, int M0, int M1>
 struct SlotLaunch {
-  static constexpr int kSmem = SlotSmem<KS>::kBytes;
-  static_assert(kSmem <= 48 * 1024, "slot stages fit the default shared-memory limit");
-  static int per_sm;
+  static bool ready;
   static cudaError_t prepare() {
-    if (per_sm > 0) return cudaSuccess;
-    constexpr auto k = spmv_slots_kernel<KS, M0, M1>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
-    if (e != cudaSuccess) return e;
-    int b = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kSlotThreads, kSmem);
-    if (e != cudaSuccess) return e;
-    per_sm = b < 1 ? 1 : b;
-    return cudaSuccess;
+    if (ready) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(spmv_slots_kernel<KS, M0, M1>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               kSlotSmemMax);
+    if (e == cudaSuccess) ready = true;
+    return e;
   }
-  static cudaError_t launch(const SlotArgs &a, int num_sms, cudaStream_t stream) {
-    const cudaError_t e = prepare();
-    if (e != cudaSuccess) return e;
-    int g = std::min(a.n_slices, per_sm * num_sms);
-    g = std::max(std::min(g, kMaxPartialBlocks), 1);
-    return launch_dependent(spmv_slots_kernel<KS, M0, M1>, g, kSlotThreads, kSmem, stream, a);
+  static int per_sm(int smem) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, spmv_slots_kernel<KS, M0, M1>,
+                                                      kSlotThreads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      b = 0;
+    }
+    return b;
+  }
+  static cudaError_t launch(const SlotArgs &a, int grid, int smem, cudaStream_t stream) {
+    return launch_dependent(spmv_slots_kernel<KS, M0, M1>, grid, kSlotThreads, smem, stream, a);
   }
 };
 template <int KS, int M0, int M1>
-int SlotLaunch<KS, M0, M1>::per_sm = 0;
+bool SlotLaunch<KS, M0, M1>::ready = false;
 
 template <int KS>
-cudaError_t prepare_ks() {
+cudaError_t prepare_ks(int smem, int *min_per_sm) {
   cudaError_t e = SlotLaunch<KS, kDotNone, kDotNone>::prepare();
   if (e == cudaSuccess) e = SlotLaunch<KS, kDotW, kDotNone>::prepare();
   if (e == cudaSuccess) e = SlotLaunch<KS, kDotW, kDotSelf>::prepare();
   if (e == cudaSuccess) e = SlotLaunch<KS, kDotSelf, kDotNone>::prepare();
-  return e;
+  if (e != cudaSuccess) return e;
+  int b = SlotLaunch<KS, kDotNone, kDotNone>::per_sm(smem);
+  b = std::min(b, SlotLaunch<KS, kDotW, kDotNone>::per_sm(smem));
+  b = std::min(b, SlotLaunch<KS, kDotW, kDotSelf>::per_sm(smem));
+  b = std::min(b, SlotLaunch<KS, kDotSelf, kDotNone>::per_sm(smem));
+  *min_per_sm = b;
+  return cudaSuccess;
 }
 
-cudaError_t slots_prepare(int K) {
+cudaError_t slots_prepare(int K, int smem, int *per_sm) {
   switch (K) {
-    case 0: return prepare_ks<0>();
-    case 1: return prepare_ks<1>();
-    case 2: return prepare_ks<2>();
-    case 3: return prepare_ks<3>();
-    case 4: return prepare_ks<4>();
-    case 5: return prepare_ks<5>();
-    case 6: return prepare_ks<6>();
-    case 7: return prepare_ks<7>();
-    default: return prepare_ks<8>();
+    case 0: return prepare_ks<0>(smem, per_sm);
+    case 1: return prepare_ks<1>(smem, per_sm);
+    case 2: return prepare_ks<2>(smem, per_sm);
+    case 3: return prepare_ks<3>(smem, per_sm);
+    case 4: return prepare_ks<4>(smem, per_sm);
+    case 5: return prepare_ks<5>(smem, per_sm);
+    case 6: return prepare_ks<6>(smem, per_sm);
+    case 7: return prepare_ks<7>(smem, per_sm);
+    default: return prepare_ks<8>(smem, per_sm);
   }
+}
+
+// The stage plan of a layout with offsets offs[0..K) (+ the diagonal): x
+// windows (offsets closer than kSlotMergeGap share one), their places in a
+// stage, and the weight runs after them.
+void plan_stages(SlotFormat &f) {
+  std::vector<std::pair<int, int>> need;  // (offset, slot or -1 for the diagonal)
+  for (int q = 0; q < f.K; ++q) need.push_back({f.offs[q], q});
+  if (f.unit) need.push_back({0, -1});
+  std::sort(need.begin(), need.end());
+  f.n_win = 0;
+  f.diag_win = -1;
+  int bytes = kSlotGroup * slot_rec_bytes(f.K);
+  int lo = 0, hi = 0;
+  auto close = [&]() {
+    const int w = f.n_win - 1;
+    f.win_lo[w] = lo;
+    f.win_len[w] = hi - lo + kGroupRows;
+    f.win_off[w] = bytes;
+    // the copy of L elements rounded out to 16-byte boundaries at both ends
+    bytes += ((4 * f.win_len[w] + 15) & ~15) + 32;
+  };
+  for (size_t i = 0; i < need.size(); ++i) {
+    const int o = need[i].first;
+    if (f.n_win == 0 || (long long)o - hi > kSlotMergeGap) {
+      if (f.n_win > 0) close();
+      ++f.n_win;
+      lo = hi = o;
+    } else {
+      hi = o;
+    }
+    if (need[i].second >= 0) f.slot_win[need[i].second] = f.n_win - 1;
+    else f.diag_win = f.n_win - 1;
+  }
+  if (f.n_win > 0) close();
+  f.w_off = bytes;
+  bytes += 2 * kWRunBytes;
+  f.stage_bytes = bytes;
 }
 
 }  // namespace
@@ -449,17 +591,32 @@ int slots_build(CsrPlan &p, cudaStream_t s) {
   const int K = (int)uni.size();
   SlotTable tab;
   for (int q = 0; q < kMaxSlots; ++q) tab.offs[q] = q < K ? uni[q] : 0;
-  e = slots_prepare(K);
-  if (e != cudaSuccess) {
-    set_last_error("slot SpMV set-up", e);
-    return MLSH_ERR_CUDA;
-  }
   SlotFormat *f = new (std::nothrow) SlotFormat();
   if (!f) return MLSH_ERR_OOM;
   for (int q = 0; q < kMaxSlots; ++q) f->offs[q] = tab.offs[q];
   f->K = K;
   f->unit = unit;
   f->n_slices = n_slices;
+  plan_stages(*f);
+  // two CTAs per SM of two stages each where they fit (twice the consumer
+  // warps to hide shared-memory latency), else as many stages as fit one
+  f->stages = 2 * (2 * f->stage_bytes + kSlotTailBytes) <= kSlotSmemPerSm
+                  ? 2
+                  : std::min(kMaxSlotStages, (kSlotSmemMax - kSlotTailBytes) / f->stage_bytes);
+  int per_sm = 0;
+  if (f->stages >= 2) {
+    e = slots_prepare(K, f->stages * f->stage_bytes + kSlotTailBytes, &per_sm);
+    if (e != cudaSuccess) {
+      delete f;
+      set_last_error("slot SpMV set-up", e);
+      return MLSH_ERR_CUDA;
+    }
+  }
+  if (f->stages < 2 || per_sm < 1) {  // windows too wide: the CRS kernel stays
+    delete f;
+    return MLSH_SUCCESS;
+  }
+  f->grid_per_sm = per_sm;
   if (pool_alloc(&f->recs, (size_t)f->bytes(), s) != cudaSuccess) {
     cudaGetLastError();
     delete f;
@@ -486,10 +643,24 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
   const SlotFormat &f = *p.slots;
   SlotArgs a;
   a.recs = f.recs;
-  for (int q = 0; q < kMaxSlots; ++q) a.tab.offs[q] = f.offs[q];
+  for (int q = 0; q < kMaxSlots; ++q) {
+    a.offs[q] = f.offs[q];
+    a.slot_win[q] = f.slot_win[q];
+  }
+  for (int w = 0; w < kMaxSlotWin; ++w) {
+    a.win_lo[w] = f.win_lo[w];
+    a.win_len[w] = f.win_len[w];
+    a.win_off[w] = f.win_off[w];
+  }
+  a.n_win = f.n_win;
+  a.diag_win = f.diag_win;
+  a.w_off = f.w_off;
+  a.stage_bytes = f.stage_bytes;
+  a.stages = f.stages;
   a.unit = f.unit;
   a.n_rows = p.n_rows;
   a.n_slices = f.n_slices;
+  a.n_groups = (f.n_slices + kSlotGroup - 1) / kSlotGroup;
   a.x = x;
   a.y_out = y_out;
   a.y_in = y_in;
@@ -502,16 +673,19 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
   a.dot_out = dot_out;
   a.done = done;
   a.err = h.err_flag;
+  const int smem = f.stages * f.stage_bytes + kSlotTailBytes;
+  const int grid = std::max(1, std::min({a.n_groups, f.grid_per_sm * h.num_sms,
+                                         kMaxPartialBlocks}));
   switch (f.K) {
-    case 0: return SlotLaunch<0, M0, M1>::launch(a, h.num_sms, stream);
-    case 1: return SlotLaunch<1, M0, M1>::launch(a, h.num_sms, stream);
-    case 2: return SlotLaunch<2, M0, M1>::launch(a, h.num_sms, stream);
-    case 3: return SlotLaunch<3, M0, M1>::launch(a, h.num_sms, stream);
-    case 4: return SlotLaunch<4, M0, M1>::launch(a, h.num_sms, stream);
-    case 5: return SlotLaunch<5, M0, M1>::launch(a, h.num_sms, stream);
-    case 6: return SlotLaunch<6, M0, M1>::launch(a, h.num_sms, stream);
-    case 7: return SlotLaunch<7, M0, M1>::launch(a, h.num_sms, stream);
-    default: return SlotLaunch<8, M0, M1>::launch(a, h.num_sms, stream);
+    case 0: return SlotLaunch<0, M0, M1>::launch(a, grid, smem, stream);
+    case 1: return SlotLaunch<1, M0, M1>::launch(a, grid, smem, stream);
+    case 2: return SlotLaunch<2, M0, M1>::launch(a, grid, smem, stream);
+    case 3: return SlotLaunch<3, M0, M1>::launch(a, grid, smem, stream);
+    case 4: return SlotLaunch<4, M0, M1>::launch(a, grid, smem, stream);
+    case 5: return SlotLaunch<5, M0, M1>::launch(a, grid, smem, stream);
+    case 6: return SlotLaunch<6, M0, M1>::launch(a, grid, smem, stream);
+    case 7: return SlotLaunch<7, M0, M1>::launch(a, grid, smem, stream);
+    default: return SlotLaunch<8, M0, M1>::launch(a, grid, smem, stream);
   }
 }
 
