@@ -58,6 +58,33 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
+// try_wait with a suspend-time hint: a warp whose phase is not complete is
+// suspended by the hardware (up to hint_ns) instead of spinning, so waiting
+// warps leave the issue slots to the working ones.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t bar, uint32_t parity,
+                                                    uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
+// The bounded wait below with suspending polls.
+__device__ __forceinline__ bool mbar_wait_sleep_bounded(uint32_t bar, uint32_t parity,
+                                                        uint64_t limit_ns) {
+  if (mbar_try_wait_sleep(bar, parity, 1000u)) return true;
+  const uint64_t t0 = global_timer_ns();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_try_wait_sleep(bar, parity, 1000u)) return true;
+    if ((it & 63u) == 0 && global_timer_ns() - t0 > limit_ns) return false;
+  }
+}
+
 // Wait for the phase with the given parity to complete, giving up after
 // `limit_ns` of wall-clock time.  Returns false on timeout.  The clock is
 // read every 1,024 polls only: timer reads in busy poll loops slow the

@@ -147,6 +147,7 @@ struct SlotArgs {
   int win_off[kMaxSlotWin];
   int n_win;
   int diag_win;
+  int dpos;  // unit diagonal: its place among the slots (the count of negative offsets)
   int w_off;
   int stage_bytes;
   int stages;
@@ -176,6 +177,12 @@ constexpr int kSlotTailBytes = 2 * kMaxSlotStages * 8 + 32 * 8 + 16 * 4;
 constexpr int kSlotFlagAbort = 0;
 constexpr int kSlotFlagLast = 1;
 constexpr int kSlotFlagWarpDone = 2;  // 8 slots: stages each consumer warp has read
+
+__device__ __forceinline__ float ld_shared_f32(uint32_t addr) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+  return v;
+}
 
 // Elements [a, a + len) of v clipped to [0, n): the first element s0, the
 // bytes of the 16-byte-rounded copy (0 if empty) and its source.  The
@@ -255,9 +262,9 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
           const uint64_t t0 = global_timer_ns();
           ok = 0;
           for (uint32_t it = 1;; ++it) {
-            if (mbar_try_wait(empty0 + 8 * s, par)) { ok = 1; break; }
-            if ((it & 63u) == 0 && flags[kSlotFlagAbort]) break;
-            if ((it & 1023u) == 0 && global_timer_ns() - t0 > kWaitLimitNs) {
+            if (mbar_try_wait_sleep(empty0 + 8 * s, par, 1000u)) { ok = 1; break; }
+            if ((it & 7u) == 0 && flags[kSlotFlagAbort]) break;
+            if ((it & 63u) == 0 && global_timer_ns() - t0 > kWaitLimitNs) {
               atomicExch(a.err, MLSH_ERR_TIMEOUT);
               break;
             }
@@ -334,20 +341,19 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
   double acc[NA];
 #pragma unroll
   for (int q = 0; q < NA; ++q) acc[q] = 0.0;
-  int off[KS > 0 ? KS : 1], woff[KS > 0 ? KS : 1];
+  int woff[KS > 0 ? KS : 1];
 #pragma unroll
-  for (int q = 0; q < KS; ++q) {
-    off[q] = a.offs[q];
-    woff[q] = a.win_off[a.slot_win[q]];
-  }
+  for (int q = 0; q < KS; ++q) woff[q] = a.win_off[a.slot_win[q]] + 4 * a.offs[q];
   const int dwoff = a.diag_win >= 0 ? a.win_off[a.diag_win] : 0;
+  const bool plain = a.alpha == 1.0 && a.beta == 0.0;
+  const uint32_t smem0 = smem_addr(smem);
   int k = 0;
   for (int g = blockIdx.x; g < a.n_groups; g += gridDim.x, ++k) {
     const int s = k % STG;
     int ok = 1;
     if (lane == 0) {
       ok = flags[kSlotFlagAbort] == 0 &&
-           mbar_wait_bounded(full0 + 8 * s, (uint32_t)((k / STG) & 1), kWaitLimitNs);
+           mbar_wait_sleep_bounded(full0 + 8 * s, (uint32_t)((k / STG) & 1), kWaitLimitNs);
       if (!ok && flags[kSlotFlagAbort] == 0) {
         flags[kSlotFlagAbort] = 1;
         atomicExch(a.err, MLSH_ERR_TIMEOUT);
@@ -357,54 +363,54 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
     const unsigned char *st = smem + s * a.stage_bytes;
     const int sl0 = g * kSlotGroup;
     const long long R0 = (long long)sl0 * kSlotRows;
-    // per slot: its window's first staged element, relative to R0 (small)
-    int ib[KS > 0 ? KS : 1];
+    // per slot: the shared address of the value for local row 0 (its
+    // window's staged base, shifted by the slot's offset)
+    const uint32_t stg = smem0 + s * a.stage_bytes;
+    uint32_t xa[KS > 0 ? KS : 1];
 #pragma unroll
     for (int q = 0; q < KS; ++q)
-      ib[q] = (int)(staged_base(a.x, R0 + a.win_lo[a.slot_win[q]]) - R0);
-    const int idb = a.diag_win >= 0 ? (int)(staged_base(a.x, R0 + a.win_lo[a.diag_win]) - R0) : 0;
-    const int iw0 = (int)(staged_base(wv0, R0) - R0), iw1 = (int)(staged_base(wv1, R0) - R0);
+      xa[q] = stg + woff[q] -
+              4 * (int)(staged_base(a.x, R0 + a.win_lo[a.slot_win[q]]) - R0);
+    const uint32_t xda =
+        stg + dwoff - 4 * (a.diag_win >= 0 ? (int)(staged_base(a.x, R0 + a.win_lo[a.diag_win]) - R0) : 0);
+    const uint32_t wa0 = stg + a.w_off - 4 * (int)(staged_base(wv0, R0) - R0);
+    const uint32_t wa1 = stg + a.w_off + kWRunBytes - 4 * (int)(staged_base(wv1, R0) - R0);
     const int ns = min(kSlotGroup, a.n_slices - sl0);
     for (int gs = 0; gs < ns; ++gs) {
       const unsigned char *rec = st + gs * rec_bytes;
       const float *vals = reinterpret_cast<const float *>(rec + kSlotHeadBytes);
       const unsigned m = rec[ct];
       const int lr = gs * kSlotRows + ct;  // row within the stage
+      const uint32_t lr4 = 4u * (uint32_t)lr;
       const long long r = R0 + lr;
       const bool live = r < a.n_rows;
       float v[KS > 0 ? KS : 1], xx[KS > 0 ? KS : 1];
 #pragma unroll
       for (int q = 0; q < KS; ++q) {
         v[q] = vals[q * kSlotRows + ct];
-        xx[q] = ((m >> q) & 1u)
-                    ? *reinterpret_cast<const float *>(st + woff[q] + 4 * (lr + off[q] - ib[q]))
-                    : 0.0f;
+        xx[q] = ((m >> q) & 1u) ? ld_shared_f32(xa[q] + lr4) : 0.0f;
       }
-      const float xd = (a.unit && live)
-                           ? *reinterpret_cast<const float *>(st + dwoff + 4 * (lr - idb))
-                           : 0.0f;
+      const float xd = a.unit ? ld_shared_f32(xda + lr4) : 0.0f;
       // ascending columns, products rounded separately: the CRS row loop
+      // (the diagonal, when implicit, comes after the dpos negative offsets)
       float sum = 0.0f;
-      bool placed = a.unit == 0;
 #pragma unroll
       for (int q = 0; q < KS; ++q) {
-        if (!placed && off[q] > 0) {
-          sum = __fadd_rn(sum, xd);
-          placed = true;
-        }
+        if (q == a.dpos) sum = __fadd_rn(sum, xd);
         if ((m >> q) & 1u) sum = __fadd_rn(sum, __fmul_rn(v[q], xx[q]));
       }
-      if (!placed) sum = __fadd_rn(sum, xd);
+      if (a.unit && a.dpos >= KS) sum = __fadd_rn(sum, xd);
       if (live) {
-        const double ds = (double)sum;
-        const float out = (a.beta == 0.0) ? (float)(a.alpha * ds)
-                                          : (float)(a.alpha * ds + a.beta * (double)a.y_in[r]);
+        float out = sum;  // alpha = 1, beta = 0: (float)(1.0 * (double)sum) == sum
+        if (!plain) {
+          const double ds = (double)sum;
+          out = (a.beta == 0.0) ? (float)(a.alpha * ds)
+                                : (float)(a.alpha * ds + a.beta * (double)a.y_in[r]);
+        }
         a.y_out[r] = out;
         float wa = 0.0f, wbv = 0.0f;
-        if constexpr (NW >= 1)
-          wa = *reinterpret_cast<const float *>(st + a.w_off + 4 * (lr - iw0));
-        if constexpr (NW >= 2)
-          wbv = *reinterpret_cast<const float *>(st + a.w_off + kWRunBytes + 4 * (lr - iw1));
+        if constexpr (NW >= 1) wa = ld_shared_f32(wa0 + lr4);
+        if constexpr (NW >= 2) wbv = ld_shared_f32(wa1 + lr4);
         if constexpr (M0 == kDotW) acc[0] += (double)wa * (double)out;
         if constexpr (M0 == kDotSelf) acc[0] += (double)out * (double)out;
         if constexpr (M1 == kDotW) acc[1] += (double)(M0 == kDotW ? wbv : wa) * (double)out;
@@ -654,6 +660,7 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
   }
   a.n_win = f.n_win;
   a.diag_win = f.diag_win;
+  a.dpos = f.unit ? (int)(std::lower_bound(f.offs, f.offs + f.K, 0) - f.offs) : kMaxSlots + 1;
   a.w_off = f.w_off;
   a.stage_bytes = f.stage_bytes;
   a.stages = f.stages;
