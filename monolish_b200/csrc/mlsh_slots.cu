@@ -147,6 +147,10 @@ struct SlotArgs {
   int win_off[kMaxSlotWin];
   int n_win;
   int diag_win;
+  int lo_min;              // smallest window start (relative to a stage's first row)
+  int xo[kMaxSlots];       // unclipped stages: byte offset of slot q's value of row 0
+  int xdo;                 // ... of the diagonal's
+  int w0o, w1o;            // ... of the dot weights'
   int dpos;  // unit diagonal: its place among the slots (the count of negative offsets)
   int w_off;
   int stage_bytes;
@@ -341,10 +345,6 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
   double acc[NA];
 #pragma unroll
   for (int q = 0; q < NA; ++q) acc[q] = 0.0;
-  int woff[KS > 0 ? KS : 1];
-#pragma unroll
-  for (int q = 0; q < KS; ++q) woff[q] = a.win_off[a.slot_win[q]] + 4 * a.offs[q];
-  const int dwoff = a.diag_win >= 0 ? a.win_off[a.diag_win] : 0;
   const bool plain = a.alpha == 1.0 && a.beta == 0.0;
   const uint32_t smem0 = smem_addr(smem);
   int k = 0;
@@ -363,27 +363,39 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
     const unsigned char *st = smem + s * a.stage_bytes;
     const int sl0 = g * kSlotGroup;
     const long long R0 = (long long)sl0 * kSlotRows;
-    // per slot: the shared address of the value for local row 0 (its
-    // window's staged base, shifted by the slot's offset)
+    // per slot: the shared address of the value for local row 0 of this
+    // stage.  Stages start on kGroupRows boundaries, so a window's 16-byte
+    // rounding is the same in every stage whose window is not clipped at
+    // row 0: there the launch's precomputed offsets hold; the first stages
+    // recompute.
     const uint32_t stg = smem0 + s * a.stage_bytes;
     uint32_t xa[KS > 0 ? KS : 1];
+    uint32_t xda = stg + a.xdo;
+    if (R0 + a.lo_min >= 0) {
 #pragma unroll
-    for (int q = 0; q < KS; ++q)
-      xa[q] = stg + woff[q] -
-              4 * (int)(staged_base(a.x, R0 + a.win_lo[a.slot_win[q]]) - R0);
-    const uint32_t xda =
-        stg + dwoff - 4 * (a.diag_win >= 0 ? (int)(staged_base(a.x, R0 + a.win_lo[a.diag_win]) - R0) : 0);
-    const uint32_t wa0 = stg + a.w_off - 4 * (int)(staged_base(wv0, R0) - R0);
-    const uint32_t wa1 = stg + a.w_off + kWRunBytes - 4 * (int)(staged_base(wv1, R0) - R0);
+      for (int q = 0; q < KS; ++q) xa[q] = stg + a.xo[q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < KS; ++q)
+        xa[q] = stg + a.win_off[a.slot_win[q]] + 4 * a.offs[q] -
+                4 * (int)(staged_base(a.x, R0 + a.win_lo[a.slot_win[q]]) - R0);
+      if (a.diag_win >= 0)
+        xda = stg + a.win_off[a.diag_win] -
+              4 * (int)(staged_base(a.x, R0 + a.win_lo[a.diag_win]) - R0);
+    }
+    const uint32_t wa0 = stg + a.w0o, wa1 = stg + a.w1o;
     const int ns = min(kSlotGroup, a.n_slices - sl0);
-    for (int gs = 0; gs < ns; ++gs) {
+    const long long left = a.n_rows - R0;
+    const int nlive = left < kGroupRows ? (int)left : kGroupRows;
+    float *ys = a.y_out + R0;
+#pragma unroll
+    for (int gs = 0; gs < kSlotGroup; ++gs) {
+      if (gs >= ns) break;
       const unsigned char *rec = st + gs * rec_bytes;
       const float *vals = reinterpret_cast<const float *>(rec + kSlotHeadBytes);
       const unsigned m = rec[ct];
       const int lr = gs * kSlotRows + ct;  // row within the stage
       const uint32_t lr4 = 4u * (uint32_t)lr;
-      const long long r = R0 + lr;
-      const bool live = r < a.n_rows;
       float v[KS > 0 ? KS : 1], xx[KS > 0 ? KS : 1];
 #pragma unroll
       for (int q = 0; q < KS; ++q) {
@@ -400,14 +412,14 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
         if ((m >> q) & 1u) sum = __fadd_rn(sum, __fmul_rn(v[q], xx[q]));
       }
       if (a.unit && a.dpos >= KS) sum = __fadd_rn(sum, xd);
-      if (live) {
+      if (lr < nlive) {
         float out = sum;  // alpha = 1, beta = 0: (float)(1.0 * (double)sum) == sum
         if (!plain) {
           const double ds = (double)sum;
           out = (a.beta == 0.0) ? (float)(a.alpha * ds)
-                                : (float)(a.alpha * ds + a.beta * (double)a.y_in[r]);
+                                : (float)(a.alpha * ds + a.beta * (double)a.y_in[R0 + lr]);
         }
-        a.y_out[r] = out;
+        ys[lr] = out;
         float wa = 0.0f, wbv = 0.0f;
         if constexpr (NW >= 1) wa = ld_shared_f32(wa0 + lr4);
         if constexpr (NW >= 2) wbv = ld_shared_f32(wa1 + lr4);
@@ -660,6 +672,27 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
   }
   a.n_win = f.n_win;
   a.diag_win = f.diag_win;
+  // Offsets of unclipped stages: a window of stage R0 starts at element
+  // R0 + lo rounded down to 16 bytes, and R0 is a multiple of kGroupRows, so
+  // the rounding depends only on lo and the vector's own address.
+  auto head = [](const float *v, long long e) {
+    return (int)((((uintptr_t)v + 4 * (uintptr_t)e) & 15u) >> 2);
+  };
+  a.lo_min = 0;
+  for (int w = 0; w < f.n_win; ++w) a.lo_min = std::min(a.lo_min, f.win_lo[w]);
+  for (int q = 0; q < kMaxSlots; ++q) {
+    const int w = f.slot_win[q];
+    a.xo[q] = q < f.K ? f.win_off[w] + 4 * f.offs[q] - 4 * (f.win_lo[w] - head(x, f.win_lo[w]))
+                      : 0;
+  }
+  a.xdo = f.diag_win >= 0
+              ? f.win_off[f.diag_win] - 4 * (f.win_lo[f.diag_win] - head(x, f.win_lo[f.diag_win]))
+              : 0;
+  {
+    const float *wv0 = (M0 == kDotW) ? w0 : w1;
+    a.w0o = f.w_off + 4 * (wv0 ? head(wv0, 0) : 0);
+    a.w1o = f.w_off + kWRunBytes + 4 * (w1 ? head(w1, 0) : 0);
+  }
   a.dpos = f.unit ? (int)(std::lower_bound(f.offs, f.offs + f.K, 0) - f.offs) : kMaxSlots + 1;
   a.w_off = f.w_off;
   a.stage_bytes = f.stage_bytes;
