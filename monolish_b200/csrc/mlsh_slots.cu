@@ -151,6 +151,9 @@ struct SlotArgs {
   int xo[kMaxSlots];       // unclipped stages: byte offset of slot q's value of row 0
   int xdo;                 // ... of the diagonal's
   int w0o, w1o;            // ... of the dot weights'
+  unsigned xal;            // bit q: slot q's offset is 16-byte aligned; bit 8: the diagonal's
+  unsigned full4;          // four rows' mask bytes with every slot present
+  int yal;                 // y is 16-byte aligned
   int dpos;  // unit diagonal: its place among the slots (the count of negative offsets)
   int w_off;
   int stage_bytes;
@@ -188,6 +191,14 @@ __device__ __forceinline__ float ld_shared_f32(uint32_t addr) {
   return v;
 }
 
+__device__ __forceinline__ float4 ld_shared_f32x4(uint32_t addr) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"(addr));
+  return v;
+}
+
 // Elements [a, a + len) of v clipped to [0, n): the first element s0, the
 // bytes of the 16-byte-rounded copy (0 if empty) and its source.  The
 // rounded range never leaves the 16-byte chunks holding elements s0 and
@@ -218,7 +229,12 @@ __device__ __forceinline__ long long staged_base(const float *v, long long a) {
 // like the vector kernels' sums (fixed order, last CTA finalises).  Every
 // wait is bounded: a consumer warp that gives up records MLSH_ERR_TIMEOUT
 // and stops; the producer then waits for its copies in flight and exits.
-template <int KS, int M0, int M1>
+// DP: where the implicit unit diagonal goes among the slots, known at
+// compile time (symmetric stencils: KS / 2), or kDpRuntime to read it from
+// the launch (a.unit, a.dpos).
+constexpr int kDpRuntime = -1;
+
+template <int KS, int DP, int M0, int M1>
 __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotArgs a) {
   constexpr int NR = (M0 != kDotNone ? 1 : 0) + (M1 != kDotNone ? 1 : 0);
   constexpr int NA = NR > 0 ? NR : 1;
@@ -346,7 +362,15 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
 #pragma unroll
   for (int q = 0; q < NA; ++q) acc[q] = 0.0;
   const bool plain = a.alpha == 1.0 && a.beta == 0.0;
+  const bool unit = DP >= 0 || a.unit != 0;
+  const int dpos = DP >= 0 ? DP : (a.unit ? a.dpos : kMaxSlots + 1);
   const uint32_t smem0 = smem_addr(smem);
+  // thread ct takes rows 4 ct .. 4 ct + 3 of each stage: slice ct / 64 of
+  // the stage, rows sr .. sr + 3 of that slice
+  const int lr0 = 4 * ct;
+  const int gs = lr0 / kSlotRows;
+  const int sr = lr0 % kSlotRows;
+  const uint32_t lr4 = 4u * (uint32_t)lr0;
   int k = 0;
   for (int g = blockIdx.x; g < a.n_groups; g += gridDim.x, ++k) {
     const int s = k % STG;
@@ -366,15 +390,17 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
     // per slot: the shared address of the value for local row 0 of this
     // stage.  Stages start on kGroupRows boundaries, so a window's 16-byte
     // rounding is the same in every stage whose window is not clipped at
-    // row 0: there the launch's precomputed offsets hold; the first stages
-    // recompute.
+    // row 0: there the launch's precomputed offsets (and their 16-byte
+    // alignment flags) hold; the first stages recompute.
     const uint32_t stg = smem0 + s * a.stage_bytes;
     uint32_t xa[KS > 0 ? KS : 1];
     uint32_t xda = stg + a.xdo;
+    unsigned xal = a.xal;
     if (R0 + a.lo_min >= 0) {
 #pragma unroll
       for (int q = 0; q < KS; ++q) xa[q] = stg + a.xo[q];
     } else {
+      xal = 0;
 #pragma unroll
       for (int q = 0; q < KS; ++q)
         xa[q] = stg + a.win_off[a.slot_win[q]] + 4 * a.offs[q] -
@@ -383,50 +409,93 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
         xda = stg + a.win_off[a.diag_win] -
               4 * (int)(staged_base(a.x, R0 + a.win_lo[a.diag_win]) - R0);
     }
-    const uint32_t wa0 = stg + a.w0o, wa1 = stg + a.w1o;
     const int ns = min(kSlotGroup, a.n_slices - sl0);
-    const long long left = a.n_rows - R0;
-    const int nlive = left < kGroupRows ? (int)left : kGroupRows;
-    float *ys = a.y_out + R0;
-#pragma unroll
-    for (int gs = 0; gs < kSlotGroup; ++gs) {
-      if (gs >= ns) break;
+    const long long left = a.n_rows - R0 - lr0;
+    const int nl = left < 4 ? (int)left : 4;  // live rows of this thread
+    if (gs < ns && nl > 0) {
       const unsigned char *rec = st + gs * rec_bytes;
-      const float *vals = reinterpret_cast<const float *>(rec + kSlotHeadBytes);
-      const unsigned m = rec[ct];
-      const int lr = gs * kSlotRows + ct;  // row within the stage
-      const uint32_t lr4 = 4u * (uint32_t)lr;
-      float v[KS > 0 ? KS : 1], xx[KS > 0 ? KS : 1];
+      const uint32_t m4 = *reinterpret_cast<const uint32_t *>(rec + sr);
+      const float *vals = reinterpret_cast<const float *>(rec + kSlotHeadBytes) + sr;
+      float v[KS > 0 ? KS : 1][4], xx[KS > 0 ? KS : 1][4], xd[4], sum[4];
 #pragma unroll
       for (int q = 0; q < KS; ++q) {
-        v[q] = vals[q * kSlotRows + ct];
-        xx[q] = ((m >> q) & 1u) ? ld_shared_f32(xa[q] + lr4) : 0.0f;
+        const float4 t = *reinterpret_cast<const float4 *>(vals + q * kSlotRows);
+        v[q][0] = t.x; v[q][1] = t.y; v[q][2] = t.z; v[q][3] = t.w;
       }
-      const float xd = a.unit ? ld_shared_f32(xda + lr4) : 0.0f;
-      // ascending columns, products rounded separately: the CRS row loop
-      // (the diagonal, when implicit, comes after the dpos negative offsets)
-      float sum = 0.0f;
+      const bool full = m4 == a.full4;
+      if (full) {
 #pragma unroll
-      for (int q = 0; q < KS; ++q) {
-        if (q == a.dpos) sum = __fadd_rn(sum, xd);
-        if ((m >> q) & 1u) sum = __fadd_rn(sum, __fmul_rn(v[q], xx[q]));
-      }
-      if (a.unit && a.dpos >= KS) sum = __fadd_rn(sum, xd);
-      if (lr < nlive) {
-        float out = sum;  // alpha = 1, beta = 0: (float)(1.0 * (double)sum) == sum
-        if (!plain) {
-          const double ds = (double)sum;
-          out = (a.beta == 0.0) ? (float)(a.alpha * ds)
-                                : (float)(a.alpha * ds + a.beta * (double)a.y_in[R0 + lr]);
+        for (int q = 0; q < KS; ++q) {
+          if ((xal >> q) & 1u) {
+            const float4 t = ld_shared_f32x4(xa[q] + lr4);
+            xx[q][0] = t.x; xx[q][1] = t.y; xx[q][2] = t.z; xx[q][3] = t.w;
+          } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) xx[q][j] = ld_shared_f32(xa[q] + lr4 + 4 * j);
+          }
         }
-        ys[lr] = out;
-        float wa = 0.0f, wbv = 0.0f;
-        if constexpr (NW >= 1) wa = ld_shared_f32(wa0 + lr4);
-        if constexpr (NW >= 2) wbv = ld_shared_f32(wa1 + lr4);
-        if constexpr (M0 == kDotW) acc[0] += (double)wa * (double)out;
-        if constexpr (M0 == kDotSelf) acc[0] += (double)out * (double)out;
-        if constexpr (M1 == kDotW) acc[1] += (double)(M0 == kDotW ? wbv : wa) * (double)out;
-        if constexpr (M1 == kDotSelf) acc[1] += (double)out * (double)out;
+      } else {
+#pragma unroll
+        for (int q = 0; q < KS; ++q)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            xx[q][j] = ((m4 >> (8 * j + q)) & 1u) ? ld_shared_f32(xa[q] + lr4 + 4 * j) : 0.0f;
+      }
+      if (unit) {
+        if (xal & (1u << kMaxSlots)) {
+          const float4 t = ld_shared_f32x4(xda + lr4);
+          xd[0] = t.x; xd[1] = t.y; xd[2] = t.z; xd[3] = t.w;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) xd[j] = j < nl ? ld_shared_f32(xda + lr4 + 4 * j) : 0.0f;
+        }
+      }
+      // per row: ascending columns, products rounded separately (the CRS
+      // row loop); the implicit diagonal after the dpos negative offsets
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        float sj = 0.0f;
+#pragma unroll
+        for (int q = 0; q < KS; ++q) {
+          if (q == dpos) sj = __fadd_rn(sj, xd[j]);
+          if (full || ((m4 >> (8 * j + q)) & 1u)) sj = __fadd_rn(sj, __fmul_rn(v[q][j], xx[q][j]));
+        }
+        if (unit && dpos >= KS) sj = __fadd_rn(sj, xd[j]);
+        sum[j] = sj;
+      }
+      const long long r0 = R0 + lr0;
+      float out[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        out[j] = sum[j];  // alpha = 1, beta = 0: (float)(1.0 * (double)sum) == sum
+        if (!plain && j < nl) {
+          const double ds = (double)sum[j];
+          out[j] = (a.beta == 0.0) ? (float)(a.alpha * ds)
+                                   : (float)(a.alpha * ds + a.beta * (double)a.y_in[r0 + j]);
+        }
+      }
+      if (nl == 4 && a.yal) {
+        *reinterpret_cast<float4 *>(a.y_out + r0) = make_float4(out[0], out[1], out[2], out[3]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (j < nl) a.y_out[r0 + j] = out[j];
+      }
+      float wa[4] = {0.0f, 0.0f, 0.0f, 0.0f}, wbv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if constexpr (NW >= 1) wa[j] = j < nl ? ld_shared_f32(stg + a.w0o + lr4 + 4 * j) : 0.0f;
+        if constexpr (NW >= 2) wbv[j] = j < nl ? ld_shared_f32(stg + a.w1o + lr4 + 4 * j) : 0.0f;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (j < nl) {
+          if constexpr (M0 == kDotW) acc[0] += (double)wa[j] * (double)out[j];
+          if constexpr (M0 == kDotSelf) acc[0] += (double)out[j] * (double)out[j];
+          if constexpr (M1 == kDotW)
+            acc[1] += (double)(M0 == kDotW ? wbv[j] : wa[j]) * (double)out[j];
+          if constexpr (M1 == kDotSelf) acc[1] += (double)out[j] * (double)out[j];
+        }
       }
     }
     // the warp is done with the stage
@@ -458,12 +527,12 @@ constexpr int kSlotSmemPerSm = 226 * 1024;
 
 // Per instantiation, once (outside any stream capture: slots_build calls
 // slots_prepare): the shared-memory opt-in.
-template <int KS, int M0, int M1>
+template <int KS, int DP, int M0, int M1>
 struct SlotLaunch {
   static bool ready;
   static cudaError_t prepare() {
     if (ready) return cudaSuccess;
-    const cudaError_t e = cudaFuncSetAttribute(spmv_slots_kernel<KS, M0, M1>,
+    const cudaError_t e = cudaFuncSetAttribute(spmv_slots_kernel<KS, DP, M0, M1>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                kSlotSmemMax);
     if (e == cudaSuccess) ready = true;
@@ -471,7 +540,7 @@ struct SlotLaunch {
   }
   static int per_sm(int smem) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, spmv_slots_kernel<KS, M0, M1>,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, spmv_slots_kernel<KS, DP, M0, M1>,
                                                       kSlotThreads, smem) != cudaSuccess) {
       cudaGetLastError();
       b = 0;
@@ -479,25 +548,35 @@ struct SlotLaunch {
     return b;
   }
   static cudaError_t launch(const SlotArgs &a, int grid, int smem, cudaStream_t stream) {
-    return launch_dependent(spmv_slots_kernel<KS, M0, M1>, grid, kSlotThreads, smem, stream, a);
+    return launch_dependent(spmv_slots_kernel<KS, DP, M0, M1>, grid, kSlotThreads, smem, stream,
+                            a);
   }
 };
-template <int KS, int M0, int M1>
-bool SlotLaunch<KS, M0, M1>::ready = false;
+template <int KS, int DP, int M0, int M1>
+bool SlotLaunch<KS, DP, M0, M1>::ready = false;
+
+template <int KS, int DP>
+cudaError_t prepare_modes(int smem, int *min_per_sm) {
+  cudaError_t e = SlotLaunch<KS, DP, kDotNone, kDotNone>::prepare();
+  if (e == cudaSuccess) e = SlotLaunch<KS, DP, kDotW, kDotNone>::prepare();
+  if (e == cudaSuccess) e = SlotLaunch<KS, DP, kDotW, kDotSelf>::prepare();
+  if (e == cudaSuccess) e = SlotLaunch<KS, DP, kDotSelf, kDotNone>::prepare();
+  if (e != cudaSuccess) return e;
+  int b = SlotLaunch<KS, DP, kDotNone, kDotNone>::per_sm(smem);
+  b = std::min(b, SlotLaunch<KS, DP, kDotW, kDotNone>::per_sm(smem));
+  b = std::min(b, SlotLaunch<KS, DP, kDotW, kDotSelf>::per_sm(smem));
+  b = std::min(b, SlotLaunch<KS, DP, kDotSelf, kDotNone>::per_sm(smem));
+  *min_per_sm = std::min(*min_per_sm, b);
+  return cudaSuccess;
+}
 
 template <int KS>
 cudaError_t prepare_ks(int smem, int *min_per_sm) {
-  cudaError_t e = SlotLaunch<KS, kDotNone, kDotNone>::prepare();
-  if (e == cudaSuccess) e = SlotLaunch<KS, kDotW, kDotNone>::prepare();
-  if (e == cudaSuccess) e = SlotLaunch<KS, kDotW, kDotSelf>::prepare();
-  if (e == cudaSuccess) e = SlotLaunch<KS, kDotSelf, kDotNone>::prepare();
-  if (e != cudaSuccess) return e;
-  int b = SlotLaunch<KS, kDotNone, kDotNone>::per_sm(smem);
-  b = std::min(b, SlotLaunch<KS, kDotW, kDotNone>::per_sm(smem));
-  b = std::min(b, SlotLaunch<KS, kDotW, kDotSelf>::per_sm(smem));
-  b = std::min(b, SlotLaunch<KS, kDotSelf, kDotNone>::per_sm(smem));
-  *min_per_sm = b;
-  return cudaSuccess;
+  *min_per_sm = 1 << 20;
+  cudaError_t e = prepare_modes<KS, kDpRuntime>(smem, min_per_sm);
+  if constexpr (KS == 4 || KS == 6 || KS == 8)
+    if (e == cudaSuccess) e = prepare_modes<KS, KS / 2>(smem, min_per_sm);
+  return e;
 }
 
 cudaError_t slots_prepare(int K, int smem, int *per_sm) {
@@ -694,6 +773,13 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
     a.w1o = f.w_off + kWRunBytes + 4 * (w1 ? head(w1, 0) : 0);
   }
   a.dpos = f.unit ? (int)(std::lower_bound(f.offs, f.offs + f.K, 0) - f.offs) : kMaxSlots + 1;
+  a.xal = 0;
+  for (int q = 0; q < f.K; ++q)
+    if ((a.xo[q] & 15) == 0) a.xal |= 1u << q;
+  if (f.diag_win >= 0 && (a.xdo & 15) == 0) a.xal |= 1u << kMaxSlots;
+  const unsigned mk = f.K >= 8 ? 0xffu : ((1u << f.K) - 1u);
+  a.full4 = mk | (mk << 8) | (mk << 16) | (mk << 24);
+  a.yal = ((uintptr_t)y_out & 15u) == 0 ? 1 : 0;
   a.w_off = f.w_off;
   a.stage_bytes = f.stage_bytes;
   a.stages = f.stages;
@@ -716,16 +802,20 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
   const int smem = f.stages * f.stage_bytes + kSlotTailBytes;
   const int grid = std::max(1, std::min({a.n_groups, f.grid_per_sm * h.num_sms,
                                          kMaxPartialBlocks}));
+  const bool sym = f.unit && a.dpos == f.K / 2 && (f.K % 2) == 0;
+  if (sym && f.K == 4) return SlotLaunch<4, 2, M0, M1>::launch(a, grid, smem, stream);
+  if (sym && f.K == 6) return SlotLaunch<6, 3, M0, M1>::launch(a, grid, smem, stream);
+  if (sym && f.K == 8) return SlotLaunch<8, 4, M0, M1>::launch(a, grid, smem, stream);
   switch (f.K) {
-    case 0: return SlotLaunch<0, M0, M1>::launch(a, grid, smem, stream);
-    case 1: return SlotLaunch<1, M0, M1>::launch(a, grid, smem, stream);
-    case 2: return SlotLaunch<2, M0, M1>::launch(a, grid, smem, stream);
-    case 3: return SlotLaunch<3, M0, M1>::launch(a, grid, smem, stream);
-    case 4: return SlotLaunch<4, M0, M1>::launch(a, grid, smem, stream);
-    case 5: return SlotLaunch<5, M0, M1>::launch(a, grid, smem, stream);
-    case 6: return SlotLaunch<6, M0, M1>::launch(a, grid, smem, stream);
-    case 7: return SlotLaunch<7, M0, M1>::launch(a, grid, smem, stream);
-    default: return SlotLaunch<8, M0, M1>::launch(a, grid, smem, stream);
+    case 0: return SlotLaunch<0, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 1: return SlotLaunch<1, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 2: return SlotLaunch<2, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 3: return SlotLaunch<3, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 4: return SlotLaunch<4, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 5: return SlotLaunch<5, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 6: return SlotLaunch<6, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 7: return SlotLaunch<7, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    default: return SlotLaunch<8, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
   }
 }
 
