@@ -33,16 +33,6 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
                               const float *w1, double *dot_out, const int *done,
                               cudaStream_t stream);
 
-// t = A s with s = r - alpha v formed on the fly (alpha = *rho / *vr0,
-// rounded to FP32, stored to *alpha_out as a double), s written out, and
-// the dots (t, s), (t, t) into dot_out[0..1]: BiCGSTAB's second SpMV with
-// its preceding vector update folded in.  Only for plans with the slot
-// layout (p.slots).
-cudaError_t launch_spmv_slots_s(const CsrPlan &p, const Handle &h, const float *r,
-                                const float *v, const double *rho, const double *vr0,
-                                double *alpha_out, float *s_out, float *t_out, double *dot_out,
-                                const int *done, cudaStream_t stream);
-
 int plan_diag(const CsrPlan &p, void *out, bool invert, cudaStream_t stream);
 int plan_inv_diag(CsrPlan &p, cudaStream_t stream, const void **out);
 

@@ -158,17 +158,11 @@ struct SlotFormat {
   int win_len[kMaxSlotWin] = {};  // window length in elements
   int win_off[kMaxSlotWin] = {};  // byte offset of the window in a stage
   int slot_win[kMaxSlots] = {};   // the window holding slot k's x values
-  int diag_win = -1;              // the window holding each row's own x_i
+  int diag_win = -1;              // the window holding x_i (unit diagonal)
   int w_off = 0;                  // byte offset of the dot weights' runs in a stage
-  int win_span = 0;               // bytes of one set of windows
   int stage_bytes = 0;
   int stages = 0;
   int grid_per_sm = 0;            // CTAs per SM of the launch
-  // the launch that also forms s = r - alpha v (two sets of windows, no
-  // weight runs)
-  int stage_bytes_fs = 0;
-  int stages_fs = 0;
-  int grid_per_sm_fs = 0;
   int64_t bytes() const { return (int64_t)n_slices * slot_rec_bytes(K); }
 };
 

@@ -951,18 +951,12 @@ cudaError_t mixbi_main(const SolveCtx &c, cudaStream_t s, CondRef cond) {
   e = launch_spmv_t<float, kDotW, kDotNone>(*c.plan, *c.h, 1.0, p, 0.0, nullptr, v, r0,
                                             nullptr, &st->vr0, done, s);
   if (e != cudaSuccess) return e;
-  if (c.plan->slots != nullptr && c.plan->slots->grid_per_sm_fs > 0) {
-    // slot layout: s = r - alpha v is formed inside the second SpMV
-    e = launch_spmv_slots_s(*c.plan, *c.h, r, v, &st->rho, &st->vr0, &st->alpha, sv, t,
-                            &st->ts, done, s);
-  } else {
-    BiSBody<float, false> sb;
-    sb.r = r; sb.v = v; sb.s = sv; sb.shat = sv; sb.d = nullptr; sb.st = st;
-    e = run_body<0, true>(*c.h, c.n, sb, done, s);
-    if (e != cudaSuccess) return e;
-    e = launch_spmv_t<float, kDotW, kDotSelf>(*c.plan, *c.h, 1.0, sv, 0.0, nullptr, t, sv,
-                                              nullptr, &st->ts, done, s);
-  }
+  BiSBody<float, false> sb;
+  sb.r = r; sb.v = v; sb.s = sv; sb.shat = sv; sb.d = nullptr; sb.st = st;
+  e = run_body<0, true>(*c.h, c.n, sb, done, s);
+  if (e != cudaSuccess) return e;
+  e = launch_spmv_t<float, kDotW, kDotSelf>(*c.plan, *c.h, 1.0, sv, 0.0, nullptr, t, sv,
+                                            nullptr, &st->ts, done, s);
   if (e != cudaSuccess) return e;
   MixXRBody xb;
   xb.x = x32; xb.r = r; xb.r0 = r0; xb.phat = p; xb.shat = sv; xb.s = sv; xb.t = t;

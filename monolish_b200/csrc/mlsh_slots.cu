@@ -152,16 +152,6 @@ struct SlotArgs {
   int xdo;                 // ... of the diagonal's
   int w0o, w1o;            // ... of the dot weights'
   unsigned xal;            // bit q: slot q's offset is 16-byte aligned; bit 8: the diagonal's
-  // the s = r - alpha v form (x = r): the second vector and its windows
-  const float *xv;
-  float *s_out;
-  const double *rho, *vr0;
-  double *alpha_out;
-  int win_span;            // bytes from an r window to the v window of the same offsets
-  int xo2[kMaxSlots];
-  int xdo2;
-  unsigned xal2;
-  int sal;                 // s_out is 16-byte aligned
   unsigned full4;          // four rows' mask bytes with every slot present
   int yal;                 // y is 16-byte aligned
   int dpos;  // unit diagonal: its place among the slots (the count of negative offsets)
@@ -244,13 +234,11 @@ __device__ __forceinline__ long long staged_base(const float *v, long long a) {
 // the launch (a.unit, a.dpos).
 constexpr int kDpRuntime = -1;
 
-template <int KS, int DP, int M0, int M1, bool FS>
+template <int KS, int DP, int M0, int M1>
 __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotArgs a) {
   constexpr int NR = (M0 != kDotNone ? 1 : 0) + (M1 != kDotNone ? 1 : 0);
   constexpr int NA = NR > 0 ? NR : 1;
-  // weight runs staged (FS: the weight of (t, s) is s itself, formed here)
-  constexpr int NW = FS ? 0 : (M0 == kDotW ? 1 : 0) + (M1 == kDotW ? 1 : 0);
-  static_assert(!FS || (M0 == kDotW && M1 == kDotSelf), "FS computes (t, s), (t, t)");
+  constexpr int NW = (M0 == kDotW ? 1 : 0) + (M1 == kDotW ? 1 : 0);
   extern __shared__ __align__(128) unsigned char smem[];
   pdl_wait();
   pdl_launch_dependents();
@@ -318,10 +306,6 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
       } else if (j < a.n_win) {
         bytes = clip_range(a.x, R0 + a.win_lo[j], a.win_len[j], a.n_rows, &src);
         dst = smem_addr(st + a.win_off[j]);
-      } else if (FS && j < 2 * a.n_win) {
-        const int jw = j - a.n_win;
-        bytes = clip_range(a.xv, R0 + a.win_lo[jw], a.win_len[jw], a.n_rows, &src);
-        dst = smem_addr(st + a.win_off[jw] + a.win_span);
       } else if (j == a.n_win && NW >= 1) {
         bytes = clip_range(wv0, R0, kGroupRows, a.n_rows, &src);
         dst = smem_addr(st + a.w_off);
@@ -377,11 +361,8 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
   double acc[NA];
 #pragma unroll
   for (int q = 0; q < NA; ++q) acc[q] = 0.0;
-  const bool plain = FS || (a.alpha == 1.0 && a.beta == 0.0);
+  const bool plain = a.alpha == 1.0 && a.beta == 0.0;
   const bool unit = DP >= 0 || a.unit != 0;
-  // FS: alpha = rho / (v, r0), rounded to FP32 (the state the previous
-  // kernel left)
-  const float alpha = FS ? (float)(*a.rho / *a.vr0) : 0.0f;
   const int dpos = DP >= 0 ? DP : (a.unit ? a.dpos : kMaxSlots + 1);
   const uint32_t smem0 = smem_addr(smem);
   // thread ct takes rows 4 ct .. 4 ct + 3 of each stage: slice ct / 64 of
@@ -412,33 +393,21 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
     // row 0: there the launch's precomputed offsets (and their 16-byte
     // alignment flags) hold; the first stages recompute.
     const uint32_t stg = smem0 + s * a.stage_bytes;
-    uint32_t xa[KS > 0 ? KS : 1], xa2[KS > 0 ? KS : 1];
-    uint32_t xda = stg + a.xdo, xda2 = stg + a.xdo2;
-    unsigned xal = a.xal, xal2 = a.xal2;
+    uint32_t xa[KS > 0 ? KS : 1];
+    uint32_t xda = stg + a.xdo;
+    unsigned xal = a.xal;
     if (R0 + a.lo_min >= 0) {
 #pragma unroll
-      for (int q = 0; q < KS; ++q) {
-        xa[q] = stg + a.xo[q];
-        if constexpr (FS) xa2[q] = stg + a.xo2[q];
-      }
+      for (int q = 0; q < KS; ++q) xa[q] = stg + a.xo[q];
     } else {
-      xal = xal2 = 0;
+      xal = 0;
 #pragma unroll
-      for (int q = 0; q < KS; ++q) {
-        const int w = a.slot_win[q];
-        xa[q] = stg + a.win_off[w] + 4 * a.offs[q] -
-                4 * (int)(staged_base(a.x, R0 + a.win_lo[w]) - R0);
-        if constexpr (FS)
-          xa2[q] = stg + a.win_off[w] + a.win_span + 4 * a.offs[q] -
-                   4 * (int)(staged_base(a.xv, R0 + a.win_lo[w]) - R0);
-      }
-      if (a.diag_win >= 0) {
+      for (int q = 0; q < KS; ++q)
+        xa[q] = stg + a.win_off[a.slot_win[q]] + 4 * a.offs[q] -
+                4 * (int)(staged_base(a.x, R0 + a.win_lo[a.slot_win[q]]) - R0);
+      if (a.diag_win >= 0)
         xda = stg + a.win_off[a.diag_win] -
               4 * (int)(staged_base(a.x, R0 + a.win_lo[a.diag_win]) - R0);
-        if constexpr (FS)
-          xda2 = stg + a.win_off[a.diag_win] + a.win_span -
-                 4 * (int)(staged_base(a.xv, R0 + a.win_lo[a.diag_win]) - R0);
-      }
     }
     const int ns = min(kSlotGroup, a.n_slices - sl0);
     const long long left = a.n_rows - R0 - lr0;
@@ -454,62 +423,32 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
         v[q][0] = t.x; v[q][1] = t.y; v[q][2] = t.z; v[q][3] = t.w;
       }
       const bool full = m4 == a.full4;
-      // four consecutive values of a window: one 16-byte load when aligned
-      auto ld4 = [&](uint32_t ad, bool al, float (&o)[4]) {
-        if (al) {
-          const float4 t = ld_shared_f32x4(ad);
-          o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
-        } else {
-#pragma unroll
-          for (int j = 0; j < 4; ++j) o[j] = ld_shared_f32(ad + 4 * j);
-        }
-      };
       if (full) {
 #pragma unroll
         for (int q = 0; q < KS; ++q) {
-          ld4(xa[q] + lr4, (xal >> q) & 1u, xx[q]);
-          if constexpr (FS) {  // s = r - alpha v at the gathered positions
-            float vv[4];
-            ld4(xa2[q] + lr4, (xal2 >> q) & 1u, vv);
+          if ((xal >> q) & 1u) {
+            const float4 t = ld_shared_f32x4(xa[q] + lr4);
+            xx[q][0] = t.x; xx[q][1] = t.y; xx[q][2] = t.z; xx[q][3] = t.w;
+          } else {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) xx[q][j] = __fmaf_rn(-alpha, vv[j], xx[q][j]);
+            for (int j = 0; j < 4; ++j) xx[q][j] = ld_shared_f32(xa[q] + lr4 + 4 * j);
           }
         }
       } else {
 #pragma unroll
         for (int q = 0; q < KS; ++q)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            float t = 0.0f;
-            if ((m4 >> (8 * j + q)) & 1u) {
-              t = ld_shared_f32(xa[q] + lr4 + 4 * j);
-              if constexpr (FS) t = __fmaf_rn(-alpha, ld_shared_f32(xa2[q] + lr4 + 4 * j), t);
-            }
-            xx[q][j] = t;
-          }
+          for (int j = 0; j < 4; ++j)
+            xx[q][j] = ((m4 >> (8 * j + q)) & 1u) ? ld_shared_f32(xa[q] + lr4 + 4 * j) : 0.0f;
       }
-      float sown[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // FS: s of the thread's own rows
-      if (unit || FS) {
-        float o[4];
-        if (nl == 4) {
-          ld4(xda + lr4, (xal >> kMaxSlots) & 1u, o);
+      if (unit) {
+        if (xal & (1u << kMaxSlots)) {
+          const float4 t = ld_shared_f32x4(xda + lr4);
+          xd[0] = t.x; xd[1] = t.y; xd[2] = t.z; xd[3] = t.w;
         } else {
 #pragma unroll
-          for (int j = 0; j < 4; ++j) o[j] = j < nl ? ld_shared_f32(xda + lr4 + 4 * j) : 0.0f;
+          for (int j = 0; j < 4; ++j) xd[j] = j < nl ? ld_shared_f32(xda + lr4 + 4 * j) : 0.0f;
         }
-        if constexpr (FS) {
-          float vv[4];
-          if (nl == 4) {
-            ld4(xda2 + lr4, (xal2 >> kMaxSlots) & 1u, vv);
-          } else {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) vv[j] = j < nl ? ld_shared_f32(xda2 + lr4 + 4 * j) : 0.0f;
-          }
-#pragma unroll
-          for (int j = 0; j < 4; ++j) sown[j] = o[j] = __fmaf_rn(-alpha, vv[j], o[j]);
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) xd[j] = o[j];
       }
       // per row: ascending columns, products rounded separately (the CRS
       // row loop); the implicit diagonal after the dpos negative offsets
@@ -543,18 +482,6 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
           if (j < nl) a.y_out[r0 + j] = out[j];
       }
       float wa[4] = {0.0f, 0.0f, 0.0f, 0.0f}, wbv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-      if constexpr (FS) {
-        float *so = a.s_out + r0;
-        if (nl == 4 && a.sal) {
-          *reinterpret_cast<float4 *>(so) = make_float4(sown[0], sown[1], sown[2], sown[3]);
-        } else {
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (j < nl) so[j] = sown[j];
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) wa[j] = sown[j];
-      }
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         if constexpr (NW >= 1) wa[j] = j < nl ? ld_shared_f32(stg + a.w0o + lr4 + 4 * j) : 0.0f;
@@ -588,7 +515,6 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
       if (ct == 0) {
 #pragma unroll
         for (int q = 0; q < NR; ++q) a.dot_out[q] = tot[q];
-        if constexpr (FS) *a.alpha_out = (double)alpha;
       }
     }
   }
@@ -601,12 +527,12 @@ constexpr int kSlotSmemPerSm = 226 * 1024;
 
 // Per instantiation, once (outside any stream capture: slots_build calls
 // slots_prepare): the shared-memory opt-in.
-template <int KS, int DP, int M0, int M1, bool FS = false>
+template <int KS, int DP, int M0, int M1>
 struct SlotLaunch {
   static bool ready;
   static cudaError_t prepare() {
     if (ready) return cudaSuccess;
-    const cudaError_t e = cudaFuncSetAttribute(spmv_slots_kernel<KS, DP, M0, M1, FS>,
+    const cudaError_t e = cudaFuncSetAttribute(spmv_slots_kernel<KS, DP, M0, M1>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                kSlotSmemMax);
     if (e == cudaSuccess) ready = true;
@@ -614,7 +540,7 @@ struct SlotLaunch {
   }
   static int per_sm(int smem) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, spmv_slots_kernel<KS, DP, M0, M1, FS>,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, spmv_slots_kernel<KS, DP, M0, M1>,
                                                       kSlotThreads, smem) != cudaSuccess) {
       cudaGetLastError();
       b = 0;
@@ -622,12 +548,12 @@ struct SlotLaunch {
     return b;
   }
   static cudaError_t launch(const SlotArgs &a, int grid, int smem, cudaStream_t stream) {
-    return launch_dependent(spmv_slots_kernel<KS, DP, M0, M1, FS>, grid, kSlotThreads, smem, stream,
+    return launch_dependent(spmv_slots_kernel<KS, DP, M0, M1>, grid, kSlotThreads, smem, stream,
                             a);
   }
 };
-template <int KS, int DP, int M0, int M1, bool FS>
-bool SlotLaunch<KS, DP, M0, M1, FS>::ready = false;
+template <int KS, int DP, int M0, int M1>
+bool SlotLaunch<KS, DP, M0, M1>::ready = false;
 
 template <int KS, int DP>
 cudaError_t prepare_modes(int smem, int *min_per_sm) {
@@ -644,39 +570,26 @@ cudaError_t prepare_modes(int smem, int *min_per_sm) {
   return cudaSuccess;
 }
 
-template <int KS, int DP>
-cudaError_t prepare_fs(int smem, int *min_per_sm) {
-  using F = SlotLaunch<KS, DP, kDotW, kDotSelf, true>;
-  const cudaError_t e = F::prepare();
-  if (e != cudaSuccess) return e;
-  *min_per_sm = std::min(*min_per_sm, F::per_sm(smem));
-  return cudaSuccess;
-}
-
 template <int KS>
-cudaError_t prepare_ks(int smem, int smem_fs, int *min_per_sm, int *min_per_sm_fs) {
+cudaError_t prepare_ks(int smem, int *min_per_sm) {
   *min_per_sm = 1 << 20;
-  *min_per_sm_fs = 1 << 20;
   cudaError_t e = prepare_modes<KS, kDpRuntime>(smem, min_per_sm);
-  if (e == cudaSuccess) e = prepare_fs<KS, kDpRuntime>(smem_fs, min_per_sm_fs);
-  if constexpr (KS == 4 || KS == 6 || KS == 8) {
+  if constexpr (KS == 4 || KS == 6 || KS == 8)
     if (e == cudaSuccess) e = prepare_modes<KS, KS / 2>(smem, min_per_sm);
-    if (e == cudaSuccess) e = prepare_fs<KS, KS / 2>(smem_fs, min_per_sm_fs);
-  }
   return e;
 }
 
-cudaError_t slots_prepare(int K, int smem, int smem_fs, int *per_sm, int *per_sm_fs) {
+cudaError_t slots_prepare(int K, int smem, int *per_sm) {
   switch (K) {
-    case 0: return prepare_ks<0>(smem, smem_fs, per_sm, per_sm_fs);
-    case 1: return prepare_ks<1>(smem, smem_fs, per_sm, per_sm_fs);
-    case 2: return prepare_ks<2>(smem, smem_fs, per_sm, per_sm_fs);
-    case 3: return prepare_ks<3>(smem, smem_fs, per_sm, per_sm_fs);
-    case 4: return prepare_ks<4>(smem, smem_fs, per_sm, per_sm_fs);
-    case 5: return prepare_ks<5>(smem, smem_fs, per_sm, per_sm_fs);
-    case 6: return prepare_ks<6>(smem, smem_fs, per_sm, per_sm_fs);
-    case 7: return prepare_ks<7>(smem, smem_fs, per_sm, per_sm_fs);
-    default: return prepare_ks<8>(smem, smem_fs, per_sm, per_sm_fs);
+    case 0: return prepare_ks<0>(smem, per_sm);
+    case 1: return prepare_ks<1>(smem, per_sm);
+    case 2: return prepare_ks<2>(smem, per_sm);
+    case 3: return prepare_ks<3>(smem, per_sm);
+    case 4: return prepare_ks<4>(smem, per_sm);
+    case 5: return prepare_ks<5>(smem, per_sm);
+    case 6: return prepare_ks<6>(smem, per_sm);
+    case 7: return prepare_ks<7>(smem, per_sm);
+    default: return prepare_ks<8>(smem, per_sm);
   }
 }
 
@@ -686,7 +599,7 @@ cudaError_t slots_prepare(int K, int smem, int smem_fs, int *per_sm, int *per_sm
 void plan_stages(SlotFormat &f) {
   std::vector<std::pair<int, int>> need;  // (offset, slot or -1 for the diagonal)
   for (int q = 0; q < f.K; ++q) need.push_back({f.offs[q], q});
-  need.push_back({0, -1});  // each row's own x_i: the unit diagonal, and s_i of the FS form
+  if (f.unit) need.push_back({0, -1});
   std::sort(need.begin(), need.end());
   f.n_win = 0;
   f.diag_win = -1;
@@ -713,19 +626,9 @@ void plan_stages(SlotFormat &f) {
     else f.diag_win = f.n_win - 1;
   }
   if (f.n_win > 0) close();
-  const int rec = kSlotGroup * slot_rec_bytes(f.K);
-  f.win_span = bytes - rec;
   f.w_off = bytes;
-  f.stage_bytes = bytes + 2 * kWRunBytes;
-  f.stage_bytes_fs = rec + 2 * f.win_span;
-}
-
-// Stages of a form whose stage takes `stage` bytes: two CTAs per SM of two
-// stages each where they fit (twice the consumer warps), else as many
-// stages as fit one CTA.
-int stages_for(int stage) {
-  if (2 * (2 * stage + kSlotTailBytes) <= kSlotSmemPerSm) return 2;
-  return std::min(kMaxSlotStages, (kSlotSmemMax - kSlotTailBytes) / stage);
+  bytes += 2 * kWRunBytes;
+  f.stage_bytes = bytes;
 }
 
 }  // namespace
@@ -792,12 +695,14 @@ int slots_build(CsrPlan &p, cudaStream_t s) {
   f->unit = unit;
   f->n_slices = n_slices;
   plan_stages(*f);
-  f->stages = stages_for(f->stage_bytes);
-  f->stages_fs = stages_for(f->stage_bytes_fs);
-  int per_sm = 0, per_sm_fs = 0;
+  // two CTAs per SM of two stages each where they fit (twice the consumer
+  // warps to hide shared-memory latency), else as many stages as fit one
+  f->stages = 2 * (2 * f->stage_bytes + kSlotTailBytes) <= kSlotSmemPerSm
+                  ? 2
+                  : std::min(kMaxSlotStages, (kSlotSmemMax - kSlotTailBytes) / f->stage_bytes);
+  int per_sm = 0;
   if (f->stages >= 2) {
-    e = slots_prepare(K, f->stages * f->stage_bytes + kSlotTailBytes,
-                      f->stages_fs * f->stage_bytes_fs + kSlotTailBytes, &per_sm, &per_sm_fs);
+    e = slots_prepare(K, f->stages * f->stage_bytes + kSlotTailBytes, &per_sm);
     if (e != cudaSuccess) {
       delete f;
       set_last_error("slot SpMV set-up", e);
@@ -809,8 +714,6 @@ int slots_build(CsrPlan &p, cudaStream_t s) {
     return MLSH_SUCCESS;
   }
   f->grid_per_sm = per_sm;
-  // the FS form is used only where it fits (else BiCGSTAB keeps its separate update)
-  f->grid_per_sm_fs = (f->stages_fs >= 2 && per_sm_fs >= 1) ? per_sm_fs : 0;
   if (pool_alloc(&f->recs, (size_t)f->bytes(), s) != cudaSuccess) {
     cudaGetLastError();
     delete f;
@@ -829,16 +732,13 @@ int slots_build(CsrPlan &p, cudaStream_t s) {
   return MLSH_SUCCESS;
 }
 
-namespace {
-
-int head_of(const float *v, long long e) {
-  return (int)((((uintptr_t)v + 4 * (uintptr_t)e) & 15u) >> 2);
-}
-
-// The launch arguments common to both forms (x is r in the FS form).
-SlotArgs make_args(const CsrPlan &p, const Handle &h, const float *x, int w_dot_w0) {
+template <int M0, int M1>
+cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, const float *x,
+                              double beta, const float *y_in, float *y_out, const float *w0,
+                              const float *w1, double *dot_out, const int *done,
+                              cudaStream_t stream) {
   const SlotFormat &f = *p.slots;
-  SlotArgs a = {};
+  SlotArgs a;
   a.recs = f.recs;
   for (int q = 0; q < kMaxSlots; ++q) {
     a.offs[q] = f.offs[q];
@@ -851,124 +751,72 @@ SlotArgs make_args(const CsrPlan &p, const Handle &h, const float *x, int w_dot_
   }
   a.n_win = f.n_win;
   a.diag_win = f.diag_win;
-  a.win_span = f.win_span;
   // Offsets of unclipped stages: a window of stage R0 starts at element
   // R0 + lo rounded down to 16 bytes, and R0 is a multiple of kGroupRows, so
   // the rounding depends only on lo and the vector's own address.
+  auto head = [](const float *v, long long e) {
+    return (int)((((uintptr_t)v + 4 * (uintptr_t)e) & 15u) >> 2);
+  };
   a.lo_min = 0;
   for (int w = 0; w < f.n_win; ++w) a.lo_min = std::min(a.lo_min, f.win_lo[w]);
-  a.xal = 0;
   for (int q = 0; q < kMaxSlots; ++q) {
     const int w = f.slot_win[q];
-    a.xo[q] = q < f.K ? f.win_off[w] + 4 * f.offs[q] - 4 * (f.win_lo[w] - head_of(x, f.win_lo[w]))
+    a.xo[q] = q < f.K ? f.win_off[w] + 4 * f.offs[q] - 4 * (f.win_lo[w] - head(x, f.win_lo[w]))
                       : 0;
-    if (q < f.K && (a.xo[q] & 15) == 0) a.xal |= 1u << q;
   }
-  const int dw = f.diag_win;
-  a.xdo = f.win_off[dw] - 4 * (f.win_lo[dw] - head_of(x, f.win_lo[dw]));
-  if ((a.xdo & 15) == 0) a.xal |= 1u << kMaxSlots;
+  a.xdo = f.diag_win >= 0
+              ? f.win_off[f.diag_win] - 4 * (f.win_lo[f.diag_win] - head(x, f.win_lo[f.diag_win]))
+              : 0;
+  {
+    const float *wv0 = (M0 == kDotW) ? w0 : w1;
+    a.w0o = f.w_off + 4 * (wv0 ? head(wv0, 0) : 0);
+    a.w1o = f.w_off + kWRunBytes + 4 * (w1 ? head(w1, 0) : 0);
+  }
   a.dpos = f.unit ? (int)(std::lower_bound(f.offs, f.offs + f.K, 0) - f.offs) : kMaxSlots + 1;
+  a.xal = 0;
+  for (int q = 0; q < f.K; ++q)
+    if ((a.xo[q] & 15) == 0) a.xal |= 1u << q;
+  if (f.diag_win >= 0 && (a.xdo & 15) == 0) a.xal |= 1u << kMaxSlots;
   const unsigned mk = f.K >= 8 ? 0xffu : ((1u << f.K) - 1u);
   a.full4 = mk | (mk << 8) | (mk << 16) | (mk << 24);
+  a.yal = ((uintptr_t)y_out & 15u) == 0 ? 1 : 0;
   a.w_off = f.w_off;
+  a.stage_bytes = f.stage_bytes;
+  a.stages = f.stages;
   a.unit = f.unit;
   a.n_rows = p.n_rows;
   a.n_slices = f.n_slices;
   a.n_groups = (f.n_slices + kSlotGroup - 1) / kSlotGroup;
   a.x = x;
-  a.partials = h.partials;
-  a.counter = h.counters;
-  a.err = h.err_flag;
-  (void)w_dot_w0;
-  return a;
-}
-
-template <int M0, int M1, bool FS>
-cudaError_t launch_slots(const SlotFormat &f, const SlotArgs &a, int grid, int smem,
-                         cudaStream_t stream) {
-  const bool sym = f.unit && a.dpos == f.K / 2 && (f.K % 2) == 0;
-  if (sym && f.K == 4) return SlotLaunch<4, 2, M0, M1, FS>::launch(a, grid, smem, stream);
-  if (sym && f.K == 6) return SlotLaunch<6, 3, M0, M1, FS>::launch(a, grid, smem, stream);
-  if (sym && f.K == 8) return SlotLaunch<8, 4, M0, M1, FS>::launch(a, grid, smem, stream);
-  switch (f.K) {
-    case 0: return SlotLaunch<0, kDpRuntime, M0, M1, FS>::launch(a, grid, smem, stream);
-    case 1: return SlotLaunch<1, kDpRuntime, M0, M1, FS>::launch(a, grid, smem, stream);
-    case 2: return SlotLaunch<2, kDpRuntime, M0, M1, FS>::launch(a, grid, smem, stream);
-    case 3: return SlotLaunch<3, kDpRuntime, M0, M1, FS>::launch(a, grid, smem, stream);
-    case 4: return SlotLaunch<4, kDpRuntime, M0, M1, FS>::launch(a, grid, smem, stream);
-    case 5: return SlotLaunch<5, kDpRuntime, M0, M1, FS>::launch(a, grid, smem, stream);
-    case 6: return SlotLaunch<6, kDpRuntime, M0, M1, FS>::launch(a, grid, smem, stream);
-    case 7: return SlotLaunch<7, kDpRuntime, M0, M1, FS>::launch(a, grid, smem, stream);
-    default: return SlotLaunch<8, kDpRuntime, M0, M1, FS>::launch(a, grid, smem, stream);
-  }
-}
-
-}  // namespace
-
-cudaError_t launch_spmv_slots_s(const CsrPlan &p, const Handle &h, const float *r,
-                                const float *v, const double *rho, const double *vr0,
-                                double *alpha_out, float *s_out, float *t_out, double *dot_out,
-                                const int *done, cudaStream_t stream) {
-  const SlotFormat &f = *p.slots;
-  SlotArgs a = make_args(p, h, r, 0);
-  a.xv = v;
-  a.s_out = s_out;
-  a.rho = rho;
-  a.vr0 = vr0;
-  a.alpha_out = alpha_out;
-  a.xal2 = 0;
-  for (int q = 0; q < kMaxSlots; ++q) {
-    const int w = f.slot_win[q];
-    a.xo2[q] = q < f.K ? f.win_off[w] + f.win_span + 4 * f.offs[q] -
-                             4 * (f.win_lo[w] - head_of(v, f.win_lo[w]))
-                       : 0;
-    if (q < f.K && (a.xo2[q] & 15) == 0) a.xal2 |= 1u << q;
-  }
-  const int dw = f.diag_win;
-  a.xdo2 = f.win_off[dw] + f.win_span - 4 * (f.win_lo[dw] - head_of(v, f.win_lo[dw]));
-  if ((a.xdo2 & 15) == 0) a.xal2 |= 1u << kMaxSlots;
-  a.sal = ((uintptr_t)s_out & 15u) == 0 ? 1 : 0;
-  a.yal = ((uintptr_t)t_out & 15u) == 0 ? 1 : 0;
-  a.y_out = t_out;
-  a.alpha = 1.0;
-  a.beta = 0.0;
-  a.dot_out = dot_out;
-  a.done = done;
-  a.stage_bytes = f.stage_bytes_fs;
-  a.stages = f.stages_fs;
-  const int smem = f.stages_fs * f.stage_bytes_fs + kSlotTailBytes;
-  const int grid = std::max(1, std::min({a.n_groups, f.grid_per_sm_fs * h.num_sms,
-                                         kMaxPartialBlocks}));
-  return launch_slots<kDotW, kDotSelf, true>(f, a, grid, smem, stream);
-}
-
-template <int M0, int M1>
-cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, const float *x,
-                              double beta, const float *y_in, float *y_out, const float *w0,
-                              const float *w1, double *dot_out, const int *done,
-                              cudaStream_t stream) {
-  const SlotFormat &f = *p.slots;
-  SlotArgs a = make_args(p, h, x, 0);
-  {
-    const float *wv0 = (M0 == kDotW) ? w0 : w1;
-    a.w0o = f.w_off + 4 * (wv0 ? head_of(wv0, 0) : 0);
-    a.w1o = f.w_off + kWRunBytes + 4 * (w1 ? head_of(w1, 0) : 0);
-  }
-  a.yal = ((uintptr_t)y_out & 15u) == 0 ? 1 : 0;
-  a.stage_bytes = f.stage_bytes;
-  a.stages = f.stages;
   a.y_out = y_out;
   a.y_in = y_in;
   a.alpha = alpha;
   a.beta = beta;
   a.w0 = w0;
   a.w1 = w1;
+  a.partials = h.partials;
+  a.counter = h.counters;
   a.dot_out = dot_out;
   a.done = done;
+  a.err = h.err_flag;
   const int smem = f.stages * f.stage_bytes + kSlotTailBytes;
   const int grid = std::max(1, std::min({a.n_groups, f.grid_per_sm * h.num_sms,
                                          kMaxPartialBlocks}));
-  return launch_slots<M0, M1, false>(f, a, grid, smem, stream);
+  const bool sym = f.unit && a.dpos == f.K / 2 && (f.K % 2) == 0;
+  if (sym && f.K == 4) return SlotLaunch<4, 2, M0, M1>::launch(a, grid, smem, stream);
+  if (sym && f.K == 6) return SlotLaunch<6, 3, M0, M1>::launch(a, grid, smem, stream);
+  if (sym && f.K == 8) return SlotLaunch<8, 4, M0, M1>::launch(a, grid, smem, stream);
+  switch (f.K) {
+    case 0: return SlotLaunch<0, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 1: return SlotLaunch<1, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 2: return SlotLaunch<2, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 3: return SlotLaunch<3, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 4: return SlotLaunch<4, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 5: return SlotLaunch<5, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 6: return SlotLaunch<6, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    case 7: return SlotLaunch<7, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+    default: return SlotLaunch<8, kDpRuntime, M0, M1>::launch(a, grid, smem, stream);
+  }
 }
 
 #define MLSH_INST_SLOTS(A, B)                                                              \
