@@ -141,8 +141,9 @@ __host__ __device__ constexpr int slot_rec_bytes(int K) {
 // The SpMV moves kSlotGroup consecutive slices per pipeline stage: their
 // records, and x as a few windows -- offsets closer than kSlotMergeGap share
 // one window x[R0 + lo .. R0 + hi + kSlotGroup * kSlotRows), R0 the stage's
-// first row.
-constexpr int kSlotGroup = 4;
+// first row.  (Two slices: small enough stages for four of them per CTA and
+// two CTAs per SM.)
+constexpr int kSlotGroup = 2;
 constexpr int kSlotMergeGap = 1024;
 constexpr int kMaxSlotWin = kMaxSlots + 1;  // the slots' windows + the diagonal's
 constexpr int kMaxSlotStages = 4;

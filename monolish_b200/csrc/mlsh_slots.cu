@@ -152,7 +152,7 @@ struct SlotArgs {
   int xdo;                 // ... of the diagonal's
   int w0o, w1o;            // ... of the dot weights'
   unsigned xal;            // bit q: slot q's offset is 16-byte aligned; bit 8: the diagonal's
-  unsigned full4;          // four rows' mask bytes with every slot present
+  unsigned fullm;          // a thread's rows' mask bytes with every slot present
   int yal;                 // y is 16-byte aligned
   int dpos;  // unit diagonal: its place among the slots (the count of negative offsets)
   int w_off;
@@ -179,6 +179,8 @@ constexpr int kSlotConsumers = kSlotRows;            // one thread per row of a 
 constexpr int kSlotThreads = kSlotConsumers + 32;   // + the producer warp
 constexpr int kGroupRows = kSlotGroup * kSlotRows;
 constexpr int kWRunBytes = 4 * kGroupRows + 16;     // a weight run, rounded ends
+constexpr int kSlotRowsPerThread = kGroupRows / kSlotConsumers;  // consecutive rows
+static_assert(kSlotRowsPerThread == 2 || kSlotRowsPerThread == 4, "vector width");
 // after the stages: mbarriers, reduction scratch, flags
 constexpr int kSlotTailBytes = 2 * kMaxSlotStages * 8 + 32 * 8 + 16 * 4;
 constexpr int kSlotFlagAbort = 0;
@@ -191,12 +193,42 @@ __device__ __forceinline__ float ld_shared_f32(uint32_t addr) {
   return v;
 }
 
+__device__ __forceinline__ float2 ld_shared_f32x2(uint32_t addr) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+  return v;
+}
+
+// N consecutive floats of shared memory at `addr` (aligned to 4 N bytes)
+template <int N>
+__device__ __forceinline__ void ld_shared_vec(uint32_t addr, float (&o)[N]);
+template <>
+__device__ __forceinline__ void ld_shared_vec<2>(uint32_t addr, float (&o)[2]) {
+  const float2 t = ld_shared_f32x2(addr);
+  o[0] = t.x; o[1] = t.y;
+}
+template <>
+__device__ __forceinline__ void ld_shared_vec<4>(uint32_t addr, float (&o)[4]);
+// N consecutive floats to global memory (aligned to 4 N bytes)
+__device__ __forceinline__ void st_global_vec(float *p, const float (&o)[2]) {
+  *reinterpret_cast<float2 *>(p) = make_float2(o[0], o[1]);
+}
+__device__ __forceinline__ void st_global_vec(float *p, const float (&o)[4]) {
+  *reinterpret_cast<float4 *>(p) = make_float4(o[0], o[1], o[2], o[3]);
+}
+
 __device__ __forceinline__ float4 ld_shared_f32x4(uint32_t addr) {
   float4 v;
   asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
                : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
                : "r"(addr));
   return v;
+}
+
+template <>
+__device__ __forceinline__ void ld_shared_vec<4>(uint32_t addr, float (&o)[4]) {
+  const float4 t = ld_shared_f32x4(addr);
+  o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
 }
 
 // Elements [a, a + len) of v clipped to [0, n): the first element s0, the
@@ -365,9 +397,10 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
   const bool unit = DP >= 0 || a.unit != 0;
   const int dpos = DP >= 0 ? DP : (a.unit ? a.dpos : kMaxSlots + 1);
   const uint32_t smem0 = smem_addr(smem);
-  // thread ct takes rows 4 ct .. 4 ct + 3 of each stage: slice ct / 64 of
-  // the stage, rows sr .. sr + 3 of that slice
-  const int lr0 = 4 * ct;
+  // thread ct takes rows RPT ct .. RPT ct + RPT - 1 of each stage: slice
+  // RPT ct / kSlotRows of the stage, rows sr .. sr + RPT - 1 of that slice
+  constexpr int RPT = kSlotRowsPerThread;
+  const int lr0 = RPT * ct;
   const int gs = lr0 / kSlotRows;
   const int sr = lr0 % kSlotRows;
   const uint32_t lr4 = 4u * (uint32_t)lr0;
@@ -411,49 +444,50 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
     }
     const int ns = min(kSlotGroup, a.n_slices - sl0);
     const long long left = a.n_rows - R0 - lr0;
-    const int nl = left < 4 ? (int)left : 4;  // live rows of this thread
+    const int nl = left < RPT ? (int)left : RPT;  // live rows of this thread
     if (gs < ns && nl > 0) {
       const unsigned char *rec = st + gs * rec_bytes;
-      const uint32_t m4 = *reinterpret_cast<const uint32_t *>(rec + sr);
-      const float *vals = reinterpret_cast<const float *>(rec + kSlotHeadBytes) + sr;
-      float v[KS > 0 ? KS : 1][4], xx[KS > 0 ? KS : 1][4], xd[4], sum[4];
+      const uint32_t m4 = RPT == 4 ? *reinterpret_cast<const uint32_t *>(rec + sr)
+                                   : *reinterpret_cast<const uint16_t *>(rec + sr);
+      const uint32_t vals = smem_addr(rec + kSlotHeadBytes) + 4 * sr;
+      float v[KS > 0 ? KS : 1][RPT], xx[KS > 0 ? KS : 1][RPT], xd[RPT], sum[RPT];
 #pragma unroll
-      for (int q = 0; q < KS; ++q) {
-        const float4 t = *reinterpret_cast<const float4 *>(vals + q * kSlotRows);
-        v[q][0] = t.x; v[q][1] = t.y; v[q][2] = t.z; v[q][3] = t.w;
-      }
-      const bool full = m4 == a.full4;
+      for (int q = 0; q < KS; ++q) ld_shared_vec<RPT>(vals + 4 * q * kSlotRows, v[q]);
+      const bool full = m4 == a.fullm;
+      // a thread's RPT consecutive values of a window: one vector load when
+      // aligned
+      auto ld4 = [&](uint32_t ad, bool al, float (&o)[RPT]) {
+        if (al) {
+          ld_shared_vec<RPT>(ad, o);
+        } else {
+#pragma unroll
+          for (int j = 0; j < RPT; ++j) o[j] = ld_shared_f32(ad + 4 * j);
+        }
+      };
       if (full) {
 #pragma unroll
         for (int q = 0; q < KS; ++q) {
-          if ((xal >> q) & 1u) {
-            const float4 t = ld_shared_f32x4(xa[q] + lr4);
-            xx[q][0] = t.x; xx[q][1] = t.y; xx[q][2] = t.z; xx[q][3] = t.w;
-          } else {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) xx[q][j] = ld_shared_f32(xa[q] + lr4 + 4 * j);
-          }
+          ld4(xa[q] + lr4, (xal >> q) & 1u, xx[q]);
         }
       } else {
 #pragma unroll
         for (int q = 0; q < KS; ++q)
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
+          for (int j = 0; j < RPT; ++j)
             xx[q][j] = ((m4 >> (8 * j + q)) & 1u) ? ld_shared_f32(xa[q] + lr4 + 4 * j) : 0.0f;
       }
       if (unit) {
-        if (xal & (1u << kMaxSlots)) {
-          const float4 t = ld_shared_f32x4(xda + lr4);
-          xd[0] = t.x; xd[1] = t.y; xd[2] = t.z; xd[3] = t.w;
+        if (nl == RPT && (xal & (1u << kMaxSlots))) {
+          ld_shared_vec<RPT>(xda + lr4, xd);
         } else {
 #pragma unroll
-          for (int j = 0; j < 4; ++j) xd[j] = j < nl ? ld_shared_f32(xda + lr4 + 4 * j) : 0.0f;
+          for (int j = 0; j < RPT; ++j) xd[j] = j < nl ? ld_shared_f32(xda + lr4 + 4 * j) : 0.0f;
         }
       }
       // per row: ascending columns, products rounded separately (the CRS
       // row loop); the implicit diagonal after the dpos negative offsets
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < RPT; ++j) {
         float sj = 0.0f;
 #pragma unroll
         for (int q = 0; q < KS; ++q) {
@@ -464,9 +498,9 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
         sum[j] = sj;
       }
       const long long r0 = R0 + lr0;
-      float out[4];
+      float out[RPT];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < RPT; ++j) {
         out[j] = sum[j];  // alpha = 1, beta = 0: (float)(1.0 * (double)sum) == sum
         if (!plain && j < nl) {
           const double ds = (double)sum[j];
@@ -474,21 +508,21 @@ __global__ void __launch_bounds__(kSlotThreads, 2) spmv_slots_kernel(const SlotA
                                    : (float)(a.alpha * ds + a.beta * (double)a.y_in[r0 + j]);
         }
       }
-      if (nl == 4 && a.yal) {
-        *reinterpret_cast<float4 *>(a.y_out + r0) = make_float4(out[0], out[1], out[2], out[3]);
+      if (nl == RPT && a.yal) {
+        st_global_vec(a.y_out + r0, out);
       } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < RPT; ++j)
           if (j < nl) a.y_out[r0 + j] = out[j];
       }
-      float wa[4] = {0.0f, 0.0f, 0.0f, 0.0f}, wbv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      float wa[RPT] = {}, wbv[RPT] = {};
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < RPT; ++j) {
         if constexpr (NW >= 1) wa[j] = j < nl ? ld_shared_f32(stg + a.w0o + lr4 + 4 * j) : 0.0f;
         if constexpr (NW >= 2) wbv[j] = j < nl ? ld_shared_f32(stg + a.w1o + lr4 + 4 * j) : 0.0f;
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < RPT; ++j) {
         if (j < nl) {
           if constexpr (M0 == kDotW) acc[0] += (double)wa[j] * (double)out[j];
           if constexpr (M0 == kDotSelf) acc[0] += (double)out[j] * (double)out[j];
@@ -695,11 +729,16 @@ int slots_build(CsrPlan &p, cudaStream_t s) {
   f->unit = unit;
   f->n_slices = n_slices;
   plan_stages(*f);
-  // two CTAs per SM of two stages each where they fit (twice the consumer
-  // warps to hide shared-memory latency), else as many stages as fit one
-  f->stages = 2 * (2 * f->stage_bytes + kSlotTailBytes) <= kSlotSmemPerSm
-                  ? 2
-                  : std::min(kMaxSlotStages, (kSlotSmemMax - kSlotTailBytes) / f->stage_bytes);
+  // two CTAs per SM with as many stages each (up to kMaxSlotStages) as fit
+  // (twice the consumer warps to hide shared-memory latency), else as many
+  // stages as fit one CTA
+  {
+    const int two = std::min(kMaxSlotStages,
+                             (kSlotSmemPerSm / 2 - kSlotTailBytes) / f->stage_bytes);
+    f->stages = two >= 2 ? two
+                         : std::min(kMaxSlotStages,
+                                    (kSlotSmemMax - kSlotTailBytes) / f->stage_bytes);
+  }
   int per_sm = 0;
   if (f->stages >= 2) {
     e = slots_prepare(K, f->stages * f->stage_bytes + kSlotTailBytes, &per_sm);
@@ -778,8 +817,9 @@ cudaError_t launch_spmv_slots(const CsrPlan &p, const Handle &h, double alpha, c
     if ((a.xo[q] & 15) == 0) a.xal |= 1u << q;
   if (f.diag_win >= 0 && (a.xdo & 15) == 0) a.xal |= 1u << kMaxSlots;
   const unsigned mk = f.K >= 8 ? 0xffu : ((1u << f.K) - 1u);
-  a.full4 = mk | (mk << 8) | (mk << 16) | (mk << 24);
-  a.yal = ((uintptr_t)y_out & 15u) == 0 ? 1 : 0;
+  a.fullm = 0;
+  for (int j = 0; j < kSlotRowsPerThread; ++j) a.fullm |= mk << (8 * j);
+  a.yal = ((uintptr_t)y_out % (4 * kSlotRowsPerThread)) == 0 ? 1 : 0;
   a.w_off = f.w_off;
   a.stage_bytes = f.stage_bytes;
   a.stages = f.stages;
