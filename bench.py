@@ -409,7 +409,7 @@ def run_spmv(args, wl, rank, world, local):
                              "evict-first); consecutive launches read two different "
                              "copies of x, so none finds the previous launch's x in L2",
                        "n_tiles": info["n_tiles"], "n_long_rows": info["n_long_rows"],
-                       "spmv_variant": variant},
+                       "spmv_variant": variant, "short_row_limit": A.tuning()[1]},
             "e2e": {"value": round(e2e_value, 2), "unit": "GB/s",
                     "h2d_bytes_per_step": n * vsz, "d2h_bytes_per_step": n * vsz,
                     "steps": e2e_steps,

@@ -143,6 +143,16 @@ int mlsh_csr_plan_autotune(mlsh_handle handle, mlsh_csr_plan plan,
 int mlsh_csr_plan_set_variant(mlsh_csr_plan plan, int variant);
 int mlsh_csr_plan_get_variant(mlsh_csr_plan plan, int *variant,
                               int *n_variants);
+/* The short-row limit: rows of up to this many entries (8, 16 or 32) are
+ * summed by one thread in row order -- the reference's loop
+ * (crs_matvec.hpp:101-108), so those rows of y are bit-identical to it for
+ * every limit; longer rows are summed by a warp (within the summation error
+ * bound).  mlsh_csr_plan_autotune times the limits that change the work
+ * (16 and 32 only when some row is longer than 8, resp. 16) together with
+ * the kernel variants and keeps the fastest pair; mlsh_csr_plan_tuning
+ * reports the pair in use.  No counterpart in the reference. */
+int mlsh_csr_plan_set_short_rows(mlsh_csr_plan plan, int max_len);
+int mlsh_csr_plan_tuning(mlsh_csr_plan plan, int *variant, int *short_max);
 
 /* Storage layout of an FP32 plan's SpMV (no counterpart in the reference,
  * whose matvec reads the CRS arrays, crs_matvec.hpp:101-108).

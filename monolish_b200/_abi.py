@@ -91,6 +91,8 @@ SIGNATURES = {
     "mlsh_csr_plan_set_variant": (i32, [vp, i32]),
     "mlsh_csr_plan_get_variant": (i32, [vp, C.POINTER(i32), C.POINTER(i32)]),
     "mlsh_csr_plan_set_layout": (i32, [vp, i32, C.POINTER(i32)]),
+    "mlsh_csr_plan_set_short_rows": (i32, [vp, i32]),
+    "mlsh_csr_plan_tuning": (i32, [vp, C.POINTER(i32), C.POINTER(i32)]),
     "mlsh_csr_plan_storage": (i32, [vp, i32, C.POINTER(i32), C.POINTER(i64)]),
     "mlsh_spmv": (i32, [vp, vp, f64, vp, f64, vp]),
     "mlsh_csr_diag": (i32, [vp, vp, vp]),

@@ -176,6 +176,7 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
   a.dot_out = dot_out;
   a.done = done;
   a.err = h.err_flag;
+  a.short_max = p.short_max;
   int v = p.variant;
   // FP64 with two fused dots does not fit 4 CTAs per SM (56 registers: it
   // spills); it runs the same pipeline depth at 3 CTAs per SM instead
@@ -506,6 +507,7 @@ int mlsh_csr_plan_create(mlsh_handle hs, int n_rows, int n_cols, int nnz,
   std::vector<Tile> tiles;
   std::vector<LongRow> longs;
   build_tiles(rp, n_rows, tiles, longs, p.n_chunks);
+  for (int i = 0; i < n_rows; ++i) p.longest_row = std::max(p.longest_row, rp[i + 1] - rp[i]);
   p.n_tiles = (int)tiles.size();
   p.n_long = (int)longs.size();
   bool ok = true;
@@ -624,39 +626,62 @@ int mlsh_csr_plan_autotune(mlsh_handle hs, mlsh_csr_plan ps, const void *d_x, vo
   cudaEvent_t e0, e1;
   MLSH_CUDA_TRY(cudaEventCreate(&e0));
   MLSH_CUDA_TRY(cudaEventCreate(&e1));
-  const int keep = p.variant;
-  int best = keep;
+  const int keep = p.variant, keep_short = p.short_max;
+  int best = keep, best_short = keep_short;
   float best_ms = 1e30f;
   int st = MLSH_SUCCESS;
-  for (int v = 0; v < kNumSpmvVariants && st == MLSH_SUCCESS; ++v) {
-    p.variant = v;
-    // warm up, then time enough launches for ~1 ms of work (at least 3)
-    int reps = 3;
-    for (int pass = 0; pass < 2 && st == MLSH_SUCCESS; ++pass) {
-      cudaEventRecord(e0, h.stream);
-      for (int r = 0; r < reps; ++r) {
-        st = mlsh_spmv(hs, ps, 1.0, d_x, 0.0, d_y);
-        if (st != MLSH_SUCCESS) break;
-      }
-      cudaEventRecord(e1, h.stream);
-      cudaEventSynchronize(e1);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (pass == 0) {
-        const float per = ms / reps;
-        reps = per > 0.f ? (int)std::min(200.f, std::max(3.f, 1.0f / per)) : 3;
-      } else if (ms / reps < best_ms) {
-        best_ms = ms / reps;
-        best = v;
+  // the short-row limits worth timing: 8, and 16 / 32 when some row is
+  // longer than the one before (else they launch the same work)
+  int limits[3] = {kShortRow, 2 * kShortRow, kMaxShortRow};
+  int n_limits = p.longest_row > kShortRow ? (p.longest_row > 2 * kShortRow ? 3 : 2) : 1;
+  for (int li = 0; li < n_limits && st == MLSH_SUCCESS; ++li) {
+    p.short_max = limits[li];
+    for (int v = 0; v < kNumSpmvVariants && st == MLSH_SUCCESS; ++v) {
+      p.variant = v;
+      // warm up, then time enough launches for ~1 ms of work (at least 3)
+      int reps = 3;
+      for (int pass = 0; pass < 2 && st == MLSH_SUCCESS; ++pass) {
+        cudaEventRecord(e0, h.stream);
+        for (int r = 0; r < reps; ++r) {
+          st = mlsh_spmv(hs, ps, 1.0, d_x, 0.0, d_y);
+          if (st != MLSH_SUCCESS) break;
+        }
+        cudaEventRecord(e1, h.stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (pass == 0) {
+          const float per = ms / reps;
+          reps = per > 0.f ? (int)std::min(200.f, std::max(3.f, 1.0f / per)) : 3;
+        } else if (ms / reps < best_ms) {
+          best_ms = ms / reps;
+          best = v;
+          best_short = limits[li];
+        }
       }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   p.variant = st == MLSH_SUCCESS ? best : keep;
+  p.short_max = st == MLSH_SUCCESS ? best_short : keep_short;
   if (chosen) *chosen = p.variant;
   if (best_seconds) *best_seconds = best_ms * 1e-3;
   return st;
+}
+
+int mlsh_csr_plan_set_short_rows(mlsh_csr_plan ps, int max_len) {
+  if (!ps || (max_len != kShortRow && max_len != 2 * kShortRow && max_len != kMaxShortRow))
+    return MLSH_ERR_INVALID_ARG;
+  ps->p.short_max = max_len;
+  return MLSH_SUCCESS;
+}
+
+int mlsh_csr_plan_tuning(mlsh_csr_plan ps, int *variant, int *short_max) {
+  if (!ps) return MLSH_ERR_INVALID_ARG;
+  if (variant) *variant = ps->p.variant;
+  if (short_max) *short_max = ps->p.short_max;
+  return MLSH_SUCCESS;
 }
 
 int mlsh_csr_diag(mlsh_handle hs, mlsh_csr_plan ps, void *d_diag) {

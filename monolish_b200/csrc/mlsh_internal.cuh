@@ -26,7 +26,10 @@ constexpr int kTileNnz = 1792;  // = 256 rows x 7 nonzeros (7-point stencil)
 constexpr int kLongRow = kTileNnz;
 constexpr int kConsumers = 256;  // consumer threads per CTA (8 warps)
 constexpr int kSpmvThreads = kConsumers + 32;  // + one producer warp
-constexpr int kShortRow = 8;     // rows up to this length: thread-per-row sum
+constexpr int kShortRow = 8;     // thread-per-row sums load x in batches of this many
+// Rows up to a plan's short-row limit (kShortRow, 2 kShortRow or 4 kShortRow,
+// picked by the autotuner) are summed by one thread in row order.
+constexpr int kMaxShortRow = 4 * kShortRow;
 constexpr int kDefaultSpmvVariant = 2;  // until the plan is autotuned
 
 // Elementwise / reduction kernels.
@@ -185,6 +188,8 @@ struct CsrPlan {
   double *long_dot = nullptr;     // device, 2 * n_long
   int spmv_grid[4] = {0, 0, 0, 0}; // CTAs of the SpMV launch, per kernel variant
   int variant = 0;                // SpMV kernel variant in use
+  int short_max = kShortRow;      // rows up to this length: one thread, in row order
+  int longest_row = 0;
   // cached derived data
   void *inv_diag = nullptr;       // 1/diag(A), dtype elements
   bool inv_diag_valid = false;

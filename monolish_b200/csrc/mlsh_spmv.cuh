@@ -21,9 +21,11 @@
 //    the stage's "full" mbarrier itself, so warps run ahead of one another
 //    within the stages in flight (no CTA barrier per tile; only chunk tiles
 //    bring them together; the fused-dot launches keep one barrier per tile):
-//      rows of up to kShortRow entries: one thread each, gathering x and
-//              summing in row order with separately rounded products (the
-//              reference's loop, so those rows are bit-identical to it);
+//      rows of up to the plan's short-row limit (8, 16 or 32 entries,
+//              picked by the autotuner): one thread each, gathering x 8
+//              entries at a time and summing in row order with separately
+//              rounded products (the reference's loop, so those rows are
+//              bit-identical to it);
 //      longer rows: the whole warp, one such row after another (lane-
 //              strided partial sums, then an xor tree) -- deterministic;
 //      then y is written coalesced and the fused dots accumulate in a
@@ -78,6 +80,7 @@ struct SpmvArgs {
   double *dot_out;  // NR results
   const int *done;  // optional: skip the launch when *done != 0
   int *err;         // set to MLSH_ERR_TIMEOUT if a wait gives up
+  int short_max;    // rows up to this length: one thread, in row order
 };
 
 template <typename VT, int STAGES, int CSZ = 4>
@@ -355,24 +358,29 @@ __global__ void __launch_bounds__(kSpmvThreads, MINB)
 
     if (normal) {
       // Each warp handles its 32 rows on its own (no CTA barrier):
-      //  * rows of <= kShortRow entries: one thread each, gathering and
-      //    summing in row order with separately rounded products -- the
-      //    reference's loop, so these rows are bit-identical to it;
+      //  * rows of up to the plan's short-row limit (8, 16 or 32 entries):
+      //    one thread each, gathering and summing in row order with
+      //    separately rounded products -- the reference's loop, so these
+      //    rows are bit-identical to it;
       //  * longer rows: the whole warp, one row after another (lane-strided
       //    partial sums, then an xor tree), the owning thread keeps the sum.
       VT sum = VT(0);
       const int s0 = g0 - nb, len = g1 - g0;
-      if (ct < nrows && len <= kShortRow) {
-        XT xx[kShortRow];
+      const int smax = a.short_max;
+      if (ct < nrows && len <= smax) {
+        // kShortRow gathers in flight at a time; the sum stays in row order
+        for (int u0 = 0; u0 < len; u0 += kShortRow) {
+          XT xx[kShortRow];
 #pragma unroll
-        for (int u = 0; u < kShortRow; ++u)
-          if (u < len) xx[u] = __ldg(a.x + col_at(s0 + u));
+          for (int u = 0; u < kShortRow; ++u)
+            if (u0 + u < len) xx[u] = __ldg(a.x + col_at(s0 + u0 + u));
 #pragma unroll
-        for (int u = 0; u < kShortRow; ++u)
-          if (u < len) sum = spmv_add_rn(sum, spmv_mul_rn(v[s0 + u], (VT)xx[u]));
+          for (int u = 0; u < kShortRow; ++u)
+            if (u0 + u < len) sum = spmv_add_rn(sum, spmv_mul_rn(v[s0 + u0 + u], (VT)xx[u]));
+        }
       }
       prefetch_next();
-      unsigned lm = __ballot_sync(0xffffffffu, ct < nrows && len > kShortRow);
+      unsigned lm = __ballot_sync(0xffffffffu, ct < nrows && len > smax);
       while (lm) {
         const int src = __ffs(lm) - 1;
         lm &= lm - 1;

@@ -160,6 +160,16 @@ class Crs:
     def set_variant(self, v):
         _abi.check(self.lib.mlsh_csr_plan_set_variant(self.plan, int(v)), "set_variant")
 
+    def set_short_rows(self, max_len):
+        _abi.check(self.lib.mlsh_csr_plan_set_short_rows(self.plan, int(max_len)),
+                   "set_short_rows")
+
+    def tuning(self):
+        """(kernel variant, short-row limit) in use."""
+        v, sm = C.c_int(), C.c_int()
+        _abi.check(self.lib.mlsh_csr_plan_tuning(self.plan, C.byref(v), C.byref(sm)), "tuning")
+        return v.value, sm.value
+
     def set_layout(self, layout) -> bool:
         """0: CRS, 1: offset-slot layout (FP32 plans); True if it is in use."""
         applied = C.c_int()

@@ -219,3 +219,39 @@ def test_diag(handle):
     handle.sync()
     ref = np.array([v[rp[i]:rp[i + 1]][ci[rp[i]:rp[i + 1]] == i][0] for i in range(n)])
     assert np.array_equal(d.cpu().numpy(), ref)
+
+
+def test_short_row_limits_and_autotune(handle, restatement):
+    """Every short-row limit (8, 16, 32) sums rows up to the limit in the
+    reference's order (bit-identical) and the rest within the summation
+    bound; the autotuner picks a (variant, limit) pair from the timings and
+    keeps it; on a stencil matrix (rows of <= 7 entries) only the limit 8 is
+    timed."""
+    import torch
+    from monolish_b200.device import Crs
+    n, rp, ci, v = W.zipf(60000, seed=5, maxlen=3000)
+    x = W.uniform_mt(n, -1, 1, 3)
+    y_ref = restatement.spmv(rp, ci, v, x)
+    lens = np.diff(rp)
+    A = Crs(handle, n, n, rp, ci, v)
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.empty(n, dtype=torch.float64, device="cuda")
+    for lim in (8, 16, 32):
+        A.set_short_rows(lim)
+        dy.fill_(float("nan"))
+        A.matvec(dx, dy)
+        handle.sync()
+        y = dy.cpu().numpy()
+        assert np.array_equal(y[lens <= lim], y_ref[lens <= lim]), lim
+        check(rp, ci, v, x, y, y_ref)
+    variant, _ = A.autotune(dx, dy)
+    v_used, lim = A.tuning()
+    assert v_used == variant and lim in (8, 16, 32)
+    A.close()
+    n, rp, ci, v = W.poisson3d(24)
+    A = Crs(handle, n, n, rp, ci, v)
+    dx = torch.from_numpy(W.uniform_mt(n, -1, 1, 4)).cuda()
+    dy = torch.empty(n, dtype=torch.float64, device="cuda")
+    A.autotune(dx, dy)
+    assert A.tuning()[1] == 8
+    A.close()
