@@ -308,6 +308,16 @@ typedef struct {
   int cluster_rows;    /* CLUSTER engine: rows per CTA (a power of two >= 1024);
                           0 picks the smallest that fits 16 CTAs */
   int reserved;
+  /* Device-side limits on waiting (no counterpart in the reference, which
+   * exit()s on a CUDA error, src/internal/monolish_internal.hpp:34-43):
+   * a kernel that runs past one gives up, the call returns MLSH_ERR_TIMEOUT
+   * and the handle stays usable. */
+  double time_limit;   /* wall-clock budget of one solve on the CLUSTER
+                          engine (single solves and batches), checked by the
+                          kernel at every reduction; <= 0: 60 s */
+  int64_t wait_polls;  /* SOR / IC / ILU solves: polls a 32-row block makes for
+                          a block it depends on before it gives up; <= 0:
+                          2^22 (a few seconds) */
 } mlsh_solver_opts;
 
 typedef struct {

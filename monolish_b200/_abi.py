@@ -43,7 +43,8 @@ class SolverOpts(C.Structure):
     _fields_ = [("tol", f64), ("maxiter", i64), ("miniter", i64), ("precond", i32),
                 ("use_graph", i32), ("check_every", i32), ("engine", i32),
                 ("history", C.POINTER(f64)), ("history_len", i64),
-                ("cluster_rows", i32), ("reserved", i32)]
+                ("cluster_rows", i32), ("reserved", i32), ("time_limit", f64),
+                ("wait_polls", i64)]
 
 
 ENGINE_AUTO = 0

@@ -251,7 +251,7 @@ int batch_run(Handle &h, Batch &B, int kind, const void *d_b, void *d_x, const d
     if (n_clusters < 1) return MLSH_NOT_IMPL;
     n_clusters = std::min(n_clusters, g.count);
     const int st = cluster_launch(h, kind, dt, jac, B.d_sys + g.first, g.count, B.d_queue + gi,
-                                  g.rpc, g.csize, n_clusters, kClusterBudgetSeconds, g.stream,
+                                  g.rpc, g.csize, n_clusters, cluster_budget(opts), g.stream,
                                   delta);
     if (st != MLSH_SUCCESS) return st;
   }

@@ -36,6 +36,10 @@ constexpr int kMaxClusterSize = 16;
 constexpr int kClusterMaxDynSmem = 196608;
 // Wall-clock budget of one cluster solve.
 constexpr double kClusterBudgetSeconds = 60.0;
+// A solve's budget: opts->time_limit when set, else the default.
+inline double cluster_budget(const mlsh_solver_opts *opts) {
+  return opts && opts->time_limit > 0.0 ? opts->time_limit : kClusterBudgetSeconds;
+}
 // AUTO engine: longest maxiter sent to the single-launch cluster engine.
 constexpr long long kClusterMaxIterAuto = 2000000;
 // Serving kernel: FP64 rows per CTA (BiCGSTAB's six vectors fit).

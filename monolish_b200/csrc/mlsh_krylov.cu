@@ -1281,7 +1281,7 @@ int cluster_solve_one(Kind kind, Handle &h, CsrPlan &p, const void *b, void *x,
                                 h.stream));
   MLSH_CUDA_TRY(cudaMemsetAsync(d_queue, 0, sizeof(unsigned), h.stream));
   st = cluster_launch(h, kind == kCG ? 0 : 1, p.dtype, jac, d_sys, 1, d_queue, rpc, csize, 1,
-                      kClusterBudgetSeconds, h.stream);
+                      cluster_budget(opts), h.stream);
   if (st != MLSH_SUCCESS) return st;
   MLSH_CUDA_TRY(cudaMemcpyAsync(hs, d_sys, sizeof(ClusterSystem), cudaMemcpyDeviceToHost,
                                 h.stream));
@@ -1341,6 +1341,17 @@ int solve_common(Kind kind, mlsh_handle hs, mlsh_csr_plan ps, const void *b, voi
     const int st = cluster_solve_one(kind, h, p, b, x, opts, res);
     if (st != MLSH_NOT_IMPL) return st;
     if (opts->engine == MLSH_ENGINE_CLUSTER) return MLSH_ERR_INVALID_ARG;
+  }
+  if (pc) {
+    // the sweeps' poll bound is a launch parameter: graphs that captured
+    // another one are dropped
+    const unsigned polls =
+        opts->wait_polls > 0 ? (unsigned)std::min<int64_t>(opts->wait_polls, 1u << 30)
+                             : kDefaultWaitPolls;
+    if (pc->wait_polls != polls) {
+      purge_precond_graphs(h, pc);
+      const_cast<Precond *>(pc)->wait_polls = polls;
+    }
   }
   SolveCtx c;
   c.kind = kind;
@@ -1637,6 +1648,8 @@ int mlsh_solver_opts_default(mlsh_solver_opts *o) {
   o->history_len = 0;
   o->cluster_rows = 0;
   o->reserved = 0;
+  o->time_limit = 0.0;
+  o->wait_polls = 0;
   return MLSH_SUCCESS;
 }
 

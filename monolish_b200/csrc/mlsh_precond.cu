@@ -31,7 +31,7 @@ namespace {
 
 constexpr int kSweepThreads = 256;
 constexpr int kSweepWarps = kSweepThreads / 32;
-constexpr unsigned kWaitPolls = 1u << 22;  // polls per wait (seconds)
+constexpr unsigned kWaitPolls = kDefaultWaitPolls;  // factorizations' polls per wait
 constexpr unsigned kFull = 0xffffffffu;
 
 // ---- explicitly rounded arithmetic
@@ -45,12 +45,14 @@ __device__ __forceinline__ double sqrt_rn(double a) { return __dsqrt_rn(a); }
 __device__ __forceinline__ float sqrt_rn(float a) { return __fsqrt_rn(a); }
 
 // Waits until *flag == want.  Gives up (recording MLSH_ERR_TIMEOUT) after
-// kWaitPolls polls, or soon after another warp has recorded an error.  The
+// `polls` polls (kWaitPolls unless the solve asked for fewer), or soon after
+// another warp has recorded an error.  The
 // loop is a bare acquire poll (no timer reads, no sleeps): measured on the
 // sweeps, this keeps the hop from a publishing warp to its waiters about
 // half as long as polls interleaved with sleeps or timer reads.
-__device__ __noinline__ bool wait_flag(const unsigned *flag, unsigned want, int *err) {
-  for (unsigned it = 0; it < kWaitPolls; ++it) {
+__device__ __noinline__ bool wait_flag(const unsigned *flag, unsigned want, int *err,
+                                      unsigned polls) {
+  for (unsigned it = 0; it < polls; ++it) {
     if (ld_acquire_gpu(flag) == want) return true;
     if ((it & 1023u) == 1023u && *(volatile int *)err != 0) return false;
   }
@@ -112,6 +114,7 @@ struct SweepArgs {
   const int *order;
   const int *dep_off;
   const int *dep_ids;
+  unsigned polls;  // polls per wait before giving up
 };
 
 template <int MODE, typename T>
@@ -170,9 +173,10 @@ __device__ __forceinline__ S affine_scan(S al, S be, int lane) {
 // Lanes wait, in parallel, for the flags of the block's dependency blocks.
 __device__ __forceinline__ void wait_deps(const int *dep_off, const int *dep_ids,
                                           const unsigned *flags, unsigned blk, unsigned epoch,
-                                          int *err, int lane) {
+                                          int *err, int lane, unsigned polls) {
   const int d1 = dep_off[blk + 1];
-  for (int d = dep_off[blk] + lane; d < d1; d += 32) wait_flag(flags + dep_ids[d], epoch, err);
+  for (int d = dep_off[blk] + lane; d < d1; d += 32)
+    wait_flag(flags + dep_ids[d], epoch, err, polls);
   __syncwarp();
 }
 
@@ -467,7 +471,7 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepArgs<T> a) {
   RowState<T> st;
   if constexpr (BWD) bwd_load<T, MODE>(a, ov, lane, st);
   else fwd_load<T, MODE>(a, ov, lane, st);
-  wait_deps(a.dep_off, a.dep_ids, a.flags, blk, epoch, a.err, lane);
+  wait_deps(a.dep_off, a.dep_ids, a.flags, blk, epoch, a.err, lane, a.polls);
   if constexpr (BWD) bwd_finish_block<T, MODE>(a, ov, lane, GlobalX<T>{a.out}, st);
   else fwd_finish_block<T, MODE>(a, ov, lane, GlobalX<T>{a.out}, st);
   publish_block(a.flags + blk, epoch, lane);
@@ -725,7 +729,7 @@ __global__ void __launch_bounds__(kSweepThreads) factor_kernel(FactorArgs<T> a) 
   const int base = (int)blk * 32;
   const int row = base + lane;
   const bool valid = row < a.n;
-  wait_deps(a.dep_off, a.dep_ids, a.flags, blk, epoch, a.err, lane);
+  wait_deps(a.dep_off, a.dep_ids, a.flags, blk, epoch, a.err, lane, kWaitPolls);
   int q = valid ? a.rp[row] : 0;
   const int le = valid ? a.lo_end[row] : 0;
   // rows outside the block, ascending
@@ -811,6 +815,7 @@ cudaError_t sweep_launch_t(const Precond &pc, const Sweep &sw, bool backward, co
   a.order = sw.order;
   a.dep_off = sw.dep_off;
   a.dep_ids = sw.dep_ids;
+  a.polls = pc.wait_polls;
   const Schedule &sc = backward ? pc.sbwd : pc.sfwd;
   const size_t xbytes = cta_smem_bytes<T>(pc.n, pc.nb, sc.levels);
   if (xbytes <= kCtaSweepBytes) {

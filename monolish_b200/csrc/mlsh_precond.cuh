@@ -78,6 +78,8 @@ struct Schedule {
   long long deps = 0;      // total dependency entries
 };
 
+constexpr unsigned kDefaultWaitPolls = 1u << 22;  // a few seconds of polling
+
 struct Precond {
   Handle *handle = nullptr;
   const CsrPlan *plan = nullptr;
@@ -99,6 +101,7 @@ struct Precond {
   unsigned *flags = nullptr;  // nb block flags
   long long pivot = -1;       // first zero pivot, -1 if none
   int structural = 0;         // 1: that row has no stored diagonal
+  unsigned wait_polls = kDefaultWaitPolls;  // polls per sweep wait (opts->wait_polls)
 };
 
 // out = sweep(rhs) (backward = the upper sweep, blocks from the last row

@@ -240,7 +240,8 @@ class SolveResult:
     outer: int = 0
 
 
-def _opts(tol, maxiter, miniter, precond, use_graph, check_every, engine, cluster_rows):
+def _opts(tol, maxiter, miniter, precond, use_graph, check_every, engine, cluster_rows,
+          time_limit=0.0, wait_polls=0):
     o = _abi.SolverOpts()
     _abi.load().mlsh_solver_opts_default(C.byref(o))
     o.tol, o.maxiter, o.miniter = tol, maxiter, miniter
@@ -249,13 +250,16 @@ def _opts(tol, maxiter, miniter, precond, use_graph, check_every, engine, cluste
     o.check_every = check_every
     o.engine = engine
     o.cluster_rows = cluster_rows
+    o.time_limit = float(time_limit)
+    o.wait_polls = int(wait_polls)
     return o
 
 
 def _solve(fn, A: Crs, b, x, tol, maxiter, miniter=0, precond=_abi.PRECOND_JACOBI,
            use_graph=True, check_every=0, engine=_abi.ENGINE_AUTO, cluster_rows=0,
-           history=None):
-    o = _opts(tol, maxiter, miniter, precond, use_graph, check_every, engine, cluster_rows)
+           history=None, time_limit=0.0):
+    o = _opts(tol, maxiter, miniter, precond, use_graph, check_every, engine, cluster_rows,
+              time_limit=time_limit)
     if history is not None:
         o.history = history.ctypes.data_as(C.POINTER(C.c_double))
         o.history_len = len(history)
@@ -336,9 +340,11 @@ class Batch:
         except Exception:
             pass
 
-    def solve(self, kind, d_b, d_x, tol, maxiter, miniter=0, precond=_abi.PRECOND_JACOBI):
+    def solve(self, kind, d_b, d_x, tol, maxiter, miniter=0, precond=_abi.PRECOND_JACOBI,
+              time_limit=0.0):
         """kind 'cg' or 'bicgstab'; tol: scalar or per-system absolute array."""
-        o = _opts(1e-8, maxiter, miniter, precond, True, 0, _abi.ENGINE_CLUSTER, 0)
+        o = _opts(1e-8, maxiter, miniter, precond, True, 0, _abi.ENGINE_CLUSTER, 0,
+                  time_limit=time_limit)
         tol_arr = np.ascontiguousarray(np.broadcast_to(np.asarray(tol, np.float64),
                                                        (self.n_systems,)))
         status = np.zeros(self.n_systems, np.int32)
@@ -427,9 +433,9 @@ class Precond:
 
 
 def _solve_pc(fn, A: Crs, pc: Precond, b, x, tol, maxiter, miniter=0, use_graph=True,
-              check_every=0, history=None):
+              check_every=0, history=None, wait_polls=0):
     o = _opts(tol, maxiter, miniter, _abi.PRECOND_NONE, use_graph, check_every,
-              _abi.ENGINE_KERNELS, 0)
+              _abi.ENGINE_KERNELS, 0, wait_polls=wait_polls)
     if history is not None:
         o.history = history.ctypes.data_as(C.POINTER(C.c_double))
         o.history_len = len(history)
