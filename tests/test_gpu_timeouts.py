@@ -46,8 +46,9 @@ def test_batch_budget_times_out_then_solves(handle, restatement):
     B = D.Batch(handle, systems)
     db = torch.from_numpy(np.concatenate(bs)).cuda()
     dx = torch.zeros_like(db)
-    status, _, _ = B.solve("cg", db, dx, tol, 20000, time_limit=1e-7)
-    assert (status == _abi.ERR_TIMEOUT).all(), status
+    with pytest.raises(_abi.MlshError) as ei:  # the batch's first non-success status
+        B.solve("cg", db, dx, tol, 20000, time_limit=1e-7)
+    assert ei.value.status == _abi.ERR_TIMEOUT
     dx.zero_()
     status, iters, _ = B.solve("cg", db, dx, tol, 20000)
     assert (status == 0).all()
