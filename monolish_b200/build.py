@@ -97,11 +97,22 @@ def build_oracle():
     _run(["make", "-s", "-j", str(os.cpu_count() or 4), *target, *extra], cwd=oracle)
 
 
+def build_reference_tests():
+    """The reference's own test programs against the C++ layer (test
+    infrastructure), when MONOLISH_REF names the reference source tree."""
+    ref = os.environ.get("MONOLISH_REF", "")
+    if not ref or not os.path.isdir(os.path.join(ref, "test")):
+        return
+    script = os.path.join(ROOT, "tests", "cpp", "reference_tests", "build_reference_tests.py")
+    _run([sys.executable, script, ref])
+
+
 def build_all(force=False):
     build_cuda(force)
     build_gen(force)
     build_facade(force)
     build_oracle()
+    build_reference_tests()
 
 
 if __name__ == "__main__":

@@ -73,3 +73,24 @@ def test_dropin_view1d(progs, cuda):
     exes, _ = progs
     r = subprocess.run([exes["view_test"]], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and "PASS" in r.stdout, r.stdout + r.stderr
+
+
+REF_TESTS = os.path.join(ROOT, "tests", "cpp", "reference_tests", "_build")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prog,args", [("ref_equation", ["test.mtx", "1"]),
+                                       ("ref_blas", ["100"]), ("ref_blas", ["123456"])])
+def test_reference_test_programs(cuda, prog, args):
+    """The reference's own test programs for this path -- the solver test
+    (test/equation/iterative/equation_kernel.hpp: CG and BiCGSTAB, none and
+    Jacobi, CRS<double> and CRS<float>, on the reference's test.mtx, answer
+    checked against ones) and the device forms of its vector BLAS tests
+    (test/vector/blas) -- compiled unchanged against this library's C++
+    layer by tests/cpp/reference_tests/build_reference_tests.py."""
+    exe = os.path.join(REF_TESTS, prog)
+    if not os.path.exists(exe):
+        pytest.skip("reference test programs not built (needs the reference tree)")
+    argv = [exe] + [os.path.join(REF_TESTS, a) if a.endswith(".mtx") else a for a in args]
+    r = subprocess.run(argv, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "PASS" in r.stdout, r.stdout[-3000:] + r.stderr[-2000:]
