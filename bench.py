@@ -982,6 +982,11 @@ def run_batch(args, wl, rank, world, local):
 
 # ---------------------------------------------------------- serving leg
 METRIC_SERVE = "served solves/s (open-loop Poisson arrivals), p50/p99 latency"
+# a stream per offered rate: about --serve-seconds of arrivals, within these
+# bounds (20,000 distinct requests of the stream's size mix would need
+# about 440 GB of host matrices, so the streams cycle through a pool)
+SERVE_MIN_REQUESTS = 100
+SERVE_MAX_REQUESTS = 2000
 # inner tolerance of the stream's mixed-precision requests (the stream's
 # recipe leaves it open; 1e-2 keeps the FP32 iterations well above their
 # attainable accuracy, see the mixed-precision sweep of bicgstab_convdiff)
@@ -1149,10 +1154,21 @@ def run_serve(args, wl, rank, world, local):
     sweep = []
     clocks = ClockSampler(local)
     head = None
+
+    def stream_of(rate):
+        # about serve_seconds of arrivals at this rate (at least 100, at most
+        # 2,000 requests), cycling through the pool of distinct requests
+        total = int(min(SERVE_MAX_REQUESTS, max(SERVE_MIN_REQUESTS, rate * args.serve_seconds)))
+        mine = max(1, int(round(total * share))) if reqs else 0
+        return [reqs[k % len(reqs)] for k in range(mine)], total
+
+    streamed = 0
     for k, rate in enumerate(rates):
         if k == len(rates) - 1:
             clocks.start()
-        res, (launches, lane_solves) = serve_stream(D, reqs, rate * share, budget, lanes,
+        stream, total = stream_of(rate)
+        streamed += total
+        res, (launches, lane_solves) = serve_stream(D, stream, rate * share, budget, lanes,
                                                     40 + k + 1000 * rank, maxiter, start)
         part = {"lat": [r.t_done - r.t_submit for r in res],
                 "span": (max(r.t_done for r in res) - min(r.t_submit for r in res)
@@ -1162,18 +1178,23 @@ def run_serve(args, wl, rank, world, local):
                 "lane": sum(1 for r in res if r.path == 1)}
         got = gather_parts(part, world)
         entry = serve_entry(rate, got)
+        entry["requests"] = total
         sweep.append(entry)
-        head = (res, launches, lane_solves, entry, max(p["span"] for p in got))
+        head = (stream, res, launches, lane_solves, entry, max(p["span"] for p in got), total)
     cl = clocks.stop()
-    res, launches, lane_solves, entry, span = head
+    stream, res, launches, lane_solves, entry, span, head_total = head
+    # the knee: the highest offered rate the server keeps up with (delivers
+    # at least 95 % of it)
+    kept = [e["rate_req_s"] for e in sweep if e["solves_per_s"] >= 0.95 * e["rate_req_s"]]
+    knee = max(kept) if kept else None
     loop_s = None
     if not args.quick and world == 1:
         loop_s, _ = serve_loop_of_single_solves(D, h, reqs, maxiter)
     h.close()
     # true residual of every request, recomputed on the host in FP64
     worst_mine = max((true_relres(q["rp"], q["ci"], q["v"], q["b"], r.x) / q["rel"]
-                      for q, r in zip(reqs, res)), default=0.0)
-    bytes_mine = float(sum(solve_bytes(q, r.iters) for q, r in zip(reqs, res)
+                      for q, r in zip(stream, res)), default=0.0)
+    bytes_mine = float(sum(solve_bytes(q, r.iters) for q, r in zip(stream, res)
                            if q["precision"] == "fp64"))
     parts = gather_parts({"worst": worst_mine, "bytes": bytes_mine,
                           "launches": int(launches + lane_solves)}, world)
@@ -1184,10 +1205,11 @@ def run_serve(args, wl, rank, world, local):
     launches_all = sum(p["launches"] for p in parts)
     reqs = reqs_all
     peak, peak_kind = measured_peak()
+    head_reqs = [reqs[k % len(reqs)] for k in range(head_total)]
     h2d = int(sum(q["rp"].nbytes + q["ci"].nbytes + q["v"].nbytes + q["b"].nbytes
-                  for q in reqs))
-    d2h = int(sum(q["b"].nbytes for q in reqs))
-    value = count / span
+                  for q in head_reqs))
+    d2h = int(sum(q["b"].nbytes for q in head_reqs))
+    value = head_total / span
     fam = {f: sum(1 for q in reqs if q["family"] == f) for f in ("cg2d", "cg3d", "bicgstab")}
     out = {
         "metric": METRIC_SERVE, "value": round(value, 2), "unit": "solves/s",
@@ -1195,11 +1217,16 @@ def run_serve(args, wl, rank, world, local):
         "ms_per_step": round(span * 1e3, 1), "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64 / f32-inner mixed",
         "data": "synthetic (seeded generators)",
-        "config": {"workload": f"open-loop stream of {count} requests (seed 4): CG on 2D/3D "
-                               "variable-coefficient diffusion or BiCGSTAB on convection-"
-                               "diffusion (Peclet U[0,20]), n log-uniform in [1e3, 2e6], tol "
-                               "1e-8 or 1e-10, FP64 or mixed, Poisson arrivals",
-                   "requests": count, "families": fam,
+        "config": {"workload": f"open-loop streams cycling through {count} distinct requests "
+                               "(seed 4): CG on 2D/3D variable-coefficient diffusion or "
+                               "BiCGSTAB on convection-diffusion (Peclet U[0,20]), n log-"
+                               "uniform in [1e3, 2e6], tol 1e-8 or 1e-10, FP64 or mixed, "
+                               f"Poisson arrivals; about {args.serve_seconds:g} s of arrivals "
+                               f"per offered rate ({SERVE_MIN_REQUESTS}-{SERVE_MAX_REQUESTS} "
+                               "requests)",
+                   "distinct_requests": count, "requests_streamed": streamed,
+                   "requests_at_headline_rate": head_total,
+                   "knee_req_s": knee, "families": fam,
                    "mixed_requests": sum(1 for q in reqs if q["precision"] == "mixed"),
                    "rows_total": int(sum(len(q["b"]) for q in reqs)),
                    "memory_budget_bytes": budget, "lanes": lanes,
@@ -1227,8 +1254,8 @@ def run_serve(args, wl, rank, world, local):
     }
     if loop_s is not None:
         out["loop_of_single_solves"] = {
-            "value": round(count / loop_s, 2), "unit": "solves/s",
-            "speedup_of_server": round(value / (count / loop_s), 2),
+            "value": round(len(reqs) / loop_s, 2), "unit": "solves/s",
+            "speedup_of_server": round(value / (len(reqs) / loop_s), 2),
             "note": "same requests one at a time, plain FP64, wall time"}
     if world == 1 and not args.no_cpu:
         cb = cpu_reference_serve(reqs, seconds=20.0)
@@ -1485,8 +1512,10 @@ def main():
                     help="cluster engine: rows per CTA (0 = auto)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="SpMV kernel variant (default: autotuned per matrix)")
-    ap.add_argument("--rates", default="100,500,2000,5000",
+    ap.add_argument("--rates", default="10,30,60,100,500,2000,5000",
                     help="serve_stream: arrival rates (req/s); the last one is the headline")
+    ap.add_argument("--serve-seconds", type=float, default=15.0,
+                    help="serve_stream: seconds of arrivals per offered rate")
     ap.add_argument("--lanes", type=int, default=4, help="serve_stream: worker lanes")
     ap.add_argument("--inner-tol", type=float, default=None,
                     help="mixed precision: inner tolerance / FP64 update threshold "
