@@ -467,6 +467,23 @@ int mlsh_batch_solve(mlsh_handle handle, mlsh_batch batch, int kind, const void 
                      void *d_x, const double *host_tol, const mlsh_solver_opts *opts,
                      int *host_status, int64_t *host_iters, double *host_resid);
 
+/* Autotuner of the batch's bins and cluster shapes (no reference
+ * counterpart).  Each system is solved by a cluster of CTAs holding slices
+ * of its rows: the widest slice (rows per CTA, a power of two) under a cap
+ * that fits the engine, which sets both how many CTAs the system takes and
+ * the group -- one persistent launch -- it joins.  This times one full
+ * batched solve of `kind` (0 CG, 1 BiCGSTAB, 2 mixed-precision CG with
+ * inner_tol as in mlsh_batch_cg_solve_mixed; inner_tol is ignored for 0
+ * and 1) for every cap from 1,024 to 16,384 rows that changes the grouping,
+ * keeps the fastest for later solves of that kind, and restores d_x (the
+ * initial guess) afterwards.  Allocates one copy of x; synchronous. */
+int mlsh_batch_autotune(mlsh_handle handle, mlsh_batch batch, int kind, const void *d_b,
+                        void *d_x, const double *host_tol, const mlsh_solver_opts *opts,
+                        double inner_tol, int *chosen_cap, double *best_seconds);
+/* The rows-per-CTA cap in use for `kind` (0 CG, 1 BiCGSTAB, 2 mixed CG) and
+ * the number of groups (bins) it makes. */
+int mlsh_batch_info(mlsh_batch batch, int kind, int *rows_per_cta_cap, int *n_groups);
+
 /* The batch's Jacobi-CG solves in mixed precision (no reference
  * counterpart): FP32 matrix values and FP32 iteration vectors inside each
  * cluster, the solution and the true residual in FP64.  The FP64 solution

@@ -137,6 +137,9 @@ SIGNATURES = {
     "mlsh_batch_create": (i32, [vp, i32, vp, vp, vp, vp, i32, C.POINTER(vp)]),
     "mlsh_batch_destroy": (i32, [vp]),
     "mlsh_batch_solve": (i32, [vp, vp, i32, vp, vp, vp, C.POINTER(SolverOpts), vp, vp, vp]),
+    "mlsh_batch_autotune": (i32, [vp, vp, i32, vp, vp, vp, C.POINTER(SolverOpts), f64,
+                                  C.POINTER(i32), C.POINTER(f64)]),
+    "mlsh_batch_info": (i32, [vp, i32, C.POINTER(i32), C.POINTER(i32)]),
     "mlsh_batch_cg_solve_mixed": (i32, [vp, vp, vp, vp, vp, C.POINTER(SolverOpts), f64, vp, vp,
                                         vp]),
     "mlsh_server_create": (i32, [C.c_size_t, i32, C.POINTER(vp)]),

@@ -22,6 +22,8 @@
 namespace mlsh {
 
 constexpr int kMaxBatchGroups = 128;
+constexpr int kMaxRowsPerCta = 16384;  // the widest slice the engine takes
+constexpr int kMinRowsPerCta = 1024;
 
 struct BatchGroup {
   int csize = 1;
@@ -43,6 +45,10 @@ struct Batch {
   const void *val = nullptr;
   std::vector<BatchGroup> groups[3];  // per kind (CG, BiCGSTAB, mixed CG)
   float *val32 = nullptr;             // FP32 copy of the values (mixed CG)
+  // rows-per-CTA cap per kind: a system takes the widest slice that fits
+  // under it, which sets both its cluster shape and the group (bin) it
+  // joins; mlsh_batch_autotune times the candidates
+  int rpc_cap[3] = {kMaxRowsPerCta, kMaxRowsPerCta, kMaxRowsPerCta};
   ClusterSystem *d_sys = nullptr;     // n_systems records
   ClusterSystem *h_sys = nullptr;     // pinned mirror
   unsigned *d_queue = nullptr;        // one counter per group
@@ -53,8 +59,12 @@ struct Batch {
 namespace {
 
 // Groups for one kind: systems by needed cluster size (largest first).
+// Each system takes the widest slice (rows per CTA, a power of two up to
+// B.rpc_cap[kind]) that fits the engine; when none under the cap fits, the
+// narrowest that does.
 int build_groups(Batch &B, int kind, std::vector<BatchGroup> &groups,
                  std::vector<int> &order) {
+  const int cap = B.rpc_cap[kind];
   const int n = B.n_systems;
   const int dt = kind == 2 ? MLSH_F32 : B.dtype;  // mixed CG iterates in FP32
   std::vector<int> rpc(n), cs(n);
@@ -64,12 +74,12 @@ int build_groups(Batch &B, int kind, std::vector<BatchGroup> &groups,
     int r = cluster_rows_for(kind, dt, nk, 0);
     if (r == 0) return MLSH_ERR_INVALID_ARG;
     int single = cluster_rows_for(kind, dt, nk, (int)std::max<int64_t>(nk, 1));
-    if (single > 0 && nk <= single) {
+    if (single > 0 && nk <= single && single <= cap) {
       r = single;
     } else {
-      // largest slice that fits: fewer CTAs per system
+      // largest slice under the cap that fits: fewer CTAs per system
       int best = r;
-      for (int t = r; t <= 16384; t <<= 1) {
+      for (int t = r; t <= std::min(cap, kMaxRowsPerCta); t <<= 1) {
         const int ok = cluster_rows_for(kind, dt, nk, t);
         if (ok == t) best = t;
       }
@@ -103,6 +113,16 @@ int build_groups(Batch &B, int kind, std::vector<BatchGroup> &groups,
     ++groups.back().count;
   }
   return MLSH_SUCCESS;
+}
+
+// Forget one kind's grouping (and its streams) so the next run rebuilds it.
+void drop_groups(Batch &B, int kind) {
+  for (BatchGroup &g : B.groups[kind])
+    if (g.stream) {
+      cudaStreamSynchronize(g.stream);
+      cudaStreamDestroy(g.stream);
+    }
+  B.groups[kind].clear();
 }
 
 void free_batch(Batch &B) {
@@ -277,27 +297,8 @@ int batch_run(Handle &h, Batch &B, int kind, const void *d_b, void *d_x, const d
   return first_bad;
 }
 
-}  // namespace
-}  // namespace mlsh
-
-extern "C" {
-
-int mlsh_batch_solve(mlsh_handle hs, mlsh_batch bs, int kind, const void *d_b, void *d_x,
-                     const double *host_tol, const mlsh_solver_opts *opts, int *host_status,
-                     int64_t *host_iters, double *host_resid) {
-  if (!hs || !bs || !opts || (kind != 0 && kind != 1)) return MLSH_ERR_INVALID_ARG;
-  return batch_run(hs->h, bs->b, kind, d_b, d_x, host_tol, opts, 0.0, host_status, host_iters,
-                   host_resid);
-}
-
-int mlsh_batch_cg_solve_mixed(mlsh_handle hs, mlsh_batch bs, const void *d_b, void *d_x,
-                              const double *host_tol, const mlsh_solver_opts *opts,
-                              double inner_tol, int *host_status, int64_t *host_iters,
-                              double *host_resid) {
-  if (!hs || !bs || !opts || !(inner_tol > 0.0) || !(inner_tol < 1.0))
-    return MLSH_ERR_INVALID_ARG;
-  Batch &B = bs->b;
-  Handle &h = hs->h;
+// The FP32 copy of the values the mixed-precision solves iterate with.
+int ensure_val32(Handle &h, Batch &B) {
   if (B.dtype != MLSH_F64) return MLSH_ERR_INVALID_ARG;
   if (B.n_systems > 0 && !B.val32) {
     int nnz = 0;
@@ -315,6 +316,122 @@ int mlsh_batch_cg_solve_mixed(mlsh_handle hs, mlsh_batch bs, const void *d_b, vo
       MLSH_CUDA_TRY(cudaGetLastError());
     }
   }
+  return MLSH_SUCCESS;
+}
+
+}  // namespace
+}  // namespace mlsh
+
+extern "C" {
+
+int mlsh_batch_solve(mlsh_handle hs, mlsh_batch bs, int kind, const void *d_b, void *d_x,
+                     const double *host_tol, const mlsh_solver_opts *opts, int *host_status,
+                     int64_t *host_iters, double *host_resid) {
+  if (!hs || !bs || !opts || (kind != 0 && kind != 1)) return MLSH_ERR_INVALID_ARG;
+  return batch_run(hs->h, bs->b, kind, d_b, d_x, host_tol, opts, 0.0, host_status, host_iters,
+                   host_resid);
+}
+
+int mlsh_batch_autotune(mlsh_handle hs, mlsh_batch bs, int kind, const void *d_b, void *d_x,
+                        const double *host_tol, const mlsh_solver_opts *opts, double inner_tol,
+                        int *chosen_cap, double *best_seconds) {
+  if (!hs || !bs || !opts || kind < 0 || kind > 2 || (bs->b.n_systems > 0 && (!d_b || !d_x)))
+    return MLSH_ERR_INVALID_ARG;
+  if (kind == 2 && !(inner_tol > 0.0 && inner_tol < 1.0)) return MLSH_ERR_INVALID_ARG;
+  Batch &B = bs->b;
+  Handle &h = hs->h;
+  if (kind == 2) {
+    const int vs = ensure_val32(h, B);
+    if (vs != MLSH_SUCCESS) return vs;
+  }
+  const int keep = B.rpc_cap[kind];
+  if (B.n_systems == 0) {
+    if (chosen_cap) *chosen_cap = keep;
+    if (best_seconds) *best_seconds = 0.0;
+    return MLSH_SUCCESS;
+  }
+  // x is the initial guess: kept aside and put back before every timed solve
+  const size_t xbytes = (size_t)dtype_size(B.dtype) * (size_t)B.total_rows;
+  void *x0 = nullptr;
+  MLSH_CUDA_TRY(cudaMalloc(&x0, xbytes));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int st = MLSH_SUCCESS;
+  if (cudaMemcpyAsync(x0, d_x, xbytes, cudaMemcpyDeviceToDevice, h.stream) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    st = MLSH_ERR_CUDA;
+  int best = keep, last_groups = -1;
+  float best_ms = 1e30f;
+  for (int cap = kMinRowsPerCta; cap <= kMaxRowsPerCta && st == MLSH_SUCCESS; cap <<= 1) {
+    B.rpc_cap[kind] = cap;
+    drop_groups(B, kind);
+    st = build_groups(B, kind, B.groups[kind], B.order[kind]);
+    if (st != MLSH_SUCCESS) break;
+    // caps that leave the grouping as the previous one launch the same work
+    int sig = 0;
+    for (const BatchGroup &g : B.groups[kind]) sig = sig * 31 + g.rpc * 7 + g.csize;
+    if (sig == last_groups) continue;
+    last_groups = sig;
+    if (cudaMemcpyAsync(d_x, x0, xbytes, cudaMemcpyDeviceToDevice, h.stream) != cudaSuccess ||
+        cudaEventRecord(e0, h.stream) != cudaSuccess) {
+      st = MLSH_ERR_CUDA;
+      break;
+    }
+    const int rs = batch_run(h, B, kind, d_b, d_x, host_tol, opts, kind == 2 ? inner_tol : 0.0,
+                             nullptr, nullptr, nullptr);
+    if (rs == MLSH_NOT_IMPL) {  // a group shape the engine cannot launch
+      for (const BatchGroup &g : B.groups[kind])
+        if (g.stream) cudaStreamSynchronize(g.stream);  // groups launched before it
+      continue;
+    }
+    if (rs < MLSH_NOT_IMPL) {  // a library error, not a solver status
+      st = rs;
+      break;
+    }
+    cudaEventRecord(e1, h.stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = cap;
+    }
+  }
+  B.rpc_cap[kind] = st == MLSH_SUCCESS ? best : keep;
+  drop_groups(B, kind);
+  const int sg = build_groups(B, kind, B.groups[kind], B.order[kind]);
+  if (st == MLSH_SUCCESS) st = sg;
+  cudaMemcpyAsync(d_x, x0, xbytes, cudaMemcpyDeviceToDevice, h.stream);
+  cudaStreamSynchronize(h.stream);
+  cudaFree(x0);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (chosen_cap) *chosen_cap = B.rpc_cap[kind];
+  if (best_seconds) *best_seconds = best_ms * 1e-3;
+  return st;
+}
+
+int mlsh_batch_info(mlsh_batch bs, int kind, int *rows_per_cta_cap, int *n_groups) {
+  if (!bs || kind < 0 || kind > 2) return MLSH_ERR_INVALID_ARG;
+  Batch &B = bs->b;
+  if (B.groups[kind].empty() && B.n_systems > 0) {
+    const int st = build_groups(B, kind, B.groups[kind], B.order[kind]);
+    if (st != MLSH_SUCCESS) return st;
+  }
+  if (rows_per_cta_cap) *rows_per_cta_cap = B.rpc_cap[kind];
+  if (n_groups) *n_groups = (int)B.groups[kind].size();
+  return MLSH_SUCCESS;
+}
+
+int mlsh_batch_cg_solve_mixed(mlsh_handle hs, mlsh_batch bs, const void *d_b, void *d_x,
+                              const double *host_tol, const mlsh_solver_opts *opts,
+                              double inner_tol, int *host_status, int64_t *host_iters,
+                              double *host_resid) {
+  if (!hs || !bs || !opts || !(inner_tol > 0.0) || !(inner_tol < 1.0))
+    return MLSH_ERR_INVALID_ARG;
+  Batch &B = bs->b;
+  Handle &h = hs->h;
+  const int st = ensure_val32(h, B);
+  if (st != MLSH_SUCCESS) return st;
   return batch_run(h, B, 2, d_b, d_x, host_tol, opts, inner_tol, host_status, host_iters,
                    host_resid);
 }

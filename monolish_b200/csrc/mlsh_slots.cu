@@ -207,28 +207,9 @@ __device__ __forceinline__ void ld_shared_vec<2>(uint32_t addr, float (&o)[2]) {
   const float2 t = ld_shared_f32x2(addr);
   o[0] = t.x; o[1] = t.y;
 }
-template <>
-__device__ __forceinline__ void ld_shared_vec<4>(uint32_t addr, float (&o)[4]);
-// N consecutive floats to global memory (aligned to 4 N bytes)
+// two consecutive floats to global memory (aligned to 8 bytes)
 __device__ __forceinline__ void st_global_vec(float *p, const float (&o)[2]) {
   *reinterpret_cast<float2 *>(p) = make_float2(o[0], o[1]);
-}
-__device__ __forceinline__ void st_global_vec(float *p, const float (&o)[4]) {
-  *reinterpret_cast<float4 *>(p) = make_float4(o[0], o[1], o[2], o[3]);
-}
-
-__device__ __forceinline__ float4 ld_shared_f32x4(uint32_t addr) {
-  float4 v;
-  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-               : "r"(addr));
-  return v;
-}
-
-template <>
-__device__ __forceinline__ void ld_shared_vec<4>(uint32_t addr, float (&o)[4]) {
-  const float4 t = ld_shared_f32x4(addr);
-  o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
 }
 
 // Elements [a, a + len) of v clipped to [0, n): the first element s0, the

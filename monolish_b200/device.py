@@ -375,6 +375,29 @@ class Batch:
             raise _abi.MlshError(st, "batch_cg_solve_mixed")
         return status, iters, resid
 
+    def autotune(self, kind, d_b, d_x, tol, maxiter, precond=_abi.PRECOND_JACOBI,
+                 inner_tol=1e-2):
+        """Times one batched solve per rows-per-CTA cap (1,024 to 16,384) and
+        keeps the fastest for later solves of `kind` ('cg', 'bicgstab' or
+        'mixed'); d_x comes back as it went in.  Returns (cap, seconds of the
+        fastest solve)."""
+        o = _opts(1e-8, maxiter, 0, precond, True, 0, _abi.ENGINE_CLUSTER, 0)
+        tol_arr = np.ascontiguousarray(np.broadcast_to(np.asarray(tol, np.float64),
+                                                       (self.n_systems,)))
+        cap, secs = C.c_int(0), C.c_double(0.0)
+        _abi.check(self.lib.mlsh_batch_autotune(
+            self.handle.h, self.b, {"cg": 0, "bicgstab": 1, "mixed": 2}[kind], ptr(d_b),
+            ptr(d_x), tol_arr.ctypes.data_as(C.c_void_p), C.byref(o), float(inner_tol),
+            C.byref(cap), C.byref(secs)), "batch_autotune")
+        return cap.value, secs.value
+
+    def info(self, kind):
+        """(rows-per-CTA cap, number of groups) for 'cg', 'bicgstab' or 'mixed'."""
+        cap, n_groups = C.c_int(0), C.c_int(0)
+        _abi.check(self.lib.mlsh_batch_info(self.b, {"cg": 0, "bicgstab": 1, "mixed": 2}[kind],
+                                            C.byref(cap), C.byref(n_groups)), "batch_info")
+        return cap.value, n_groups.value
+
 
 def cg_solve(A: Crs, b, x, tol, maxiter, **kw) -> SolveResult:
     return _solve(A.lib.mlsh_cg_solve, A, b, x, tol, maxiter, **kw)

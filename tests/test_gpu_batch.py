@@ -160,3 +160,34 @@ def test_batch_mixed_cg(handle, restatement):
     assert np.array_equal(dx1.cpu().numpy(), xs[k])
     B.close()
     B1.close()
+
+
+def test_batch_autotune(handle, restatement):
+    """The autotuner times one solve per rows-per-CTA cap, keeps the fastest,
+    leaves the initial guess as it found it, and the batch solves to the
+    oracle's statuses and iteration counts (+-2%) under the chosen cap."""
+    import torch
+    from monolish_b200 import device as D
+    systems = make_systems([500, 3000, 9000, 17000, 30000, 60000], seed=23)
+    bs, x0s = [], []
+    for k, (rp, ci, v) in enumerate(systems):
+        bs.append(restatement.spmv(rp, ci, v, W.uniform_mt(len(rp) - 1, -1, 1, 41 + k)))
+        x0s.append(W.uniform_mt(len(rp) - 1, -0.1, 0.1, 61 + k))
+    tol = np.array([1e-8 * np.linalg.norm(b) for b in bs])
+    B = D.Batch(handle, systems)
+    assert B.info("cg")[0] == 16384
+    db = torch.from_numpy(np.concatenate(bs)).cuda()
+    x0 = torch.from_numpy(np.concatenate(x0s)).cuda()
+    dx = x0.clone()
+    cap, secs = B.autotune("cg", db, dx, tol, 5000)
+    assert cap in (1024, 2048, 4096, 8192, 16384) and secs > 0
+    assert torch.equal(dx, x0)
+    assert B.info("cg")[0] == cap and B.info("cg")[1] >= 1
+    status, iters, resid = B.solve("cg", db, dx, tol, 5000)
+    xs = np.split(dx.cpu().numpy(), np.cumsum([len(b) for b in bs])[:-1])
+    for k, (rp, ci, v) in enumerate(systems):
+        st, it, _, _ = restatement.cg(rp, ci, v, bs[k], x0s[k], tol[k], 5000)
+        assert status[k] == st == 0
+        assert abs(iters[k] - it) <= max(1, it // 50), (k, iters[k], it)
+        assert restatement.true_relres(rp, ci, v, bs[k], xs[k]) < 1e-7
+    B.close()
