@@ -652,6 +652,9 @@ def run_precond(args, wl, rank, world, local):
     torch.cuda.synchronize()
     setup_ms = (time.perf_counter() - t0) * 1e3
     lv_lo, lv_up, nblocks = pc.info()
+    forms = pc.sweep_form()
+    form_names = {0: "sweep_kernel (flags across the GPU)", 1: "sweep_cta_kernel (one CTA)",
+                  2: "sweep_ring_kernel (one CTA, record ring)", -1: "none"}
     # one apply (both sweeps) on its own
     r = torch.from_numpy(b / np.linalg.norm(b)).cuda()
     z = torch.empty_like(r)
@@ -729,12 +732,14 @@ def run_precond(args, wl, rank, world, local):
             "roofline": {"bound": "latency", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "peak_kind": peak_kind, "traffic": None,
-                         "kernel": "sweep_fwd_kernel / sweep_bwd_kernel (one apply)",
+                         "kernel": f"lower: {form_names[forms[0]]}; upper: "
+                                   f"{form_names[forms[1]]} (one apply)",
                          "bytes_per_apply": B_apply,
                          "us_per_level": round(apply_ms * 1e3 / max(hops, 1), 2),
                          "note": "algorithmic bytes of one apply / apply time against HBM; the "
                                  "sweeps are bound by their dependency chains: an apply is "
-                                 f"{hops} block levels long, each one wait for another warp"},
+                                 f"{hops} block levels long, each one wait for other warps' "
+                                 "results"},
             # per iteration: CG 6 (SpMV, x/r update, 2 sweeps, z.r, p update),
             # BiCGSTAB 9 (p, 2 sweeps, SpMV, s, 2 sweeps, SpMV, x/r); set-up of a
             # solve: CG 4 (SpMV, 2 sweeps, init), BiCGSTAB 2 (SpMV, init)

@@ -412,6 +412,17 @@ int mlsh_precond_destroy(mlsh_precond pc);
  * (levels_lower + levels_upper) such hops -- and the block count. */
 int mlsh_precond_info(mlsh_precond pc, int *levels_lower, int *levels_upper,
                       int64_t *blocks);
+/* Which kernel runs each sweep: MLSH_SWEEP_FLAGS (blocks spread over the
+ * GPU, one warp per block, per-block flags between warps), MLSH_SWEEP_CTA
+ * (one CTA, the solution in shared memory, a barrier between levels) or
+ * MLSH_SWEEP_RING (one CTA as before, each block's matrix-only row state
+ * precomputed at creation and streamed into a shared-memory ring by bulk
+ * copies ahead of the level being solved).  -1: the sweep does not exist
+ * (SOR as a solver has no upper sweep). */
+#define MLSH_SWEEP_FLAGS 0
+#define MLSH_SWEEP_CTA 1
+#define MLSH_SWEEP_RING 2
+int mlsh_precond_sweep_form(mlsh_precond pc, int *lower, int *upper);
 
 /* CG / BiCGSTAB preconditioned by `pc` (the reference's solvers with
  * set_create_precond / set_apply_precond bound to equation::SOR, IC or

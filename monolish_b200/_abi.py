@@ -128,6 +128,7 @@ SIGNATURES = {
     "mlsh_precond_factor": (i32, [vp, vp, vp]),
     "mlsh_precond_destroy": (i32, [vp]),
     "mlsh_precond_info": (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i64)]),
+    "mlsh_precond_sweep_form": (i32, [vp, C.POINTER(i32), C.POINTER(i32)]),
     "mlsh_cg_solve_precond": (i32, [vp, vp, vp, vp, vp, C.POINTER(SolverOpts),
                                     C.POINTER(SolverResult)]),
     "mlsh_bicgstab_solve_precond": (i32, [vp, vp, vp, vp, vp, C.POINTER(SolverOpts),

@@ -211,7 +211,8 @@ struct RowState {
 
 // Loading a row's state takes two dependent steps: the row's own arrays
 // (stage 1), then what they point to (stage 2).
-template <typename T, int MODE>
+// RHS = false: the matrix-only state (the sweep records), acc left 0.
+template <typename T, int MODE, bool RHS = true>
 __device__ __forceinline__ void fwd_load1(const SweepArgs<T> &a, unsigned ov, int lane,
                                           RowState<T> &st) {
   const int row = (int)(ov & kBlockMask) * 32 + lane;
@@ -223,7 +224,7 @@ __device__ __forceinline__ void fwd_load1(const SweepArgs<T> &a, unsigned ov, in
   if (row < a.n) {
     st.j = a.rp[row];
     st.e = a.lo_end[row];
-    st.acc = a.rhs[row];
+    if constexpr (RHS) st.acc = a.rhs[row];
     if constexpr (MODE == kSorFwd) st.fin = a.scale[row];
     if constexpr (MODE == kDiagFwd) st.split = a.up_beg[row] > st.e;
   }
@@ -333,7 +334,7 @@ __device__ __forceinline__ void fwd_finish_block(const SweepArgs<T> &a, unsigned
   if (valid) X.put(row, xv);
 }
 
-template <typename T, int MODE>
+template <typename T, int MODE, bool RHS = true>
 __device__ __forceinline__ void bwd_load1(const SweepArgs<T> &a, unsigned ov, int lane,
                                           RowState<T> &st) {
   const int row = (int)(ov & kBlockMask) * 32 + lane;
@@ -347,7 +348,7 @@ __device__ __forceinline__ void bwd_load1(const SweepArgs<T> &a, unsigned ov, in
   if (row < a.n) {
     st.jb = a.up_beg[row];
     st.e = a.rp[row + 1];
-    st.rh = a.rhs[row];
+    if constexpr (RHS) st.rh = a.rhs[row];
     if constexpr (MODE == kSorBwd) {
       st.fin = a.scale[row];
     } else {
@@ -580,6 +581,203 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
 }
 
 // ---------------------------------------------------------------------------
+// The single-CTA ring sweep.  What a block's lanes load before any solution
+// value is needed depends on the matrix only, so it is computed once, when
+// the preconditioner is built, into one record per block in level order:
+//   [block entry (id | scan bit), 12 bytes pad]
+//   [T: first entries' values (kPre x 32), finishing factor, a1v (32 each)]
+//   [int: first entries' columns (kPre x 32), j, e, jb, split (32 each)]
+// During a sweep a producer warp streams the records into a ring of slots in
+// shared memory by 1-D bulk copies, up to `ring` blocks ahead of the level
+// being solved (slots free once their level has passed the level barrier),
+// and the right-hand side is bulk-copied into the shared solution vector at
+// the start: each row reads its own right-hand side there before its block
+// writes the row's solution over it (no other block reads an unsolved row).
+// So a level's critical path holds shared-memory reads, the block's
+// arithmetic and the barrier, and no global-memory latency.
+template <typename T>
+struct SweepRec {
+  static constexpr int kHead = 16;
+  static constexpr int kTBytes = (kPre + 2) * 32 * (int)sizeof(T);
+  static constexpr int kIntBytes = (kPre + 4) * 32 * 4;
+  static constexpr int kBytes = kHead + kTBytes + kIntBytes;
+  static_assert(kBytes % 16 == 0, "records are copied in 16-byte units");
+  __device__ static const T *tv(const unsigned char *r) {
+    return reinterpret_cast<const T *>(r + kHead);
+  }
+  __device__ static const int *iv(const unsigned char *r) {
+    return reinterpret_cast<const int *>(r + kHead + kTBytes);
+  }
+};
+
+template <typename T, int MODE, bool BWD>
+__global__ void __launch_bounds__(kSweepThreads)
+    sweep_rec_kernel(SweepArgs<T> a, unsigned char *rec) {
+  const unsigned q = blockIdx.x * kSweepWarps + (threadIdx.x >> 5);
+  if (q >= a.nb) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned ov = (unsigned)a.order[q];
+  RowState<T> st{};
+  if constexpr (BWD) {
+    bwd_load1<T, MODE, false>(a, ov, lane, st);
+    bwd_load2<T, MODE>(a, ov, st);
+  } else {
+    fwd_load1<T, MODE, false>(a, ov, lane, st);
+    fwd_load2<T, MODE>(a, st);
+  }
+  unsigned char *r = rec + (size_t)q * SweepRec<T>::kBytes;
+  T *tv = reinterpret_cast<T *>(r + SweepRec<T>::kHead);
+  int *iv = reinterpret_cast<int *>(r + SweepRec<T>::kHead + SweepRec<T>::kTBytes);
+  if (lane < 4) reinterpret_cast<unsigned *>(r)[lane] = lane == 0 ? ov : 0u;
+#pragma unroll
+  for (int u = 0; u < kPre; ++u) {
+    tv[u * 32 + lane] = st.pv[u];
+    iv[u * 32 + lane] = st.pc[u];
+  }
+  tv[kPre * 32 + lane] = st.fin;
+  tv[(kPre + 1) * 32 + lane] = st.a1v;
+  iv[kPre * 32 + lane] = st.j;
+  iv[(kPre + 1) * 32 + lane] = st.e;
+  iv[(kPre + 2) * 32 + lane] = st.jb;
+  iv[(kPre + 3) * 32 + lane] = st.split;
+}
+
+constexpr int kRingMaxSlots = 64;
+constexpr int kRingMinSlots = 8;
+constexpr size_t kRingSweepBytes = 225 * 1024;
+
+// shared memory of the ring sweep: solution, level starts, ring, barriers
+template <typename T>
+inline size_t ring_smem_bytes(int n, int levels, int slots) {
+  const size_t loff = ((size_t)(levels + 1) * sizeof(int) + 15) / 16 * 16;
+  return cta_x_bytes<T>(n) + loff + (size_t)slots * SweepRec<T>::kBytes +
+         ((size_t)slots + 2) * 8;
+}
+
+// Waits for a ring barrier phase, at most `polls` polls.
+__device__ __forceinline__ bool ring_wait(uint32_t bar, uint32_t parity, unsigned polls) {
+  for (unsigned it = 0; it < polls; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+template <typename T, int MODE, bool BWD>
+__global__ void __launch_bounds__(kCtaThreads, 1)
+    sweep_ring_kernel(SweepArgs<T> a, const int *level_off, int levels,
+                      const unsigned char *rec, int slots) {
+  extern __shared__ __align__(16) unsigned char sweep_smem[];
+  if (a.done != nullptr && *(volatile const int *)a.done != 0) return;
+  constexpr int kRec = SweepRec<T>::kBytes;
+  const size_t xb = cta_x_bytes<T>(a.n);
+  const size_t lb = ((size_t)(levels + 1) * sizeof(int) + 15) / 16 * 16;
+  T *xs = reinterpret_cast<T *>(sweep_smem);
+  int *s_loff = reinterpret_cast<int *>(sweep_smem + xb);
+  unsigned char *ring = sweep_smem + xb + lb;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(ring + (size_t)slots * kRec);
+  // bars[0, slots): one per ring slot; bars[slots]: the right-hand side;
+  // bars[slots + 1] (as an int): set when a wait gave up
+  int *s_fail = reinterpret_cast<int *>(bars + slots + 1);
+  const uint32_t bar0 = smem_addr(bars);
+  const uint32_t bar_rhs = bar0 + 8u * (uint32_t)slots;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kWarps = kCtaThreads / 32;
+  const int nw = kWarps - 1;  // the last warp produces
+  const bool producer = warp == kWarps - 1;
+  const int shift = 31 - __clz(slots);  // slots is a power of two
+  for (int i = threadIdx.x; i <= levels; i += blockDim.x) s_loff[i] = level_off[i];
+  // the right-hand side's bulk-copyable part: 16-byte aligned, whole chunks
+  const bool rhs_bulk = (reinterpret_cast<uintptr_t>(a.rhs) & 15u) == 0;
+  const uint32_t rhs_bytes = rhs_bulk ? (uint32_t)((size_t)a.n * sizeof(T) / 16 * 16) : 0u;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < slots + 1; ++k) mbar_init(bar0 + 8u * (uint32_t)k, 1);
+    *s_fail = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+  int issued = 0;  // producer lane 0: records copied so far
+  if (producer && lane == 0 && rhs_bytes > 0) {
+    mbar_arrive_expect_tx(bar_rhs, rhs_bytes);
+    bulk_g2s(smem_addr(xs), a.rhs, rhs_bytes, bar_rhs);
+  }
+  // what the bulk copy does not cover, by plain loads
+  for (int i = (int)(rhs_bytes / sizeof(T)) + (int)threadIdx.x; i < a.n; i += blockDim.x)
+    xs[i] = a.rhs[i];
+  if (rhs_bytes > 0 && !ring_wait(bar_rhs, 0, a.polls)) *s_fail = 1;
+  __syncthreads();
+  const SharedX<T> X{xs};
+  for (int lv = 0; lv < levels; ++lv) {
+    const int q0 = s_loff[lv], q1 = s_loff[lv + 1];
+    if (producer) {
+      if (lane == 0 && *s_fail == 0) {
+        // slots of blocks below q0 are free: their level has passed the
+        // barrier (after a failed wait nothing more is issued, so every slot
+        // has at most one copy in flight)
+        const int lim = min((int)a.nb, q0 + slots);
+        if (issued < lim) fence_proxy_async_smem();
+        for (; issued < lim; ++issued) {
+          const int slot = issued & (slots - 1);
+          const uint32_t bar = bar0 + 8u * (uint32_t)slot;
+          mbar_arrive_expect_tx(bar, (uint32_t)kRec);
+          bulk_g2s(smem_addr(ring + (size_t)slot * kRec), rec + (size_t)issued * kRec,
+                   (uint32_t)kRec, bar);
+        }
+      }
+    } else {
+      for (int q = q0 + warp; q < q1; q += nw) {
+        if (*(volatile int *)s_fail) break;
+        const int slot = q & (slots - 1);
+        if (!ring_wait(bar0 + 8u * (uint32_t)slot, (uint32_t)(q >> shift) & 1u, a.polls)) {
+          *s_fail = 1;
+          break;
+        }
+        const unsigned char *r = ring + (size_t)slot * kRec;
+        const T *tv = SweepRec<T>::tv(r);
+        const int *iv = SweepRec<T>::iv(r);
+        const unsigned ov = *reinterpret_cast<const unsigned *>(r);
+        RowState<T> st;
+#pragma unroll
+        for (int u = 0; u < kPre; ++u) {
+          st.pv[u] = tv[u * 32 + lane];
+          st.pc[u] = iv[u * 32 + lane];
+        }
+        st.fin = tv[kPre * 32 + lane];
+        st.a1v = tv[(kPre + 1) * 32 + lane];
+        st.j = iv[kPre * 32 + lane];
+        st.e = iv[(kPre + 1) * 32 + lane];
+        st.jb = iv[(kPre + 2) * 32 + lane];
+        st.split = iv[(kPre + 3) * 32 + lane];
+        const int row = (int)(ov & kBlockMask) * 32 + lane;
+        const T own = row < a.n ? xs[row] : T(0);
+        if constexpr (BWD) {
+          st.rh = own;
+          st.acc = MODE == kSorBwd ? T(0) : own;
+          bwd_finish_block<T, MODE>(a, ov, lane, X, st);
+        } else {
+          st.acc = own;
+          fwd_finish_block<T, MODE>(a, ov, lane, X, st);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (*s_fail) {
+    // a wait gave up: record it, and let the copies still in flight land
+    // (bounded) before the CTA's shared memory goes away
+    if (threadIdx.x == 0) {
+      atomicCAS(a.err, 0, MLSH_ERR_TIMEOUT);
+      if (rhs_bytes > 0) ring_wait(bar_rhs, 0, a.polls);
+    }
+    if (producer && lane == 0) {
+      for (int q = max(0, issued - slots); q < issued; ++q)
+        ring_wait(bar0 + 8u * (uint32_t)(q & (slots - 1)), (uint32_t)(q >> shift) & 1u,
+                  a.polls);
+    }
+    return;
+  }
+  for (int i = threadIdx.x; i < a.n; i += blockDim.x) a.out[i] = xs[i];
+}
+
+// ---------------------------------------------------------------------------
 // Schedules: each block's dependency blocks, counted (FILL = false) or
 // written (FILL = true) in ascending order without repeats.  Lower: the
 // blocks of the columns < base its rows reference; upper: those >= base+32.
@@ -766,7 +964,13 @@ int grid_of(long long n, int threads) { return (int)std::max<long long>(1, (n + 
 
 template <typename T, int MODE, bool BWD>
 cudaError_t cta_launch(const SweepArgs<T> &a, const Schedule &sc, size_t xbytes, cudaStream_t s) {
-  sweep_cta_kernel<T, MODE, BWD><<<1, kCtaThreads, xbytes, s>>>(a, sc.level_off, sc.levels);
+  if (sc.ring > 0) {
+    const size_t bytes = ring_smem_bytes<T>(a.n, sc.levels, sc.ring);
+    sweep_ring_kernel<T, MODE, BWD><<<1, kCtaThreads, bytes, s>>>(
+        a, sc.level_off, sc.levels, static_cast<const unsigned char *>(sc.rec), sc.ring);
+  } else {
+    sweep_cta_kernel<T, MODE, BWD><<<1, kCtaThreads, xbytes, s>>>(a, sc.level_off, sc.levels);
+  }
   return cudaGetLastError();
 }
 
@@ -782,6 +986,12 @@ cudaError_t configure_cta_t() {
   if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_cta_kernel<T, kDiagFwd, false>, at, bytes);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_cta_kernel<T, kSorBwd, true>, at, bytes);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_cta_kernel<T, kDiagBwd, true>, at, bytes);
+  const int rb = (int)kRingSweepBytes;
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_ring_kernel<T, kSorFwd, false>, at, rb);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_ring_kernel<T, kUnitFwd, false>, at, rb);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_ring_kernel<T, kDiagFwd, false>, at, rb);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_ring_kernel<T, kSorBwd, true>, at, rb);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_ring_kernel<T, kDiagBwd, true>, at, rb);
   return e;
 }
 
@@ -902,7 +1112,8 @@ void precond_release(Precond &pc) {
                   pc.ci_t,          pc.val_t,         pc.lo_t,          pc.up_t,
                   pc.scale,         pc.tmp,           pc.ticket,        pc.flags,
                   pc.sfwd.order,    pc.sfwd.dep_off,  pc.sfwd.dep_ids,  pc.sbwd.order,
-                  pc.sbwd.dep_off,  pc.sbwd.dep_ids,  pc.sfwd.level_off, pc.sbwd.level_off};
+                  pc.sbwd.dep_off,  pc.sbwd.dep_ids,  pc.sfwd.level_off, pc.sbwd.level_off,
+                  pc.sfwd.rec,      pc.sbwd.rec};
   for (void *b : bufs) pool_free(b, s);
   pc.sfwd = Schedule{};
   pc.sbwd = Schedule{};
@@ -1000,6 +1211,8 @@ int build_schedule(Handle &h, const int *rp, const int *ci, const int *lo, const
   // blocks by level (within a level in sweep direction)
   std::vector<int> start((size_t)levels + 1, 0), order(nb);
   for (unsigned b = 0; b < nb; ++b) ++start[(size_t)lvl[b] + 1];
+  sc.width = 0;
+  for (int l = 0; l < levels; ++l) sc.width = std::max(sc.width, start[(size_t)l + 1]);
   for (int l = 0; l < levels; ++l) start[(size_t)l + 1] += start[(size_t)l];
   MLSH_CUDA_TRY(pool_alloc(&sc.level_off, sizeof(int) * ((size_t)levels + 1), s));
   MLSH_CUDA_TRY(cudaMemcpyAsync(sc.level_off, start.data(), sizeof(int) * ((size_t)levels + 1),
@@ -1120,9 +1333,66 @@ int build_impl(Handle &h, const CsrPlan &p, int kind, double omega, bool solver_
 
 }  // namespace
 
+namespace {
+
+// The ring form of one sweep's single-CTA kernel, where it applies: the
+// solution fits in shared memory beside a ring of at least kRingMinSlots
+// slots, at least twice the widest level (so a level's and the next level's
+// records are all in flight at once).
+template <typename T>
+int build_records_t(Handle &h, const Precond &pc, const Sweep &sw, Schedule &sc) {
+  sc.ring = 0;
+  if (sc.order == nullptr || pc.nb == 0 || sc.levels == 0) return MLSH_SUCCESS;
+  if (cta_smem_bytes<T>(pc.n, pc.nb, sc.levels) > kCtaSweepBytes) return MLSH_SUCCESS;
+  int slots = kRingMaxSlots;
+  while (slots >= kRingMinSlots && ring_smem_bytes<T>(pc.n, sc.levels, slots) > kRingSweepBytes)
+    slots >>= 1;
+  if (slots < kRingMinSlots || slots < 2 * sc.width) return MLSH_SUCCESS;
+  cudaStream_t s = h.stream;
+  MLSH_CUDA_TRY(pool_alloc(&sc.rec, (size_t)SweepRec<T>::kBytes * pc.nb, s));
+  SweepArgs<T> a{};
+  a.rp = sw.rp;
+  a.ci = sw.ci;
+  a.val = static_cast<const T *>(sw.val);
+  a.lo_end = sw.lo_end;
+  a.up_beg = sw.up_beg;
+  a.scale = static_cast<const T *>(sw.scale);
+  a.n = pc.n;
+  a.nb = pc.nb;
+  a.order = sw.order;
+  unsigned char *rec = static_cast<unsigned char *>(sc.rec);
+  const int g = grid_of(pc.nb, kSweepWarps);
+  switch (sw.mode) {
+    case kSorFwd: sweep_rec_kernel<T, kSorFwd, false><<<g, kSweepThreads, 0, s>>>(a, rec); break;
+    case kUnitFwd: sweep_rec_kernel<T, kUnitFwd, false><<<g, kSweepThreads, 0, s>>>(a, rec); break;
+    case kDiagFwd: sweep_rec_kernel<T, kDiagFwd, false><<<g, kSweepThreads, 0, s>>>(a, rec); break;
+    case kSorBwd: sweep_rec_kernel<T, kSorBwd, true><<<g, kSweepThreads, 0, s>>>(a, rec); break;
+    default: sweep_rec_kernel<T, kDiagBwd, true><<<g, kSweepThreads, 0, s>>>(a, rec); break;
+  }
+  MLSH_CUDA_TRY(cudaGetLastError());
+  sc.ring = slots;
+  return MLSH_SUCCESS;
+}
+
+int build_records(Handle &h, Precond &pc) {
+  int st = MLSH_SUCCESS;
+  if (pc.dtype == MLSH_F64) {
+    st = build_records_t<double>(h, pc, pc.fwd, pc.sfwd);
+    if (st == MLSH_SUCCESS) st = build_records_t<double>(h, pc, pc.bwd, pc.sbwd);
+  } else {
+    st = build_records_t<float>(h, pc, pc.fwd, pc.sfwd);
+    if (st == MLSH_SUCCESS) st = build_records_t<float>(h, pc, pc.bwd, pc.sbwd);
+  }
+  if (st == MLSH_SUCCESS) MLSH_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  return st;
+}
+
+}  // namespace
+
 int precond_build(Handle &h, const CsrPlan &p, int kind, double omega, bool solver_scale,
                   Precond &out) {
-  const int st = build_impl(h, p, kind, omega, solver_scale, out);
+  int st = build_impl(h, p, kind, omega, solver_scale, out);
+  if (st == MLSH_SUCCESS) st = build_records(h, out);
   if (st != MLSH_SUCCESS) {
     cudaGetLastError();
     precond_release(out);
@@ -1194,6 +1464,21 @@ int mlsh_precond_factor(mlsh_handle hs, mlsh_precond pc, void *out) {
                                   h.stream));
   }
   MLSH_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  return MLSH_SUCCESS;
+}
+
+int mlsh_precond_sweep_form(mlsh_precond pc, int *lower, int *upper) {
+  if (!pc) return MLSH_ERR_INVALID_ARG;
+  const Precond &p = pc->p;
+  auto form = [&](const Schedule &sc) {
+    if (sc.order == nullptr) return -1;
+    if (sc.ring > 0) return MLSH_SWEEP_RING;
+    const size_t bytes = p.dtype == MLSH_F64 ? cta_smem_bytes<double>(p.n, p.nb, sc.levels)
+                                             : cta_smem_bytes<float>(p.n, p.nb, sc.levels);
+    return bytes <= kCtaSweepBytes ? MLSH_SWEEP_CTA : MLSH_SWEEP_FLAGS;
+  };
+  if (lower) *lower = form(p.sfwd);
+  if (upper) *upper = form(p.sbwd);
   return MLSH_SUCCESS;
 }
 

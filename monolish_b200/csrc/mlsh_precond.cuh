@@ -76,6 +76,12 @@ struct Schedule {
   int *level_off = nullptr;  // levels + 1: where each level starts in order
   int levels = 0;          // length of the longest dependency chain
   long long deps = 0;      // total dependency entries
+  int width = 0;           // most blocks in one level
+  // single-CTA ring sweep: each block's matrix-only row state, in level
+  // order (one record per block), and the shared-memory ring's slot count
+  // (0: the sweep does not take the ring form)
+  void *rec = nullptr;
+  int ring = 0;
 };
 
 constexpr unsigned kDefaultWaitPolls = 1u << 22;  // a few seconds of polling

@@ -436,6 +436,13 @@ class Precond:
         _abi.check(self.lib.mlsh_precond_info(self.pc, C.byref(lo), C.byref(up), C.byref(nb)))
         return int(lo.value), int(up.value), int(nb.value)
 
+    def sweep_form(self):
+        """Kernel form of the (lower, upper) sweep: 0 flags across the GPU,
+        1 single CTA, 2 single CTA with the record ring; -1 none."""
+        lo, up = C.c_int(), C.c_int()
+        _abi.check(self.lib.mlsh_precond_sweep_form(self.pc, C.byref(lo), C.byref(up)))
+        return int(lo.value), int(up.value)
+
     def factor(self):
         """SOR: M (n); IC / ILU: the factor's values in A's pattern (nnz)."""
         n = self.A.n_rows if self.kind == _abi.PRECOND_SOR else self.A.nnz
