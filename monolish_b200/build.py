@@ -7,7 +7,7 @@
   function names) over the C ABI.
 * the checker libraries under ``oracle/`` (``make -C oracle``): the C
   restatement and the generators' oracle-side copy always, the reference CPU
-  build when ``MONOLISH_REF`` names the reference source tree.
+  build when the reference source tree is found (``reference_tree()``).
 """
 from __future__ import annotations
 
@@ -79,17 +79,28 @@ def build_facade(force=False):
     return out
 
 
+def reference_tree():
+    """The monolish source tree the checker libraries are built from:
+    ``MONOLISH_REF`` when set, else a checkout named ``reference`` beside
+    this repository; "" when neither holds a ``src/`` directory."""
+    for ref in (os.environ.get("MONOLISH_REF", ""),
+                os.path.join(os.path.dirname(ROOT), "reference")):
+        if ref and os.path.isdir(os.path.join(ref, "src")):
+            return ref
+    return ""
+
+
 def build_oracle():
     """Checker libraries (test infrastructure only).
 
     The C restatement and the oracle-side copy of the generators always; the
-    reference CPU build only when ``MONOLISH_REF`` names a monolish source
-    tree (its ``src/`` is compiled in place, outputs go to ``oracle/_ref``)."""
+    reference CPU build only when a monolish source tree is found (its
+    ``src/`` is compiled in place, outputs go to ``oracle/_ref``)."""
     oracle = os.path.join(ROOT, "oracle")
     target = ["restatement", "gen"]
-    ref = os.environ.get("MONOLISH_REF", "")
+    ref = reference_tree()
     extra = []
-    if ref and os.path.isdir(os.path.join(ref, "src")):
+    if ref:
         target.append("ref")
         extra.append(f"REF={ref}")
     elif not os.path.exists(os.path.join(oracle, "_ref", "libmlsh_refcapi.so")):
@@ -99,8 +110,8 @@ def build_oracle():
 
 def build_reference_tests():
     """The reference's own test programs against the C++ layer (test
-    infrastructure), when MONOLISH_REF names the reference source tree."""
-    ref = os.environ.get("MONOLISH_REF", "")
+    infrastructure), when the reference source tree is found."""
+    ref = reference_tree()
     if not ref or not os.path.isdir(os.path.join(ref, "test")):
         return
     script = os.path.join(ROOT, "tests", "cpp", "reference_tests", "build_reference_tests.py")
