@@ -23,7 +23,7 @@ namespace cgs = cooperative_groups;
 
 // Shared state of one CTA of the cluster engine.
 struct ClusterShared {
-  double slots[2 * 3 * kMaxClusterSize];  // [parity][k][rank]
+  double slots[2 * kClusterMaxNR * kMaxClusterSize];  // [parity][k][rank]
   double red_warp[32 * 3];
   void *remote_vec[kMaxClusterSize];      // gathered-vector slice of each CTA
   double *remote_slots[kMaxClusterSize];

@@ -142,16 +142,23 @@ __device__ __forceinline__ T cluster_row_dot(const int *__restrict__ rp, const i
   return sum;
 }
 
-// Cluster-wide sum of NR doubles.  `slots` is this CTA's [2][NR][16]
-// buffer; `remote_slots[r]` the same buffer in CTA r.  `parity` alternates
-// between calls (two buffers make one barrier per reduction enough: a slot
-// is rewritten only after a later barrier that every reader has passed).
+// Cluster-wide sum of NR doubles.  `slots` is this CTA's
+// [2][kClusterMaxNR][16] buffer; `remote_slots[r]` the same buffer in CTA r.
+// `parity` alternates between calls (two buffers make one barrier per
+// reduction enough: a slot is rewritten only after a later barrier that every
+// reader has passed).  Each parity owns a fixed kClusterMaxNR-wide half
+// whatever NR is, so consecutive reductions of different widths never share
+// a slot (with a stride of NR, a one-value reduction at parity 1 and the next
+// three-value one at parity 0 would: a CTA ahead could overwrite a slot that
+// another CTA has yet to read).
+constexpr int kClusterMaxNR = 3;
 template <int NR>
 __device__ __forceinline__ void cluster_sum(double (&v)[NR], double *red_warp,
                                             double *const *remote_slots, double *slots,
                                             int parity, unsigned csize, unsigned rank,
                                             cooperative_groups::cluster_group &cl) {
   static_assert(kClusterThreads == 32 * 32, "one warp partial per lane of warp 0");
+  static_assert(NR >= 1 && NR <= kClusterMaxNR, "slots hold kClusterMaxNR values per parity");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < NR; ++k) v[k] = warp_sum(v[k]);
@@ -166,13 +173,14 @@ __device__ __forceinline__ void cluster_sum(double (&v)[NR], double *red_warp,
 #pragma unroll
     for (int k = 0; k < NR; ++k) {
       const double s = warp_sum(red_warp[lane * NR + k]);
-      if ((unsigned)lane < csize) remote_slots[lane][(parity * NR + k) * 16 + rank] = s;
+      if ((unsigned)lane < csize)
+        remote_slots[lane][(parity * kClusterMaxNR + k) * kMaxClusterSize + rank] = s;
     }
   }
   cl.sync();
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
-    const double *sl = slots + (parity * NR + k) * 16;
+    const double *sl = slots + (parity * kClusterMaxNR + k) * kMaxClusterSize;
     double part[kMaxClusterSize];
 #pragma unroll
     for (int r = 0; r < kMaxClusterSize; ++r) part[r] = (unsigned)r < csize ? sl[r] : 0.0;

@@ -191,3 +191,31 @@ def test_batch_autotune(handle, restatement):
         assert abs(iters[k] - it) <= max(1, it // 50), (k, iters[k], it)
         assert restatement.true_relres(rp, ci, v, bs[k], xs[k]) < 1e-7
     B.close()
+
+
+def test_batch_repeats_bitwise(handle, restatement):
+    """Every reduction of the cluster engine has a fixed order, so solving the
+    same batch again gives the same bits; repeats of the 2,048-system batch
+    (the size at which CTAs of one cluster drift furthest apart between
+    barriers) must agree exactly in x, statuses and iteration counts."""
+    import torch
+    from monolish_b200 import device as D
+    systems = W.diffusion_batch(2048, seed=3)
+    bs = [restatement.spmv(rp, ci, v, W.uniform_mt(len(rp) - 1, -1.0, 1.0, 3 + k))
+          for k, (rp, ci, v) in enumerate(systems)]
+    tol = np.array([1e-8 * np.linalg.norm(b) for b in bs])
+    B = D.Batch(handle, systems)
+    db = torch.from_numpy(np.concatenate(bs)).cuda()
+    dx = torch.zeros_like(db)
+    first = None
+    for _ in range(6):
+        dx.zero_()
+        status, iters, _ = B.solve("cg", db, dx, tol, 20000)
+        got = (dx.cpu().numpy(), status.copy(), iters.copy())
+        if first is None:
+            first = got
+            assert (status == 0).all()
+        else:
+            assert np.array_equal(got[1], first[1]) and np.array_equal(got[2], first[2])
+            assert np.array_equal(got[0], first[0])
+    B.close()
