@@ -90,11 +90,13 @@ static int set_spmv_smem() {
   if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 1>();
   if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 2>();
   if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 3>();
+  if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 4>();
   if constexpr (sizeof(VT) == 4) {
     if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 0, true>();
     if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 1, true>();
     if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 2, true>();
     if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 3, true>();
+    if (s == MLSH_SUCCESS) s = set_spmv_smem_one<VT, M0, M1, 4, true>();
   }
   return s;
 }
@@ -143,6 +145,7 @@ static void spmv_grids(int n_tiles, int num_sms, int *grid) {
   grid[1] = spmv_grid_one<VT, 1>(n_tiles, num_sms);
   grid[2] = spmv_grid_one<VT, 2>(n_tiles, num_sms);
   grid[3] = spmv_grid_one<VT, 3>(n_tiles, num_sms);
+  grid[4] = spmv_grid_one<VT, 4>(n_tiles, num_sms);
 }
 
 // ------------------------------------------------------- SpMV launcher --
@@ -184,7 +187,11 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
     static_assert(kSpmvVariants[2].min_blocks == 4 && kSpmvVariants[1].min_blocks == 3 &&
                       kSpmvVariants[1].stages == kSpmvVariants[2].stages,
                   "variant 1 is variant 2 at 3 CTAs per SM");
+    static_assert(kSpmvVariants[4].min_blocks == 4 && kSpmvVariants[0].min_blocks == 3 &&
+                      kSpmvVariants[0].stages == kSpmvVariants[4].stages,
+                  "variant 0 is variant 4 at 3 CTAs per SM");
     if (v == 2) v = 1;
+    if (v == 4) v = 0;
   }
   const int g = p.spmv_grid[v];
   cudaError_t e = cudaSuccess;
@@ -206,6 +213,10 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
           e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 3, true>(), g, kSpmvThreads,
                                spmv_smem_bytes<VT, 3, true>(), stream, a);
           break;
+        case 4:
+          e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 4, true>(), g, kSpmvThreads,
+                               spmv_smem_bytes<VT, 4, true>(), stream, a);
+          break;
         default:
           e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 0, true>(), g, kSpmvThreads,
                                spmv_smem_bytes<VT, 0, true>(), stream, a);
@@ -226,6 +237,10 @@ cudaError_t launch_spmv_t(const CsrPlan &p, const Handle &h, double alpha,
     case 3:
       e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 3>(), g, kSpmvThreads,
                            spmv_smem_bytes<VT, 3>(), stream, a);
+      break;
+    case 4:
+      e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 4>(), g, kSpmvThreads,
+                           spmv_smem_bytes<VT, 4>(), stream, a);
       break;
     default:
       e = launch_dependent(spmv_kernel_ptr<VT, M0, M1, 0>(), g, kSpmvThreads,

@@ -186,7 +186,7 @@ struct CsrPlan {
   double *chunk_part = nullptr;   // device, n_chunks
   unsigned *long_cnt = nullptr;   // device, n_long (zero between launches)
   double *long_dot = nullptr;     // device, 2 * n_long
-  int spmv_grid[4] = {0, 0, 0, 0}; // CTAs of the SpMV launch, per kernel variant
+  int spmv_grid[5] = {0, 0, 0, 0, 0}; // CTAs of the SpMV launch, per kernel variant
   int variant = 0;                // SpMV kernel variant in use
   int short_max = kShortRow;      // rows up to this length: one thread, in row order
   int longest_row = 0;

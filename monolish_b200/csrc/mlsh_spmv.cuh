@@ -505,7 +505,7 @@ struct SpmvVariant {
   int stages;
   int min_blocks;
 };
-constexpr int kNumSpmvVariants = 4;
-constexpr SpmvVariant kSpmvVariants[kNumSpmvVariants] = {{3, 3}, {2, 3}, {2, 4}, {4, 2}};
+constexpr int kNumSpmvVariants = 5;
+constexpr SpmvVariant kSpmvVariants[kNumSpmvVariants] = {{3, 3}, {2, 3}, {2, 4}, {4, 2}, {3, 4}};
 
 }  // namespace mlsh
