@@ -851,6 +851,13 @@ def run_batch(args, wl, rank, world, local):
     for _ in range(args.warmup):
         dx.zero_()
         status, iters, resid = batch_solve()
+    n_launch = B.info("mixed" if mixed else "cg")[1]  # one launch per group
+    batch_traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "batch_cg.traffic.json")) as f:
+            batch_traffic = json.load(f).get("dram_bytes_per_step")
+    except (OSError, ValueError):
+        pass
     clocks = ClockSampler(local)
     clocks.start()
     if world > 1:
@@ -961,10 +968,16 @@ def run_batch(args, wl, rank, world, local):
             "roofline": {"bound": "hbm", "achieved": round(bytes_all / per_step_s / 1e9, 1),
                          "peak": peak, "unit": "GB/s",
                          "frac": round(bytes_all / per_step_s / 1e9 / peak, 4),
-                         "peak_kind": peak_kind, "traffic": None,
-                         "note": "fused-CG algorithmic bytes summed over systems / batch time "
-                                 "(small systems run from L2, so this can exceed HBM)"},
-            "gpu_launches": args.steps,
+                         "peak_kind": peak_kind,
+                         "traffic": batch_traffic if (not mixed and count_total == 2048) else None,
+                         "traffic_unit": "DRAM bytes per batch solve (all its launches)",
+                         "note": "fused-CG algorithmic bytes summed over systems / batch time; "
+                                 "the iteration vectors live in the clusters' shared memory and "
+                                 "each system's matrix stays in L2, so DRAM moves about 5 % of "
+                                 "these bytes: a throughput figure, not a fraction of HBM "
+                                 "traffic (the batch is bound by its largest systems' "
+                                 "iteration latency)"},
+            "gpu_launches": args.steps * n_launch,
         }
         if loop_ms is not None:
             out["loop_of_single_solves"] = {
